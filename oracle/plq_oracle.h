@@ -1,0 +1,147 @@
+/*
+ * plq_oracle.h -- CPU restatement of swvasquez/plaquette's lattice Monte Carlo
+ * hot path.  TEST INFRASTRUCTURE ONLY: this library is the checker that the
+ * CUDA product is compared against (and the timed CPU baseline).  Nothing in
+ * the product links, loads or calls it.
+ *
+ * Two randomness back-ends, matching the two streams the reference uses:
+ *
+ *   STREAM  the reference CPU `Rng` (src/rng.rs:30-50): rand_pcg 0.10.2
+ *           `Pcg64` (= Lcg128Xsl64) seeded by rand_core 0.10.1
+ *           `seed_from_u64`, with rand 0.10.2's `random::<f64>()` and
+ *           `random_range(0..n)` conversions.  Those crates are NOT vendored
+ *           in the reference (Cargo.lock:681-701); their published algorithms
+ *           are restated here.  The LCG128/XSL-RR core is pinned against
+ *           numpy's PCG64 and the PCG paper's known-answer vectors; the
+ *           seeding and the two conversions are restated from the crates'
+ *           documented algorithms and are PARITY UNPINNED (no cargo here).
+ *
+ *   KEYED   the reference GPU stream: `lowbias32` / `keyed_uniform`
+ *           (src/wgsl/rng.wgsl:34-52), fully specified by reference source.
+ *
+ * Every update rule is restated from the reference file:line named beside it.
+ */
+#ifndef PLQ_ORACLE_H
+#define PLQ_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- RNG */
+
+/* PCG64 state as four 64-bit words plus a draw counter (next_u64 calls). */
+typedef struct {
+    uint64_t state_lo, state_hi;
+    uint64_t inc_lo, inc_hi;
+    uint64_t draws;
+} orc_rng;
+
+void     orc_rng_seed_from_u64(orc_rng *r, uint64_t seed);
+void     orc_rng_from_state(orc_rng *r, uint64_t slo, uint64_t shi,
+                            uint64_t ilo, uint64_t ihi);
+uint64_t orc_rng_next_u64(orc_rng *r);
+double   orc_rng_next_f64(orc_rng *r);
+uint64_t orc_rng_next_below(orc_rng *r, uint64_t n);
+/* Advance by `delta` next_u64 steps (O(log delta) jump-ahead). */
+void     orc_rng_advance(orc_rng *r, uint64_t delta);
+
+uint32_t orc_lowbias32(uint32_t x);
+float    orc_keyed_uniform(uint32_t seed, uint32_t variable, uint32_t sweep);
+uint32_t orc_fold_seed(uint64_t seed);
+
+/* ------------------------------------------------------------- lattice */
+
+#define ORC_MAX_D 16
+
+typedef struct {
+    int32_t  d;
+    int64_t  shape[ORC_MAX_D];
+    int64_t  n_sites;
+    int64_t  stride[ORC_MAX_D];
+    int64_t *neighbors;   /* n_sites * 2d, row +0,-0,+1,-1,... */
+    uint8_t *parity;      /* n_sites */
+    int64_t *staples;     /* n_links * 6(d-1), or NULL until built */
+} orc_lattice;
+
+int  orc_lattice_init(orc_lattice *lat, int32_t d, const int64_t *shape);
+int  orc_lattice_build_staples(orc_lattice *lat);
+void orc_lattice_free(orc_lattice *lat);
+
+/* -------------------------------------------------------------- models */
+
+enum { ORC_ISING = 0, ORC_POTTS = 1, ORC_GAUGE = 2 };
+enum { ORC_METROPOLIS = 0, ORC_HEATBATH = 1 };
+enum { ORC_SCHED_RANDOM = 0, ORC_SCHED_CHECKERBOARD = 1 };
+enum { ORC_EXTENT_ALL = 0, ORC_EXTENT_SEEDED = 1 };
+enum { ORC_RELABEL_REDRAW = 0, ORC_RELABEL_FORCED = 1 };
+
+#define ORC_MAX_Q 64
+
+typedef struct {
+    int32_t model;
+    int32_t q;
+    double  j;
+    double  h;                 /* Ising field */
+    double  offsets[ORC_MAX_Q];/* Potts per-label offsets */
+} orc_model;
+
+double orc_energy(const orc_model *m, const orc_lattice *lat, const uint8_t *cfg);
+double orc_energy_delta(const orc_model *m, const orc_lattice *lat,
+                        const uint8_t *cfg, int64_t var, int32_t proposed);
+/* Integer primaries: Ising {bond_sum, spin_sum}; Potts {agree, counts[q]};
+ * gauge {plaquette_sum}.  Returns how many int64 were written. */
+int    orc_primaries(const orc_model *m, const orc_lattice *lat,
+                     const uint8_t *cfg, int64_t *out);
+
+/* -------------------------------------------------- CPU reference path */
+
+/* LocalUpdate::sweep (src/updater.rs:283-348).  Returns the net dE. */
+double orc_local_sweep(const orc_model *m, const orc_lattice *lat, uint8_t *cfg,
+                       int32_t kernel, int32_t schedule, double beta, orc_rng *r);
+double orc_local_sweeps(const orc_model *m, const orc_lattice *lat, uint8_t *cfg,
+                        int32_t kernel, int32_t schedule, double beta, orc_rng *r,
+                        int64_t n_sweeps);
+/* A bounded slice of a checkerboard site sweep: the colour-`color` sites with
+ * index in [lo, hi), in index order (used to time a fixed update budget). */
+double orc_local_site_slice(const orc_model *m, const orc_lattice *lat, uint8_t *cfg,
+                            int32_t kernel, double beta, orc_rng *r,
+                            int32_t color, int64_t lo, int64_t hi, int64_t *updates);
+
+/* ClusterUpdate::bond_probability (src/updater.rs:499-501). */
+double orc_bond_probability(const orc_model *m, double beta);
+/* site_clusters (src/cluster.rs:44-62) with the ClusterUpdate predicate
+ * `peek(i)==peek(j) && next_f64() < p`; writes compacted labels (n_sites)
+ * and returns the cluster count.  sizes may be NULL. */
+int64_t orc_site_clusters(const orc_lattice *lat, const uint8_t *cfg, double p,
+                          orc_rng *r, int64_t *labels, int64_t *sizes);
+/* grow_cluster (src/cluster.rs:88-111) with the same predicate; returns the
+ * member count, members in the order reached. */
+int64_t orc_grow_cluster(const orc_lattice *lat, const uint8_t *cfg, int64_t seed,
+                         double p, orc_rng *r, int64_t *members);
+/* ClusterUpdate::sweep (src/updater.rs:541-613).  Returns the net dE. */
+double orc_cluster_sweep(const orc_model *m, const orc_lattice *lat, uint8_t *cfg,
+                         int32_t extent, int32_t relabel, double beta, orc_rng *r);
+
+/* ----------------------------------------- reference GPU (keyed) path */
+
+/* One sweep of the WGSL checkerboard (metropolis.wgsl / heat_bath.wgsl under
+ * site_schedule.wgsl / link_schedule.wgsl) keyed by (seed32, var, sweep).
+ * Arithmetic is f32 with each operation rounded separately in source order;
+ * exp is evaluated as (float)exp((double)x). */
+void orc_keyed_local_sweep(const orc_model *m, const orc_lattice *lat, uint8_t *cfg,
+                           int32_t kernel, double beta, uint32_t seed32, uint32_t sweep);
+/* One keyed cluster sweep (cluster_prelude.wgsl + cluster_relabel.wgsl):
+ * bonds keyed by bond index, clusters rooted at their minimum site index,
+ * relabel keyed on the root.  root_out (n_sites, may be NULL) receives the
+ * canonical min-site label of every site before relabelling. */
+void orc_keyed_cluster_sweep(const orc_model *m, const orc_lattice *lat, uint8_t *cfg,
+                             int32_t extent, int32_t relabel, double beta,
+                             uint32_t seed32, uint32_t sweep, int64_t *root_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
