@@ -1,0 +1,145 @@
+/*
+ * plaquette.h -- C ABI of the B200 lattice Monte Carlo backend.
+ *
+ * This library replaces the reference's wgpu device path (src/device.rs,
+ * src/gpu_cluster.rs, src/models/{ising,potts,gauge}/gpu.rs, src/wgsl/*)
+ * behind the same chain semantics: a chain owns all device state, `advance`
+ * runs sweeps without waiting, `next` runs `sweeps_between` sweeps and hands
+ * back an owned copy of the configuration.  Plain C types only; the library
+ * owns device memory, callers own host buffers.
+ *
+ * Two randomness modes:
+ *   PLQ_RNG_STREAM  the reference CPU stream (src/rng.rs:30-50, PCG64 from
+ *                   seed_from_u64): a sweep is bit-identical to
+ *                   `LocalUpdate::sweep` with `Schedule::Checkerboard`
+ *                   (src/updater.rs:283-348) or `ClusterUpdate::sweep`
+ *                   (src/updater.rs:541-613) on the CPU.
+ *   PLQ_RNG_KEYED   the reference GPU stream keyed by (seed, variable, sweep)
+ *                   (src/wgsl/rng.wgsl:47-52), order-independent.
+ *
+ * Error handling: every entry point returns PLQ_OK or an error code; the
+ * message of the last failure on the calling thread is plq_last_error().
+ * Contract violations use the reference's panic wording.
+ */
+#ifndef PLAQUETTE_H
+#define PLAQUETTE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ codes */
+#define PLQ_OK 0
+#define PLQ_ENODEV 1        /* no CUDA device: the reference's Gpu::new() == None */
+#define PLQ_EINVAL 2        /* contract violation (message in plq_last_error) */
+#define PLQ_EUNSUPPORTED 3  /* valid for the reference, outside this device path */
+#define PLQ_ECUDA 4         /* a CUDA runtime call failed */
+#define PLQ_ENOMEM 5        /* device or pinned-host allocation failed / over budget */
+#define PLQ_ECAP 6          /* cluster labelling hit its pass cap (gpu_cluster.rs:512-518) */
+#define PLQ_EDEVICE 7       /* a kernel reported a fault in its status word */
+#define PLQ_EBUSY 8         /* serving: no slot or memory free right now */
+
+#define PLQ_MAX_D 8
+#define PLQ_MAX_Q 64
+
+enum plq_model { PLQ_ISING = 0, PLQ_POTTS = 1, PLQ_GAUGE = 2 };
+/* Kernel (src/updater.rs:179-190) or a cluster move (updater.rs:357-445). */
+enum plq_updater { PLQ_METROPOLIS = 0, PLQ_HEATBATH = 1, PLQ_CLUSTER = 2 };
+enum plq_extent { PLQ_EXTENT_ALL = 0, PLQ_EXTENT_SEEDED = 1 };       /* updater.rs:358-373 */
+enum plq_relabel { PLQ_RELABEL_REDRAW = 0, PLQ_RELABEL_FORCED = 1 }; /* updater.rs:377-395 */
+enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
+
+typedef struct plq_ctx plq_ctx;
+typedef struct plq_chain plq_chain;
+
+/* Everything a chain needs; the union of the per-model `gpu_chain` argument
+ * lists (src/models/ising/gpu.rs:57-68, potts/gpu.rs:93-103,
+ * gauge/gpu.rs:54-64) and GpuClusterChain::new (src/gpu_cluster.rs:209-221). */
+typedef struct plq_chain_desc {
+    int32_t model;              /* enum plq_model */
+    int32_t q;                  /* states per variable: 2 for Ising and gauge */
+    int32_t d;                  /* lattice dimension, 1..PLQ_MAX_D */
+    int32_t updater;            /* enum plq_updater */
+    int64_t shape[PLQ_MAX_D];   /* extents, direction 0 fastest (lattice.rs:73-99) */
+    int32_t extent;             /* enum plq_extent (PLQ_CLUSTER only) */
+    int32_t relabel;            /* enum plq_relabel (PLQ_CLUSTER only) */
+    int32_t rng;                /* enum plq_rng */
+    int32_t flags;              /* reserved, 0 */
+    double beta;
+    double j;                   /* coupling J */
+    double h;                   /* Ising field h */
+    double offsets[PLQ_MAX_Q];  /* Potts per-label offsets h[a] */
+    uint64_t seed;              /* keyed: folded as in device.rs:761-763; stream: seed_from_u64 */
+    uint64_t stream_offset;     /* stream: next_u64 draws already consumed (e.g. the hot start) */
+    int64_t sweeps_between;     /* sweeps per `next` (device.rs:590-701) */
+    int64_t batch;              /* samples per device round-trip (GPU_BATCH, device.rs:501) */
+} plq_chain_desc;
+
+/* ------------------------------------------------------- library */
+const char *plq_version(void);
+const char *plq_strerror(int code);
+/* Message of the last failure on this thread (empty string if none). */
+const char *plq_last_error(void);
+int plq_device_count(int *count);
+
+/* Gpu::new (src/device.rs:42-78): PLQ_ENODEV when no device is present. */
+int plq_ctx_create(int device_ordinal, plq_ctx **out);
+void plq_ctx_destroy(plq_ctx *ctx);
+
+/* ------------------------------------------------ host-side helpers */
+/* Contract checks of GpuChain::build (device.rs:609-646), assert_even_extents
+ * (device.rs:714-719), GpuClusterChain::new (gpu_cluster.rs:209-300) and
+ * ClusterUpdate::new (updater.rs:447-483); no device needed. */
+int plq_chain_validate(const plq_chain_desc *desc);
+/* ClusterUpdate::bond_probability (updater.rs:499-501) for the model's gap. */
+double plq_bond_probability(int32_t model, double j, double beta);
+/* fold_seed (device.rs:761-763). */
+uint32_t plq_fold_seed(uint64_t seed);
+/* RandRng::seed_from_u64(seed) then Configuration::hot (configuration.rs:82-87):
+ * n_vars draws of next_below(q).  *draws_out = next_u64 calls consumed, i.e.
+ * the stream offset at which a chain continuing that rng starts. */
+int plq_hot_start(uint64_t seed, int32_t q, int64_t n_vars, uint8_t *out, uint64_t *draws_out);
+
+/* ------------------------------------------------------------ chains */
+/* GpuChain::build (device.rs:609-681) / GpuClusterChain::new
+ * (gpu_cluster.rs:209-300): uploads `start` (n_vars bytes, one state index
+ * per variable in the reference's linear order; links are site*d+dir). */
+int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const uint8_t *start,
+                     plq_chain **out);
+/* GpuChain::advance (device.rs:387-399) / GpuClusterChain::advance
+ * (gpu_cluster.rs:477-481): enqueue sweeps, return without waiting. */
+int plq_chain_advance(plq_chain *chain, uint64_t sweeps);
+/* Iterator::next (device.rs:692-700, gpu_cluster.rs:627-637): run
+ * sweeps_between sweeps, then copy the configuration (n_vars bytes, may be
+ * NULL) and its integer primaries (may be NULL; see plq_chain_primaries). */
+int plq_chain_next(plq_chain *chain, uint8_t *out_states, int64_t *out_primaries);
+/* run_batch (device.rs:435-484): `count` samples, one device round-trip. */
+int plq_chain_next_batch(plq_chain *chain, int64_t count, uint8_t *out_states,
+                         int64_t *out_primaries);
+/* Copy the current configuration without sweeping. */
+int plq_chain_read(plq_chain *chain, uint8_t *out_states);
+/* Exact integer primaries of the current configuration, summed in int64 on
+ * the device: Ising {bond_sum, spin_sum} (ising/mod.rs:67-117); Potts
+ * {agree, count[0..q)} (potts/mod.rs:125-271); gauge {plaquette_sum}
+ * (gauge/mod.rs:99-124).  Returns the count written via *n_out (may be NULL). */
+int plq_chain_primaries(plq_chain *chain, int64_t *out, int32_t *n_out);
+int plq_chain_sync(plq_chain *chain);
+/* Device status word: PLQ_OK, or PLQ_ECAP / PLQ_EDEVICE after a fault. */
+int plq_chain_status(plq_chain *chain);
+uint64_t plq_chain_sweeps_done(plq_chain *chain);
+/* Stream mode: next_u64 draws consumed so far (stream_offset included). */
+int plq_chain_stream_position(plq_chain *chain, uint64_t *out);
+int64_t plq_chain_n_vars(plq_chain *chain);
+/* The chain's cudaStream_t, for callers that time or order work around it. */
+void *plq_chain_cuda_stream(plq_chain *chain);
+/* Kernels this chain has launched so far. */
+uint64_t plq_chain_launches(plq_chain *chain);
+void plq_chain_destroy(plq_chain *chain);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,582 @@
+// plq_abi.cu -- the C ABI: contexts, chains, validation, pass scheduling.
+//
+// Host-side counterpart of the reference's DeviceSweeper / GpuChain
+// (src/device.rs:198-701) and GpuClusterChain (src/gpu_cluster.rs:144-637):
+// the chain owns all device state, one CUDA stream per chain, `advance`
+// enqueues sweeps without waiting, `next` hands back an owned copy.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/plaquette.h"
+#include "plq_abi_internal.h"
+#include "plq_cluster.h"
+#include "plq_device.cuh"
+#include "plq_local.h"
+#include "plq_tables.h"
+
+using namespace plq;
+
+static thread_local std::string g_last_error;
+
+int plq_fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+static int cuda_fail(cudaError_t e, const char *what) {
+    return plq_fail(e == cudaErrorMemoryAllocation ? PLQ_ENOMEM : PLQ_ECUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PLQ_CUDA(call, what)                         \
+    do {                                             \
+        cudaError_t _e = (call);                     \
+        if (_e != cudaSuccess) return cuda_fail(_e, what); \
+    } while (0)
+
+extern "C" const char *plq_version(void) { return "plaquette-b200 0.1 (sm_100a)"; }
+
+extern "C" const char *plq_strerror(int code) {
+    switch (code) {
+        case PLQ_OK: return "ok";
+        case PLQ_ENODEV: return "no CUDA device";
+        case PLQ_EINVAL: return "invalid argument";
+        case PLQ_EUNSUPPORTED: return "unsupported on this device path";
+        case PLQ_ECUDA: return "CUDA runtime error";
+        case PLQ_ENOMEM: return "out of memory";
+        case PLQ_ECAP: return "cluster labeling did not converge within its pass cap";
+        case PLQ_EDEVICE: return "a device kernel reported a fault";
+        case PLQ_EBUSY: return "no slot or memory free";
+        default: return "unknown error";
+    }
+}
+
+extern "C" const char *plq_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int plq_device_count(int *count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) n = 0;
+    if (count) *count = n;
+    return PLQ_OK;
+}
+
+extern "C" int plq_ctx_create(int device_ordinal, plq_ctx **out) {
+    if (!out) return plq_fail(PLQ_EINVAL, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return plq_fail(PLQ_ENODEV, "no CUDA device is available");
+    }
+    if (device_ordinal < 0 || device_ordinal >= n)
+        return plq_fail(PLQ_ENODEV, "device ordinal out of range");
+    PLQ_CUDA(cudaSetDevice(device_ordinal), "cudaSetDevice");
+    cudaDeviceProp prop;
+    PLQ_CUDA(cudaGetDeviceProperties(&prop, device_ordinal), "cudaGetDeviceProperties");
+    plq_ctx *c = new plq_ctx();
+    c->device = device_ordinal;
+    c->sm_count = prop.multiProcessorCount;
+    c->mem_total = prop.totalGlobalMem;
+    c->cc_major = prop.major;
+    *out = c;
+    return PLQ_OK;
+}
+
+extern "C" void plq_ctx_destroy(plq_ctx *ctx) { delete ctx; }
+
+// ------------------------------------------------------------ helpers
+extern "C" uint32_t plq_fold_seed(uint64_t seed) { return (uint32_t)(seed ^ (seed >> 32)); }
+
+static double bond_gap(int32_t model, double j) { return model == PLQ_ISING ? 2.0 * j : j; }
+
+extern "C" double plq_bond_probability(int32_t model, double j, double beta) {
+    return 1.0 - std::exp(-beta * bond_gap(model, j));
+}
+
+extern "C" int plq_hot_start(uint64_t seed, int32_t q, int64_t n_vars, uint8_t *out,
+                             uint64_t *draws_out) {
+    if (q < 2 || q > PLQ_MAX_Q || n_vars < 0 || (!out && n_vars > 0))
+        return plq_fail(PLQ_EINVAL, "plq_hot_start: bad arguments");
+    HostPcg r = host_pcg_from_seed(seed);
+    for (int64_t i = 0; i < n_vars; ++i) out[i] = (uint8_t)r.next_below((uint64_t)q);
+    if (draws_out) *draws_out = r.draws;
+    return PLQ_OK;
+}
+
+std::string shape_string(const plq_chain_desc *d) {
+    std::string s = "[";
+    for (int i = 0; i < d->d; ++i) {
+        if (i) s += ", ";
+        s += std::to_string(d->shape[i]);
+    }
+    return s + "]";
+}
+
+static std::string fmt_gap(double g) {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%g", g);
+    return buf;
+}
+
+extern "C" int plq_chain_validate(const plq_chain_desc *d) {
+    if (!d) return plq_fail(PLQ_EINVAL, "desc is NULL");
+    if (d->model < PLQ_ISING || d->model > PLQ_GAUGE) return plq_fail(PLQ_EINVAL, "unknown model");
+    if (d->d < 1 || d->d > PLQ_MAX_D)
+        return plq_fail(PLQ_EINVAL, "lattice dimension must be in 1..=" + std::to_string(PLQ_MAX_D));
+    if (d->model == PLQ_GAUGE && d->d < 2)
+        return plq_fail(PLQ_EINVAL,
+                        "the Z2 gauge action scores plaquettes, which need at least two dimensions");
+    if (d->model == PLQ_POTTS && d->q < 2)
+        return plq_fail(PLQ_EINVAL,
+                        "the Potts action scores agreement between labels, which needs at least two states");
+    if (d->model != PLQ_POTTS && d->q != 2)
+        return plq_fail(PLQ_EINVAL, "Ising spins and gauge links have q = 2");
+    if (d->q > PLQ_MAX_Q) return plq_fail(PLQ_EINVAL, "q above the supported maximum");
+    int64_t n = 1;
+    for (int i = 0; i < d->d; ++i) {
+        if (d->shape[i] <= 0) return plq_fail(PLQ_EINVAL, "every extent must be positive");
+        if (n > (int64_t(1) << 31) / d->shape[i])
+            return plq_fail(PLQ_EINVAL, "shape" + shape_string(d) + " names more variables than this device path indexes (2^31)");
+        n *= d->shape[i];
+    }
+    int64_t n_vars = d->model == PLQ_GAUGE ? n * d->d : n;
+    if (n_vars > (int64_t(1) << 31))
+        return plq_fail(PLQ_EINVAL, "too many variables for this device path (2^31)");
+    if (d->batch <= 0) return plq_fail(PLQ_EINVAL, "batch size must be positive");
+    if (d->sweeps_between < 0) return plq_fail(PLQ_EINVAL, "sweeps_between must be non-negative");
+    if (d->rng != PLQ_RNG_STREAM && d->rng != PLQ_RNG_KEYED) return plq_fail(PLQ_EINVAL, "unknown rng mode");
+    if (d->updater == PLQ_METROPOLIS || d->updater == PLQ_HEATBATH) {
+        for (int i = 0; i < d->d; ++i)
+            if (d->shape[i] % 2 != 0)
+                return plq_fail(PLQ_EINVAL, std::string("the parallel ") +
+                                                (d->model == PLQ_GAUGE ? "link" : "site") +
+                                                " checkerboard needs even lattice extents, got " +
+                                                shape_string(d));
+        if (d->model == PLQ_POTTS && d->q > 2 && d->updater == PLQ_METROPOLIS && d->rng == PLQ_RNG_STREAM)
+            return plq_fail(PLQ_EUNSUPPORTED,
+                            "Potts Metropolis at q >= 3 on the PCG stream draws its proposal through "
+                            "rand's range sampler; this device path runs it on the keyed stream only");
+        return PLQ_OK;
+    }
+    if (d->updater == PLQ_CLUSTER) {
+        if (d->model == PLQ_GAUGE)
+            return plq_fail(PLQ_EINVAL,
+                            "the cluster update bonds nearest-neighbor sites, so the start must be a site field");
+        bool invariant = d->model == PLQ_ISING ? d->h == 0.0 : true;
+        if (d->model == PLQ_POTTS)
+            for (int a = 0; a < d->q; ++a)
+                if (d->offsets[a] != 0.0) invariant = false;
+        if (!invariant)
+            return plq_fail(PLQ_EINVAL,
+                            "the cluster move relabels a whole cluster at once, which is only weight-preserving "
+                            "when the energy is invariant under relabeling; this model has a per-label offset "
+                            "or an external field set");
+        if (d->extent != PLQ_EXTENT_ALL && d->extent != PLQ_EXTENT_SEEDED)
+            return plq_fail(PLQ_EINVAL, "unknown extent");
+        if (d->relabel != PLQ_RELABEL_REDRAW && d->relabel != PLQ_RELABEL_FORCED)
+            return plq_fail(PLQ_EINVAL, "unknown relabel rule");
+        if (d->q == 2 && d->extent == PLQ_EXTENT_ALL && d->relabel == PLQ_RELABEL_FORCED)
+            return plq_fail(PLQ_EINVAL,
+                            "at Q = 2 a forced change of every cluster is the deterministic global flip on any "
+                            "uniform configuration, so the chain falls into a two-cycle and stops being ergodic; "
+                            "use Relabel::Redraw for the all-clusters extent, or the seeded extent for a forced change");
+        double gap = bond_gap(d->model, d->j);
+        if (!std::isfinite(gap) || gap < 0.0)
+            return plq_fail(PLQ_EINVAL,
+                            "the bond probability 1 - exp(-beta * gap) needs a finite, non-negative gap, got " +
+                                fmt_gap(gap) +
+                                "; an antiferromagnetic coupling is frustrated rather than merely inverted and "
+                                "needs a different construction");
+        return cluster_validate(d);
+    }
+    return plq_fail(PLQ_EINVAL, "unknown updater");
+}
+
+// ------------------------------------------------------------ chains
+static ModelParams model_params(const plq_chain_desc *d) {
+    ModelParams p;
+    std::memset(&p, 0, sizeof p);
+    p.model = d->model;
+    p.q = d->model == PLQ_POTTS ? d->q : 2;
+    p.d = d->d;
+    p.beta = d->beta;
+    p.j = d->j;
+    p.h = d->h;
+    for (int a = 0; a < PLQ_MAX_Q; ++a) p.offsets[a] = d->offsets[a];
+    return p;
+}
+
+template <class T>
+static int upload(std::vector<T> &host, T **dev, cudaStream_t s) {
+    if (host.empty()) return PLQ_OK;
+    PLQ_CUDA(cudaMalloc((void **)dev, host.size() * sizeof(T)), "cudaMalloc(table)");
+    PLQ_CUDA(cudaMemcpyAsync(*dev, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, s),
+             "cudaMemcpyAsync(table)");
+    return PLQ_OK;
+}
+
+static u128 to_u128(uint64_t lo, uint64_t hi) {
+    u128 r;
+    r.lo = lo;
+    r.hi = hi;
+    return r;
+}
+
+void chain_free(plq_chain *c) {
+    if (!c) return;
+    if (c->ctx) cudaSetDevice(c->ctx->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cluster_free(c);
+    void *ptrs[] = {c->d_state, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
+                    c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const uint8_t *start,
+                                plq_chain **out) {
+    if (!ctx || !desc || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
+    *out = nullptr;
+    int rc = plq_chain_validate(desc);
+    if (rc != PLQ_OK) return rc;
+    {
+        // State::new (src/state.rs) refuses an index >= Q; the kernels index
+        // their tables by state, so a bad start is refused here.
+        int q = desc->model == PLQ_POTTS ? desc->q : 2;
+        int64_t n = 1;
+        for (int i = 0; i < desc->d; ++i) n *= desc->shape[i];
+        int64_t n_vars = desc->model == PLQ_GAUGE ? n * desc->d : n;
+        if (start)
+            for (int64_t i = 0; i < n_vars; ++i)
+                if (start[i] >= q)
+                    return plq_fail(PLQ_EINVAL, "start variable " + std::to_string(i) + " holds state " +
+                                                    std::to_string(start[i]) + ", not below q = " +
+                                                    std::to_string(q));
+    }
+    PLQ_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+
+    plq_chain *c = new plq_chain();
+    c->ctx = ctx;
+    c->desc = *desc;
+    c->q = desc->model == PLQ_POTTS ? desc->q : 2;
+    c->d = desc->d;
+    c->link = desc->model == PLQ_GAUGE;
+    c->cluster = desc->updater == PLQ_CLUSTER;
+    c->g.d = desc->d;
+    int64_t n = 1;
+    for (int i = 0; i < kMaxD; ++i) {
+        c->g.L[i] = i < desc->d ? (int32_t)desc->shape[i] : 1;
+        c->g.stride[i] = n;
+        if (i < desc->d) n *= desc->shape[i];
+    }
+    c->g.n_sites = n;
+    c->n_sites = n;
+    c->n_vars = c->link ? n * desc->d : n;
+    c->seed32 = plq_fold_seed(desc->seed);
+
+    auto fail = [&](int code) {
+        chain_free(c);
+        return code;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
+    e = cudaMalloc((void **)&c->d_state, (size_t)c->n_vars);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(state)"));
+    e = cudaMalloc((void **)&c->d_ctrl, sizeof(Control));
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(control)"));
+    cudaMemsetAsync(c->d_ctrl, 0, sizeof(Control), c->stream);
+    e = cudaMalloc((void **)&c->d_obs, sizeof(long long) * (PLQ_MAX_Q + 2));
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(observables)"));
+
+    // start configuration
+    if (start) {
+        if (c->link) {
+            e = cudaMalloc((void **)&c->d_io, (size_t)c->n_vars);
+            if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(io)"));
+            e = cudaMemcpyAsync(c->d_io, start, (size_t)c->n_vars, cudaMemcpyHostToDevice, c->stream);
+            if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemcpyAsync(start)"));
+            e = launch_links_to_planes(c->d_io, c->d_state, n, c->d, c->stream);
+            c->launches++;
+        } else {
+            e = cudaMemcpyAsync(c->d_state, start, (size_t)c->n_vars, cudaMemcpyHostToDevice, c->stream);
+        }
+        if (e != cudaSuccess) return fail(cuda_fail(e, "upload start"));
+    } else {
+        cudaMemsetAsync(c->d_state, 0, (size_t)c->n_vars, c->stream);
+    }
+
+    // PCG stream: base state such that draw n = xsl_rr(jump(base, n))
+    if (desc->rng == PLQ_RNG_STREAM) {
+        uint64_t slo, shi, ilo, ihi;
+        pcg_seed_from_u64(desc->seed, slo, shi, ilo, ihi);
+        std::vector<AffineHost> tab;
+        build_jump_table(ilo, ihi, tab);
+        c->inc = to_u128(ilo, ihi);
+        // host-side jump to stream_offset + 1 steps
+        u128 s = to_u128(slo, shi);
+        uint64_t steps = desc->stream_offset;
+        const Affine *T = reinterpret_cast<const Affine *>(tab.data());
+        s = jump(T, s, steps);
+        s = pcg_step(s, c->inc);
+        c->base = s;
+        AffineHost *dj = nullptr;
+        int r2 = upload(tab, &dj, c->stream);
+        if (r2 != PLQ_OK) return fail(r2);
+        c->d_jump = reinterpret_cast<Affine *>(dj);
+    }
+
+    if (!c->cluster) {
+        ModelParams p = model_params(desc);
+        Tables t;
+        std::string err;
+        if (!build_tables(p, desc->updater, desc->rng, t, err)) return fail(plq_fail(PLQ_EUNSUPPORTED, err));
+        int r2 = upload(t.hb53, &c->d_hb53, c->stream);
+        if (r2 == PLQ_OK) r2 = upload(t.hb24, &c->d_hb24, c->stream);
+        if (r2 == PLQ_OK) r2 = upload(t.metro53, &c->d_metro53, c->stream);
+        if (r2 == PLQ_OK) r2 = upload(t.metro24, &c->d_metro24, c->stream);
+        if (r2 != PLQ_OK) return fail(r2);
+        // packing weights of the site environment key
+        int32_t w = 1;
+        for (int s = 0; s < 64; ++s) c->pw[s] = 0;
+        for (int s = 0; s < c->q - 1; ++s) {
+            c->pw[s] = w;
+            w *= 2 * desc->d + 1;
+        }
+        c->lookback = desc->rng == PLQ_RNG_STREAM && desc->updater == PLQ_METROPOLIS;
+        if (c->lookback) {
+            c->n_chunks = local_chunks(n);
+            e = cudaMalloc((void **)&c->d_desc, sizeof(unsigned long long) * (size_t)c->n_chunks);
+            if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(lookback)"));
+            cudaMemsetAsync(c->d_desc, 0, sizeof(unsigned long long) * (size_t)c->n_chunks, c->stream);
+        }
+    } else {
+        int r2 = cluster_create(c);
+        if (r2 != PLQ_OK) return fail(r2);
+    }
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "chain setup"));
+    *out = c;
+    return PLQ_OK;
+}
+
+static LocalArgs local_args(plq_chain *c) {
+    LocalArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.state = c->d_state;
+    a.g = c->g;
+    a.q = c->q;
+    a.kernel = c->desc.updater;
+    a.model = c->desc.model;
+    for (int s = 0; s < 64; ++s) a.pw[s] = c->pw[s];
+    a.hb53 = c->d_hb53;
+    a.hb24 = c->d_hb24;
+    a.metro53 = c->d_metro53;
+    a.metro24 = c->d_metro24;
+    a.seed32 = c->seed32;
+    a.jump = c->d_jump;
+    a.base = c->base;
+    a.inc = c->inc;
+    a.ctrl = c->d_ctrl;
+    a.desc = c->d_desc;
+    a.n_chunks = c->n_chunks;
+    return a;
+}
+
+// One sweep of local passes, in the reference's colour order
+// (updater.rs:316-343; device.rs:417-430 for the keyed sweep index).
+int local_sweep(plq_chain *c) {
+    LocalArgs a = local_args(c);
+    a.sweep32 = (uint32_t)c->sweeps_done;
+    const int64_t half = c->n_sites / 2;
+    const int passes = c->link ? 2 * c->d : 2;
+    for (int pass = 0; pass < passes; ++pass) {
+        a.dir = c->link ? pass >> 1 : 0;
+        a.color = pass & 1;
+        if (c->lookback) {
+            a.epoch = (uint32_t)(c->lookback_passes + 1);
+            a.ticket_base = c->lookback_passes * (uint64_t)c->n_chunks;
+            a.pos_in = (int)(c->lookback_passes & 1);
+            c->lookback_passes++;
+        } else if (c->desc.rng == PLQ_RNG_STREAM) {
+            a.pass_offset = c->host_pos + (uint64_t)pass * (uint64_t)half;
+        }
+        cudaError_t e = launch_local_pass(a, c->link, c->lookback, c->stream);
+        c->launches++;
+        if (e != cudaSuccess) return cuda_fail(e, "local pass launch");
+    }
+    if (c->desc.rng == PLQ_RNG_STREAM && !c->lookback) c->host_pos += (uint64_t)c->n_vars;
+    c->sweeps_done++;
+    return PLQ_OK;
+}
+
+static int run_sweeps(plq_chain *c, uint64_t sweeps) {
+    for (uint64_t t = 0; t < sweeps; ++t) {
+        int rc = c->cluster ? cluster_sweep(c) : local_sweep(c);
+        if (rc != PLQ_OK) return rc;
+    }
+    return PLQ_OK;
+}
+
+extern "C" int plq_chain_advance(plq_chain *c, uint64_t sweeps) {
+    if (!c) return plq_fail(PLQ_EINVAL, "chain is NULL");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    return run_sweeps(c, sweeps);
+}
+
+static int check_status(plq_chain *c) {
+    unsigned int st = 0;
+    PLQ_CUDA(cudaMemcpyAsync(&st, &c->d_ctrl->status, sizeof st, cudaMemcpyDeviceToHost, c->stream),
+             "status read");
+    PLQ_CUDA(cudaStreamSynchronize(c->stream), "stream sync");
+    if (st & kStatusPassCap)
+        return plq_fail(PLQ_ECAP, "cluster labeling did not converge in " + std::to_string(c->pass_cap) +
+                                      " passes on " + std::to_string(c->n_sites) +
+                                      " sites; the cap already allows many times the lattice diameter, "
+                                      "so this is a bug rather than a hard lattice");
+    if (st)
+        return plq_fail(PLQ_EDEVICE, "device status word " + std::to_string(st) +
+                                         " (1 = look-back wait limit, 4 = bounds, 8 = queue overflow)");
+    return PLQ_OK;
+}
+
+// Configuration (host order) into a device buffer.
+static int state_to_host_order(plq_chain *c, uint8_t *dst_dev) {
+    if (c->link) {
+        cudaError_t e = launch_planes_to_links(c->d_state, dst_dev, c->n_sites, c->d, c->stream);
+        c->launches++;
+        if (e != cudaSuccess) return cuda_fail(e, "planes_to_links");
+    } else {
+        PLQ_CUDA(cudaMemcpyAsync(dst_dev, c->d_state, (size_t)c->n_vars, cudaMemcpyDeviceToDevice, c->stream),
+                 "snapshot copy");
+    }
+    return PLQ_OK;
+}
+
+static int ensure_io(plq_chain *c) {
+    if (!c->d_io) PLQ_CUDA(cudaMalloc((void **)&c->d_io, (size_t)c->n_vars), "cudaMalloc(io)");
+    return PLQ_OK;
+}
+
+extern "C" int plq_chain_read(plq_chain *c, uint8_t *out) {
+    if (!c || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    if (c->link) {
+        int rc = ensure_io(c);
+        if (rc == PLQ_OK) rc = state_to_host_order(c, c->d_io);
+        if (rc != PLQ_OK) return rc;
+        PLQ_CUDA(cudaMemcpyAsync(out, c->d_io, (size_t)c->n_vars, cudaMemcpyDeviceToHost, c->stream), "read");
+    } else {
+        PLQ_CUDA(cudaMemcpyAsync(out, c->d_state, (size_t)c->n_vars, cudaMemcpyDeviceToHost, c->stream), "read");
+    }
+    return check_status(c);
+}
+
+extern "C" int plq_chain_primaries(plq_chain *c, int64_t *out, int32_t *n_out) {
+    if (!c) return plq_fail(PLQ_EINVAL, "NULL argument");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    int np = primaries_count(c->desc.model, c->q);
+    cudaError_t e = launch_primaries(c->d_state, c->g, c->desc.model, c->q, c->d_obs, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "primaries");
+    if (out)
+        PLQ_CUDA(cudaMemcpyAsync(out, c->d_obs, sizeof(long long) * np, cudaMemcpyDeviceToHost, c->stream),
+                 "primaries read");
+    if (n_out) *n_out = np;
+    return check_status(c);
+}
+
+extern "C" int plq_chain_next(plq_chain *c, uint8_t *out_states, int64_t *out_primaries) {
+    return plq_chain_next_batch(c, 1, out_states, out_primaries);
+}
+
+extern "C" int plq_chain_next_batch(plq_chain *c, int64_t count, uint8_t *out_states, int64_t *out_primaries) {
+    if (!c || count < 0) return plq_fail(PLQ_EINVAL, "bad arguments");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    const int np = primaries_count(c->desc.model, c->q);
+    // snapshot capacity: the reference clamps its staging batch by the
+    // device's buffer limit (device.rs:268-274); here by 1 GiB of snapshots.
+    int64_t cap = out_states ? std::max<int64_t>(1, (int64_t(1) << 30) / std::max<int64_t>(1, c->n_vars)) : count;
+    cap = std::min<int64_t>(cap, std::max<int64_t>(count, 1));
+    if (out_states && c->snap_cap < cap) {
+        if (c->d_snap) cudaFree(c->d_snap);
+        c->d_snap = nullptr;
+        PLQ_CUDA(cudaMalloc((void **)&c->d_snap, (size_t)(cap * c->n_vars)), "cudaMalloc(snapshots)");
+        c->snap_cap = cap;
+    }
+    if (out_primaries && c->snap_obs_cap < cap) {
+        if (c->d_snap_obs) cudaFree(c->d_snap_obs);
+        c->d_snap_obs = nullptr;
+        PLQ_CUDA(cudaMalloc((void **)&c->d_snap_obs, sizeof(long long) * (size_t)(cap * np)), "cudaMalloc(obs)");
+        c->snap_obs_cap = cap;
+    }
+    int64_t done = 0;
+    while (done < count) {
+        int64_t m = std::min<int64_t>(cap, count - done);
+        for (int64_t k = 0; k < m; ++k) {
+            int rc = run_sweeps(c, (uint64_t)c->desc.sweeps_between);
+            if (rc != PLQ_OK) return rc;
+            if (out_states) {
+                rc = state_to_host_order(c, c->d_snap + k * c->n_vars);
+                if (rc != PLQ_OK) return rc;
+            }
+            if (out_primaries) {
+                cudaError_t e = launch_primaries(c->d_state, c->g, c->desc.model, c->q,
+                                                 c->d_snap_obs + k * np, c->stream);
+                c->launches++;
+                if (e != cudaSuccess) return cuda_fail(e, "primaries");
+            }
+        }
+        if (out_states)
+            PLQ_CUDA(cudaMemcpyAsync(out_states + done * c->n_vars, c->d_snap, (size_t)(m * c->n_vars),
+                                     cudaMemcpyDeviceToHost, c->stream),
+                     "batch read-back");
+        if (out_primaries)
+            PLQ_CUDA(cudaMemcpyAsync(out_primaries + done * np, c->d_snap_obs, sizeof(long long) * (size_t)(m * np),
+                                     cudaMemcpyDeviceToHost, c->stream),
+                     "batch primaries read-back");
+        int rc = check_status(c);
+        if (rc != PLQ_OK) return rc;
+        done += m;
+    }
+    return PLQ_OK;
+}
+
+extern "C" int plq_chain_sync(plq_chain *c) {
+    if (!c) return plq_fail(PLQ_EINVAL, "chain is NULL");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    return check_status(c);
+}
+
+extern "C" int plq_chain_status(plq_chain *c) { return plq_chain_sync(c); }
+
+extern "C" uint64_t plq_chain_sweeps_done(plq_chain *c) { return c ? c->sweeps_done : 0; }
+
+extern "C" int plq_chain_stream_position(plq_chain *c, uint64_t *out) {
+    if (!c || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
+    if (c->desc.rng != PLQ_RNG_STREAM) return plq_fail(PLQ_EINVAL, "not a PCG-stream chain");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    uint64_t rel = c->host_pos;
+    if (c->lookback || c->cluster) {
+        unsigned long long pos[2];
+        PLQ_CUDA(cudaMemcpyAsync(pos, c->d_ctrl->pos, sizeof pos, cudaMemcpyDeviceToHost, c->stream), "pos read");
+        PLQ_CUDA(cudaStreamSynchronize(c->stream), "sync");
+        rel = c->cluster ? pos[c->cluster_pos_parity] : pos[c->lookback_passes & 1];
+    }
+    *out = c->desc.stream_offset + rel;
+    return PLQ_OK;
+}
+
+extern "C" int64_t plq_chain_n_vars(plq_chain *c) { return c ? c->n_vars : 0; }
+extern "C" void *plq_chain_cuda_stream(plq_chain *c) { return c ? (void *)c->stream : nullptr; }
+extern "C" uint64_t plq_chain_launches(plq_chain *c) { return c ? c->launches : 0; }
+extern "C" void plq_chain_destroy(plq_chain *c) { chain_free(c); }

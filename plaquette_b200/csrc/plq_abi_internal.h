@@ -1,0 +1,58 @@
+// plq_abi_internal.h -- the objects behind the opaque C handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/plaquette.h"
+#include "plq_device.cuh"
+
+struct plq_ctx {
+    int device = 0;
+    int sm_count = 0;
+    int cc_major = 0;
+    size_t mem_total = 0;
+};
+
+struct plq_chain {
+    plq_ctx *ctx = nullptr;
+    plq_chain_desc desc;
+    int q = 2, d = 1;
+    bool link = false, cluster = false, lookback = false;
+    int64_t n_sites = 0, n_vars = 0;
+    plq::Geom g;
+    uint32_t seed32 = 0;
+    cudaStream_t stream = nullptr;
+
+    uint8_t *d_state = nullptr;  // device layout (links as direction planes)
+    uint8_t *d_io = nullptr;     // host-order staging on the device
+    uint64_t *d_hb53 = nullptr, *d_metro53 = nullptr;
+    uint32_t *d_hb24 = nullptr, *d_metro24 = nullptr;
+    int32_t pw[64];
+    plq::Affine *d_jump = nullptr;
+    plq::u128 base{0, 0}, inc{0, 0};
+    plq::Control *d_ctrl = nullptr;
+    unsigned long long *d_desc = nullptr;
+    int64_t n_chunks = 0;
+    long long *d_obs = nullptr;
+    uint8_t *d_snap = nullptr;
+    long long *d_snap_obs = nullptr;
+    int64_t snap_cap = 0, snap_obs_cap = 0;
+    void *h_pinned = nullptr;
+
+    uint64_t sweeps_done = 0;
+    uint64_t host_pos = 0;          // deterministic stream passes: draws consumed
+    uint64_t lookback_passes = 0;   // data-dependent passes launched
+    uint64_t launches = 0;
+
+    // cluster state (plq_cluster.cu)
+    void *cl = nullptr;
+    int cluster_pos_parity = 0;
+    int64_t pass_cap = 0;
+};
+
+int plq_fail(int code, const std::string &msg);
+std::string shape_string(const plq_chain_desc *d);
+void chain_free(plq_chain *c);
+int local_sweep(plq_chain *c);

@@ -1,0 +1,28 @@
+// plq_local.h -- launchers of the local (single-variable) passes.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "plq_device.cuh"
+
+namespace plq {
+
+// Chunks (CTAs) one colour pass launches; also the look-back descriptor count.
+int64_t local_chunks(int64_t n_sites);
+// One colour pass: sites (link=false) or the links of direction a.dir.
+cudaError_t launch_local_pass(const LocalArgs &a, bool link, bool lookback, cudaStream_t stream);
+
+// Exact integer primaries of a configuration into out (int64, zeroed by the
+// launcher): Ising {bond_sum, spin_sum}, Potts {agree, counts[q]}, gauge
+// {plaquette_sum}.  Returns the number of values.
+int primaries_count(int model, int q);
+cudaError_t launch_primaries(const uint8_t *state, const Geom &g, int model, int q,
+                             long long *out, cudaStream_t stream);
+
+// Layout conversion of link variables: host order (site*d + dir) <-> device
+// planes (dir*n_sites + site).
+cudaError_t launch_links_to_planes(const uint8_t *in, uint8_t *out, int64_t n_sites, int d,
+                                   cudaStream_t stream);
+cudaError_t launch_planes_to_links(const uint8_t *in, uint8_t *out, int64_t n_sites, int d,
+                                   cudaStream_t stream);
+
+}  // namespace plq

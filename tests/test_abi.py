@@ -1,0 +1,107 @@
+"""CPU-side checks of the C-ABI library: it loads, exports every entry point
+``include/*.h`` declares, and its host logic (contract checks, hot start,
+bond probability, seed folding) agrees with the oracle.  No device calls."""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+import plaquette_b200 as plq
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(plq_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(plq.LIB_PATH)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert len(declared_symbols()) >= 20
+
+
+def test_python_binding_covers_the_header():
+    plq.lib()
+    assert set(declared_symbols()) <= set(plq.exported_symbols())
+
+
+def test_version_and_strerror():
+    assert "sm_100a" in plq.version()
+    assert plq.lib().plq_strerror(plq.PLQ_ECAP).decode().startswith("cluster labeling")
+
+
+def _desc(**kw):
+    base = dict(beta=0.44, seed=1)
+    base.update(kw)
+    model = base.pop("model", plq.ISING)
+    q = base.pop("q", 2)
+    shape = base.pop("shape", (4, 4))
+    upd = base.pop("updater", plq.METROPOLIS)
+    return plq.make_desc(model, q, shape, upd, **base)
+
+
+def test_even_extents_message_matches_reference():
+    # src/device.rs:714-719
+    with pytest.raises(plq.ContractError, match=r"the parallel site checkerboard needs even lattice extents, got \[3, 4\]"):
+        plq.validate(_desc(shape=(3, 4)))
+    with pytest.raises(plq.ContractError, match=r"the parallel link checkerboard needs even lattice extents, got \[4, 5\]"):
+        plq.validate(_desc(model=plq.GAUGE, shape=(4, 5)))
+
+
+def test_cluster_contracts_match_reference():
+    # src/updater.rs:447-483
+    with pytest.raises(plq.ContractError, match="invariant under relabeling"):
+        plq.validate(_desc(updater=plq.CLUSTER, h=0.5))
+    with pytest.raises(plq.ContractError, match="two-cycle"):
+        plq.validate(_desc(updater=plq.CLUSTER, extent=plq.EXTENT_ALL, relabel=plq.RELABEL_FORCED))
+    with pytest.raises(plq.ContractError, match="non-negative gap, got -2"):
+        plq.validate(_desc(updater=plq.CLUSTER, j=-1.0))
+    with pytest.raises(plq.ContractError, match="site field"):
+        plq.validate(_desc(model=plq.GAUGE, updater=plq.CLUSTER))
+    # odd extents are fine for a cluster chain (gpu_cluster.rs:52-53)
+    plq.validate(_desc(updater=plq.CLUSTER, shape=(5, 3)))
+
+
+def test_other_contracts():
+    with pytest.raises(plq.ContractError, match="batch size must be positive"):
+        plq.validate(_desc(batch=0))
+    with pytest.raises(plq.ContractError, match="at least two dimensions"):
+        plq.validate(_desc(model=plq.GAUGE, shape=(4,)))
+    with pytest.raises(plq.ContractError, match="at least two states"):
+        plq.validate(_desc(model=plq.POTTS, q=1))
+    with pytest.raises(plq.UnsupportedError):
+        plq.validate(_desc(model=plq.POTTS, q=3, rng=plq.RNG_STREAM))
+
+
+@pytest.mark.parametrize("seed,q,n", [(20260718, 2, 4096), (7, 3, 5000), (1, 5, 777)])
+def test_hot_start_matches_oracle(oracle, seed, q, n):
+    got, draws = plq.hot_start(seed, q, n)
+    rng = oracle.PcgStream(seed)
+    want = oracle.hot_start(n, q, rng)
+    assert np.array_equal(got, want)
+    assert draws == rng.draws
+
+
+def test_bond_probability_and_fold_seed(oracle):
+    for beta in (0.0, 0.2216544, 0.4406868, 3.0):
+        assert plq.bond_probability(plq.ISING, 1.0, beta) == oracle.Model.ising(1.0).bond_probability(beta)
+        assert plq.bond_probability(plq.POTTS, 0.7, beta) == oracle.Model.potts(3, 0.7).bond_probability(beta)
+    for s in (0, 1, 2**40 + 5, 20260718):
+        assert plq.fold_seed(s) == oracle.fold_seed(s)
+
+
+def test_no_device_here_is_none_or_context():
+    # Gpu::new() is None without a device (src/device.rs:42-44)
+    g = plq.Gpu.new()
+    if plq.device_count() == 0:
+        assert g is None

@@ -1,0 +1,190 @@
+"""Parity of the CUDA checkerboard sweeps with the oracle, bit for bit.
+
+Stream mode: configurations after N sweeps equal the reference CPU
+``LocalUpdate`` checkerboard (src/updater.rs:283-348) driven by the same
+PCG64 stream, and the chain consumed exactly as many draws.  Keyed mode:
+configurations equal the reference WGSL sweep (src/wgsl/*.wgsl) restated in
+the oracle.  Plus the reference's own GPU goldens (src/models/ising/gpu.rs:116-192).
+"""
+import numpy as np
+import pytest
+
+import plaquette_b200 as plq
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    g = plq.Gpu.new()
+    if g is None:
+        pytest.fail("no CUDA device")
+    return g
+
+
+def _models(oracle, kind, q, j, h, offsets):
+    if kind == plq.ISING:
+        return oracle.Model.ising(j, h)
+    if kind == plq.POTTS:
+        return oracle.Model.potts(q, j, offsets)
+    return oracle.Model.gauge(j)
+
+
+def run_pair(oracle, gpu, kind, q, shape, kernel, rng_mode, beta, sweeps, *, j=1.0, h=0.0, offsets=None,
+             seed=20260718, start="hot", sweeps_between=None):
+    lat = oracle.Lattice(shape, staples=kind == plq.GAUGE)
+    model = _models(oracle, kind, q, j, h, offsets)
+    n_vars = model.n_vars(lat)
+    if start == "hot":
+        cfg, offset = plq.hot_start(seed, q, n_vars)
+    else:
+        cfg, offset = np.zeros(n_vars, dtype=np.uint8), 0
+    d = plq.make_desc(kind, q, shape, kernel, beta=beta, j=j, h=h, offsets=offsets, seed=seed, rng=rng_mode,
+                      stream_offset=offset, sweeps_between=sweeps_between or sweeps, batch=1)
+    chain = plq.GpuChain(gpu, d, cfg)
+    got = next(chain)
+    want = cfg.copy()
+    if rng_mode == plq.RNG_STREAM:
+        r = oracle.PcgStream(seed)
+        r.advance(offset)
+        oracle.local_sweeps(model, lat, want, kernel, beta, r, sweeps)
+        assert chain.stream_position() == r.draws
+    else:
+        s32 = oracle.fold_seed(seed)
+        for t in range(sweeps):
+            oracle.keyed_local_sweep(model, lat, want, kernel, beta, s32, t)
+    return got, want, chain, model, lat
+
+
+CASES = [
+    # kind, q, shape, beta, extra
+    (plq.ISING, 2, (16, 16), 0.4406868, {}),
+    (plq.ISING, 2, (8, 6), 0.3, {"h": 0.25}),
+    (plq.ISING, 2, (32,), 0.7, {}),
+    (plq.ISING, 2, (4, 6, 8), 0.2216544, {}),
+    (plq.ISING, 2, (4, 4, 4, 4), 0.15, {"j": 0.75, "h": -0.1}),
+    (plq.ISING, 2, (2, 2, 2, 2, 2, 2), 0.1, {}),
+    (plq.POTTS, 2, (10, 8), 0.9, {}),
+    (plq.POTTS, 3, (12, 10), 1.0050, {}),
+    (plq.POTTS, 3, (8, 8, 6), 0.5505, {}),
+    (plq.POTTS, 3, (6, 4), 0.8, {"offsets": [0.3, -0.2, 0.1]}),
+    (plq.POTTS, 4, (6, 6, 4), 0.62, {}),
+    (plq.POTTS, 5, (8, 8), 1.1, {"j": 1.5}),
+    (plq.GAUGE, 2, (8, 8), 0.7, {}),
+    (plq.GAUGE, 2, (4, 4, 6), 0.6, {}),
+    (plq.GAUGE, 2, (4, 4, 4, 4), 0.4407, {}),
+    (plq.GAUGE, 2, (2, 4, 2), 0.9, {"j": 1.25}),
+]
+
+
+@pytest.mark.parametrize("rng_mode", [plq.RNG_STREAM, plq.RNG_KEYED], ids=["stream", "keyed"])
+@pytest.mark.parametrize("kernel", [plq.METROPOLIS, plq.HEATBATH], ids=["metropolis", "heatbath"])
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{['ising','potts','gauge'][c[0]]}{c[1]}-{'x'.join(map(str, c[2]))}")
+def test_sweeps_bit_exact(oracle, gpu, case, kernel, rng_mode):
+    kind, q, shape, beta, extra = case
+    if kind == plq.POTTS and q > 2 and kernel == plq.METROPOLIS and rng_mode == plq.RNG_STREAM:
+        pytest.skip("Potts q>=3 Metropolis runs on the keyed stream only")
+    got, want, *_ = run_pair(oracle, gpu, kind, q, shape, kernel, rng_mode, beta, 7, **extra)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("rng_mode", [plq.RNG_STREAM, plq.RNG_KEYED], ids=["stream", "keyed"])
+def test_config1_64sq_cold_critical_10k_sweeps(oracle, gpu, rng_mode):
+    """2D Ising 64x64, cold, J=1, h=0, beta_c, checkerboard Metropolis, 10^4
+    sweeps (10^3 thermalisation), E and |M| every 10 sweeps: every sample's
+    integer primaries and the final configuration bit-exact."""
+    beta, seed = 0.4406868, 20260718
+    lat = oracle.Lattice((64, 64))
+    model = oracle.Model.ising(1.0, 0.0)
+    d = plq.make_desc(plq.ISING, 2, (64, 64), plq.METROPOLIS, beta=beta, seed=seed, rng=rng_mode,
+                      sweeps_between=10, batch=64)
+    cfg = np.zeros(4096, dtype=np.uint8)
+    chain = plq.GpuChain(gpu, d, cfg)
+    chain.advance(1000)
+    states, prims = chain.next_batch(900, states=False)
+    want = cfg.copy()
+    r = oracle.PcgStream(seed)
+    s32 = oracle.fold_seed(seed)
+    sweep = 0
+
+    def sweeps(n):
+        nonlocal sweep
+        if rng_mode == plq.RNG_STREAM:
+            oracle.local_sweeps(model, lat, want, plq.METROPOLIS, beta, r, n)
+        else:
+            for _ in range(n):
+                oracle.keyed_local_sweep(model, lat, want, plq.METROPOLIS, beta, s32, sweep)
+                sweep += 1
+
+    sweeps(1000)
+    for k in range(900):
+        sweeps(10)
+        assert list(prims[k]) == list(model.primaries(lat, want)), k
+    assert np.array_equal(chain.read(), want)
+    if rng_mode == plq.RNG_STREAM:
+        assert chain.stream_position() == r.draws
+
+
+@pytest.mark.parametrize("rng_mode", [plq.RNG_STREAM, plq.RNG_KEYED])
+def test_a_launch_spanning_many_chunks_reaches_every_site(gpu, rng_mode):
+    # src/models/ising/gpu.rs:160-192: j = 0, h = -1, cold, one sweep => M = -N.
+    shape = (2048, 2048)
+    d = plq.make_desc(plq.ISING, 2, shape, plq.METROPOLIS, beta=1.0, j=0.0, h=-1.0, seed=7, rng=rng_mode,
+                      sweeps_between=1, batch=1)
+    chain = plq.GpuChain(gpu, d, np.zeros(2048 * 2048, dtype=np.uint8))
+    _, prim = chain.next_sample()
+    assert prim[1] == -(2048 * 2048)
+
+
+def test_zero_sweep_round_trip(gpu):
+    # src/models/ising/gpu.rs:116-140
+    start, _ = plq.hot_start(0, 2, 16)
+    chain = plq.ising.gpu_chain(gpu, (4, 4), 1.0, 0.0, 0.5, 7, start, 0, 1, plq.METROPOLIS)
+    assert np.array_equal(next(chain), start)
+    links = (np.arange(4 * 4 * 3 * 2) % 2).astype(np.uint8)
+    gchain = plq.gauge.gpu_chain(gpu, (4, 4, 2), 1.0, 0.5, 7, links[: 4 * 4 * 2 * 3], 0, 1, plq.HEATBATH)
+    assert np.array_equal(next(gchain), links[: 4 * 4 * 2 * 3])
+
+
+def test_odd_extent_rejected(gpu):
+    # src/models/potts/gpu.rs:427-449
+    with pytest.raises(plq.ContractError, match="even lattice extents"):
+        plq.potts.gpu_chain(gpu, (5, 4), 3, 1.0, None, 0.5, 1, np.zeros(20, np.uint8), 1, 1, plq.HEATBATH)
+
+
+def test_primaries_match_oracle(oracle, gpu):
+    for kind, q, shape in [(plq.ISING, 2, (6, 4, 2)), (plq.POTTS, 4, (8, 6)), (plq.GAUGE, 2, (4, 2, 4, 2))]:
+        got, want, chain, model, lat = run_pair(oracle, gpu, kind, q, shape, plq.HEATBATH, plq.RNG_STREAM, 0.5, 3)
+        assert np.array_equal(got, want)
+        assert list(chain.primaries()) == list(model.primaries(lat, want))
+
+
+def test_energy_matches_oracle_energy(oracle, gpu):
+    # E from the integer primaries, as Ising::energy forms it (ising/mod.rs:116)
+    got, want, chain, model, lat = run_pair(oracle, gpu, plq.ISING, 2, (12, 8), plq.METROPOLIS, plq.RNG_STREAM, 0.3,
+                                            5, j=1.5, h=0.25)
+    bond, spin = chain.primaries()
+    assert -1.5 * float(bond) - 0.25 * float(spin) == model.energy(lat, want)
+
+
+@pytest.mark.parametrize("kernel", [plq.METROPOLIS, plq.HEATBATH])
+def test_large_lattice_stream_parity(oracle, gpu, kernel):
+    got, want, *_ = run_pair(oracle, gpu, plq.ISING, 2, (256, 128, 8), kernel, plq.RNG_STREAM, 0.2216544, 3)
+    assert np.array_equal(got, want)
+
+
+def test_batch_samples_equal_sequential(oracle, gpu):
+    d = plq.make_desc(plq.POTTS, 3, (16, 16), plq.HEATBATH, beta=1.0, seed=3, rng=plq.RNG_STREAM,
+                      sweeps_between=2, batch=8)
+    start, off = plq.hot_start(3, 3, 256)
+    d.stream_offset = off
+    a = plq.GpuChain(gpu, d, start)
+    samples = [next(a) for _ in range(10)]
+    lat = oracle.Lattice((16, 16))
+    model = oracle.Model.potts(3, 1.0)
+    r = oracle.PcgStream(3)
+    r.advance(off)
+    want = start.copy()
+    for s in samples:
+        oracle.local_sweeps(model, lat, want, plq.HEATBATH, 1.0, r, 2)
+        assert np.array_equal(s, want)
