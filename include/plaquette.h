@@ -51,6 +51,9 @@ enum plq_updater { PLQ_METROPOLIS = 0, PLQ_HEATBATH = 1, PLQ_CLUSTER = 2 };
 enum plq_extent { PLQ_EXTENT_ALL = 0, PLQ_EXTENT_SEEDED = 1 };       /* updater.rs:358-373 */
 enum plq_relabel { PLQ_RELABEL_REDRAW = 0, PLQ_RELABEL_FORCED = 1 }; /* updater.rs:377-395 */
 enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
+/* Force the per-colour pass kernels even where the fused two-colour sweep
+ * applies (both give identical results; used to check one against the other). */
+#define PLQ_FLAG_NO_FUSED 1
 
 typedef struct plq_ctx plq_ctx;
 typedef struct plq_chain plq_chain;
@@ -67,7 +70,7 @@ typedef struct plq_chain_desc {
     int32_t extent;             /* enum plq_extent (PLQ_CLUSTER only) */
     int32_t relabel;            /* enum plq_relabel (PLQ_CLUSTER only) */
     int32_t rng;                /* enum plq_rng */
-    int32_t flags;              /* reserved, 0 */
+    int32_t flags;              /* PLQ_FLAG_* bits, normally 0 */
     double beta;
     double j;                   /* coupling J */
     double h;                   /* Ising field h */

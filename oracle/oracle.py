@@ -94,6 +94,7 @@ def lib():
         L.orc_rng_next_below.argtypes = [P(Rng), C.c_uint64]
         L.orc_rng_next_below.restype = C.c_uint64
         L.orc_rng_advance.argtypes = [P(Rng), C.c_uint64]
+        L.orc_hot_start.argtypes = [P(Rng), C.c_int32, C.c_int64, u8p]
         L.orc_lowbias32.argtypes = [C.c_uint32]
         L.orc_lowbias32.restype = C.c_uint32
         L.orc_keyed_uniform.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
@@ -337,7 +338,5 @@ def keyed_cluster_sweep(model: Model, lat: Lattice, cfg: np.ndarray, extent: int
 def hot_start(n_vars: int, q: int, rng: PcgStream) -> np.ndarray:
     """``Configuration::hot`` (src/configuration.rs:82-87): next_below(Q) per variable."""
     out = np.empty(n_vars, dtype=np.uint8)
-    nb = lib().orc_rng_next_below
-    for i in range(n_vars):
-        out[i] = nb(rng.ref, q)
+    lib().orc_hot_start(rng.ref, q, n_vars, _u8(out))
     return out

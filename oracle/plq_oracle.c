@@ -151,6 +151,10 @@ void orc_rng_advance(orc_rng *r, uint64_t delta) {
     r->draws += delta;
 }
 
+void orc_hot_start(orc_rng *r, int32_t q, int64_t n, uint8_t *out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = (uint8_t)orc_rng_next_below(r, (uint64_t)q);
+}
+
 /* src/wgsl/rng.wgsl:34-42 */
 uint32_t orc_lowbias32(uint32_t x) {
     uint32_t v = x;

@@ -52,6 +52,9 @@ uint32_t orc_lowbias32(uint32_t x);
 float    orc_keyed_uniform(uint32_t seed, uint32_t variable, uint32_t sweep);
 uint32_t orc_fold_seed(uint64_t seed);
 
+/* Configuration::hot (src/configuration.rs:82-87): n draws of next_below(q). */
+void     orc_hot_start(orc_rng *r, int32_t q, int64_t n, uint8_t *out);
+
 /* ------------------------------------------------------------- lattice */
 
 #define ORC_MAX_D 16

@@ -31,6 +31,7 @@ METROPOLIS, HEATBATH, CLUSTER = 0, 1, 2
 EXTENT_ALL, EXTENT_SEEDED = 0, 1
 RELABEL_REDRAW, RELABEL_FORCED = 0, 1
 RNG_STREAM, RNG_KEYED = 0, 1
+FLAG_NO_FUSED = 1
 MAX_D = 8
 MAX_Q = 64
 GPU_BATCH = 64  # src/device.rs:501
@@ -202,7 +203,7 @@ class Gpu:
 
 def make_desc(model, q, shape, updater, *, beta, j=1.0, h=0.0, offsets=None, seed=0, rng=RNG_STREAM,
               stream_offset=0, sweeps_between=1, batch=GPU_BATCH, extent=EXTENT_ALL,
-              relabel=RELABEL_REDRAW) -> ChainDesc:
+              relabel=RELABEL_REDRAW, flags=0) -> ChainDesc:
     d = ChainDesc()
     d.model = model
     d.q = q
@@ -223,6 +224,7 @@ def make_desc(model, q, shape, updater, *, beta, j=1.0, h=0.0, offsets=None, see
     d.stream_offset = stream_offset
     d.sweeps_between = sweeps_between
     d.batch = batch
+    d.flags = flags
     return d
 
 

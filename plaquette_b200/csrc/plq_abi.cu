@@ -17,6 +17,7 @@
 #include "plq_abi_internal.h"
 #include "plq_cluster.h"
 #include "plq_device.cuh"
+#include "plq_fused.h"
 #include "plq_local.h"
 #include "plq_tables.h"
 
@@ -234,7 +235,7 @@ void chain_free(plq_chain *c) {
     if (c->ctx) cudaSetDevice(c->ctx->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     cluster_free(c);
-    void *ptrs[] = {c->d_state, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
+    void *ptrs[] = {c->d_state, c->d_state_alt, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
                     c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -333,6 +334,7 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
         int r2 = upload(tab, &dj, c->stream);
         if (r2 != PLQ_OK) return fail(r2);
         c->d_jump = reinterpret_cast<Affine *>(dj);
+        c->h_jump = tab;
     }
 
     if (!c->cluster) {
@@ -348,11 +350,22 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
         // packing weights of the site environment key
         int32_t w = 1;
         for (int s = 0; s < 64; ++s) c->pw[s] = 0;
-        for (int s = 0; s < c->q - 1; ++s) {
+        for (int s = 1; s < c->q; ++s) {
             c->pw[s] = w;
             w *= 2 * desc->d + 1;
         }
         c->lookback = desc->rng == PLQ_RNG_STREAM && desc->updater == PLQ_METROPOLIS;
+        // the fused two-colour sweep where a variable's draw is a closed form
+        size_t table_bytes = desc->updater == PLQ_HEATBATH
+                                 ? (desc->rng == PLQ_RNG_STREAM ? t.hb53.size() * 8 : t.hb24.size() * 4)
+                                 : t.metro24.size() * 4;
+        if (!(desc->flags & PLQ_FLAG_NO_FUSED) && fused3d_eligible(desc->model, c->q, c->d, c->g.L, desc->updater, desc->rng) &&
+            table_bytes <= (size_t)fused3d_table_limit_bytes()) {
+            c->fused = true;
+            c->fused_tz = fused3d_default_tz(c->g.L[2]);
+            e = cudaMalloc((void **)&c->d_state_alt, (size_t)c->n_vars);
+            if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(state_alt)"));
+        }
         if (c->lookback) {
             c->n_chunks = local_chunks(n);
             e = cudaMalloc((void **)&c->d_desc, sizeof(unsigned long long) * (size_t)c->n_chunks);
@@ -392,9 +405,62 @@ static LocalArgs local_args(plq_chain *c) {
     return a;
 }
 
+static Affine to_affine(const AffineHost &h) {
+    Affine f;
+    f.m.lo = h.m_lo;
+    f.m.hi = h.m_hi;
+    f.p.lo = h.p_lo;
+    f.p.hi = h.p_hi;
+    return f;
+}
+
+// One fused two-colour sweep (out of place; the buffers swap).
+static int fused_sweep(plq_chain *c) {
+    FusedArgs f;
+    std::memset(&f, 0, sizeof f);
+    f.src = c->d_state;
+    f.dst = c->d_state_alt;
+    f.L0 = c->g.L[0];
+    f.L1 = c->g.L[1];
+    f.L2 = c->g.L[2];
+    f.tz = c->fused_tz;
+    const bool stream = c->desc.rng == PLQ_RNG_STREAM;
+    const bool hb = c->desc.updater == PLQ_HEATBATH;
+    if (hb) {
+        if (stream) {
+            f.table = c->d_hb53;
+            f.table_words = (int)(env_key_count(model_params(&c->desc)) * (c->q - 1) * 2);
+        } else {
+            f.table = c->d_hb24;
+            f.table_words = (int)(env_key_count(model_params(&c->desc)) * (c->q - 1));
+        }
+    } else {
+        f.table = c->d_metro24;
+        f.table_words = (int)env_key_count(model_params(&c->desc));
+    }
+    f.seed32 = c->seed32;
+    f.sweep32 = (uint32_t)c->sweeps_done;
+    if (stream) {
+        f.jump = c->d_jump;
+        f.base = c->base;
+        f.inc = c->inc;
+        f.off0 = c->host_pos;
+        f.off1 = c->host_pos + (uint64_t)(c->n_sites / 2);
+        f.plane = to_affine(affine_steps(c->h_jump, (uint64_t)f.L0 * (uint64_t)f.L1 / 2));
+    }
+    cudaError_t e = launch_fused3d(f, c->q, stream, hb, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "fused sweep launch");
+    std::swap(c->d_state, c->d_state_alt);
+    if (stream) c->host_pos += (uint64_t)c->n_vars;
+    c->sweeps_done++;
+    return PLQ_OK;
+}
+
 // One sweep of local passes, in the reference's colour order
 // (updater.rs:316-343; device.rs:417-430 for the keyed sweep index).
 int local_sweep(plq_chain *c) {
+    if (c->fused) return fused_sweep(c);
     LocalArgs a = local_args(c);
     a.sweep32 = (uint32_t)c->sweeps_done;
     const int64_t half = c->n_sites / 2;

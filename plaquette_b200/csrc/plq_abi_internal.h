@@ -4,9 +4,11 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/plaquette.h"
 #include "plq_device.cuh"
+#include "plq_tables.h"
 
 struct plq_ctx {
     int device = 0;
@@ -26,6 +28,10 @@ struct plq_chain {
     cudaStream_t stream = nullptr;
 
     uint8_t *d_state = nullptr;  // device layout (links as direction planes)
+    uint8_t *d_state_alt = nullptr;  // second buffer of the out-of-place fused sweep
+    bool fused = false;
+    int fused_tz = 0;
+    std::vector<plq::AffineHost> h_jump;  // host copy of the jump table
     uint8_t *d_io = nullptr;     // host-order staging on the device
     uint64_t *d_hb53 = nullptr, *d_metro53 = nullptr;
     uint32_t *d_hb24 = nullptr, *d_metro24 = nullptr;

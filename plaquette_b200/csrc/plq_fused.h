@@ -1,0 +1,28 @@
+// plq_fused.h -- the fused two-colour 3D site sweep (plq_fused.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "plq_device.cuh"
+
+namespace plq {
+
+struct FusedArgs {
+    const uint8_t *src;
+    uint8_t *dst;
+    int L0, L1, L2, tz;
+    const void *table;   // decision table in global memory (copied to smem)
+    int table_words;     // its size in 32-bit words
+    uint32_t seed32, sweep32;
+    const Affine *jump;  // PCG stream (null on the keyed stream)
+    u128 base, inc;
+    uint64_t off0, off1; // stream positions of rank 0 of colours 0 and 1
+    Affine plane;        // stream jump by one z-plane of one colour (L0*L1/2 draws)
+};
+
+bool fused3d_eligible(int model, int q, int d, const int32_t *L, int updater, int rng);
+int fused3d_default_tz(int L2);
+size_t fused3d_smem_bytes();
+int fused3d_table_limit_bytes();
+cudaError_t launch_fused3d(const FusedArgs &a, int q, bool stream, bool hb, cudaStream_t s);
+
+}  // namespace plq

@@ -32,17 +32,18 @@ int64_t potts_metro_key_count(const ModelParams &p) {
 }
 
 // Neighbour-state counts of a site environment; false if the packed index
-// names no composition of 2d neighbours.
+// names no composition of 2d neighbours.  State 0 is the implied one:
+// packed = sum over s >= 1 of c_s * (2d+1)^(s-1).
 static bool unpack_counts(const ModelParams &p, int64_t packed, int *c) {
     int64_t base = 2 * p.d + 1;
     int rest = 2 * p.d;
-    for (int s = 0; s < p.q - 1; ++s) {
+    for (int s = 1; s < p.q; ++s) {
         c[s] = (int)(packed % base);
         packed /= base;
         rest -= c[s];
     }
     if (rest < 0) return false;
-    c[p.q - 1] = rest;
+    c[0] = rest;
     return true;
 }
 
@@ -363,6 +364,20 @@ void build_jump_table(uint64_t inc_lo, uint64_t inc_hi, std::vector<AffineHost> 
         // next digit's unit = base^256 (acc is base^256 after the loop)
         base = acc;
     }
+}
+
+AffineHost affine_steps(const std::vector<AffineHost> &table, uint64_t n) {
+    AffH acc = {1, 0};
+    for (int d = 0; d < 8 && n; ++d) {
+        unsigned v = (unsigned)(n & 255u);
+        if (v) {
+            const AffineHost &e = table[(size_t)d * 256 + v];
+            AffH f = {((u128h)e.m_hi << 64) | e.m_lo, ((u128h)e.p_hi << 64) | e.p_lo};
+            acc = comp(acc, f);
+        }
+        n >>= 8;
+    }
+    return {(uint64_t)acc.m, (uint64_t)(acc.m >> 64), (uint64_t)acc.p, (uint64_t)(acc.p >> 64)};
 }
 
 }  // namespace plq

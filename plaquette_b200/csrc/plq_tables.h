@@ -33,7 +33,8 @@ struct ModelParams {
 
 // Environment keys (the device computes the same index):
 //   site models: key = cur + q * packed, packed = sum over the 2d neighbours
-//                of pw[state], pw[s] = (2d+1)^s for s < q-1 and 0 for q-1;
+//                of pw[state], pw[0] = 0 and pw[s] = (2d+1)^(s-1) for s >= 1
+//                (for q = 2 the packed value is the neighbour state sum);
 //   gauge links: key = cur + 2 * ((S + 2(d-1)) / 2), S the staple sum.
 int64_t env_key_count(const ModelParams &p);
 // Potts Metropolis key: ((cur*q + prop)*(2d+1) + c_prop)*(2d+1) + c_cur.
@@ -63,6 +64,8 @@ struct AffineHost {
     uint64_t m_lo, m_hi, p_lo, p_hi;
 };
 void build_jump_table(uint64_t inc_lo, uint64_t inc_hi, std::vector<AffineHost> &out);
+// The affine map of n LCG steps, composed from the jump table.
+AffineHost affine_steps(const std::vector<AffineHost> &table, uint64_t n);
 
 // rand_core seed_from_u64 + rand_pcg from_seed: the stream's state s_0
 // (after construction) and increment.

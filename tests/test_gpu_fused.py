@@ -1,0 +1,58 @@
+"""The fused two-colour 3D sweep: bit-exact with the oracle on small
+lattices, and identical to the per-colour pass kernels on larger ones."""
+import numpy as np
+import pytest
+
+import plaquette_b200 as plq
+from tests.test_gpu_local import run_pair
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    g = plq.Gpu.new()
+    if g is None:
+        pytest.fail("no CUDA device")
+    return g
+
+
+MODES = [
+    (plq.POTTS, 3, plq.HEATBATH, plq.RNG_STREAM),
+    (plq.POTTS, 3, plq.HEATBATH, plq.RNG_KEYED),
+    (plq.ISING, 2, plq.HEATBATH, plq.RNG_STREAM),
+    (plq.ISING, 2, plq.HEATBATH, plq.RNG_KEYED),
+    (plq.ISING, 2, plq.METROPOLIS, plq.RNG_KEYED),
+    (plq.POTTS, 2, plq.HEATBATH, plq.RNG_STREAM),
+]
+IDS = ["potts3-hb-stream", "potts3-hb-keyed", "ising-hb-stream", "ising-hb-keyed", "ising-metro-keyed",
+       "potts2-hb-stream"]
+
+
+@pytest.mark.parametrize("shape", [(128, 16, 16), (128, 32, 24), (256, 16, 8)], ids=str)
+@pytest.mark.parametrize("mode", MODES, ids=IDS)
+def test_fused_matches_oracle(oracle, gpu, shape, mode):
+    kind, q, kernel, rng = mode
+    beta = {plq.ISING: 0.2216544, plq.POTTS: 0.5505}[kind]
+    got, want, chain, model, lat = run_pair(oracle, gpu, kind, q, shape, kernel, rng, beta, 5)
+    assert np.array_equal(got, want)
+    assert list(chain.primaries()) == list(model.primaries(lat, want))
+
+
+@pytest.mark.parametrize("mode", MODES, ids=IDS)
+def test_fused_equals_pass_kernels(gpu, mode):
+    kind, q, kernel, rng = mode
+    shape = (256, 64, 64)
+    n = 256 * 64 * 64
+    start, off = plq.hot_start(99, q, n)
+    outs = []
+    for flags in (0, plq.FLAG_NO_FUSED):
+        d = plq.make_desc(kind, q, shape, kernel, beta=0.4, seed=99, rng=rng, stream_offset=off,
+                          sweeps_between=6, batch=1, flags=flags)
+        c = plq.GpuChain(gpu, d, start)
+        outs.append(next(c))
+        if rng == plq.RNG_STREAM:
+            outs.append(c.stream_position())
+    assert np.array_equal(outs[0], outs[2 if rng == plq.RNG_STREAM else 1])
+    if rng == plq.RNG_STREAM:
+        assert outs[1] == outs[3] == off + 6 * n
