@@ -142,6 +142,26 @@ void *plq_chain_cuda_stream(plq_chain *chain);
 uint64_t plq_chain_launches(plq_chain *chain);
 void plq_chain_destroy(plq_chain *chain);
 
+/* ------------------------------------------- allocation-free sweep */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a host that owns the device memory and lends this library one buffer, or
+ * a loop that must not risk cudaMalloc's implicit synchronisation): `sweeps`
+ * checkerboard Metropolis sweeps of an Ising lattice on the PCG stream, in
+ * place on `spins` -- device memory the caller owns, n_sites bytes in the
+ * reference's site order -- with exactly the results of a PLQ_ISING /
+ * PLQ_METROPOLIS / PLQ_RNG_STREAM chain.  Allocates no device memory: its
+ * scratch is a fixed 384 KiB array that every GPU loading the library holds
+ * until exit, which limits the lattice to PLQ_NOALLOC_MAX_SITES sites (larger
+ * lattices are refused with PLQ_EINVAL).  All calls share that array, so calls
+ * that overlap on the GPU race and must not be issued.  The first call on a
+ * device looks up the array's device address.  Runs on `cuda_stream` (NULL =
+ * the default stream) and returns after it drained; *stream_position_out (may
+ * be NULL) receives stream_offset plus the draws consumed. */
+#define PLQ_NOALLOC_MAX_SITES 134217728
+int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int64_t *shape, double j, double h,
+                                 double beta, uint64_t seed, uint64_t stream_offset, uint64_t sweeps,
+                                 void *cuda_stream, uint64_t *stream_position_out);
+
 #ifdef __cplusplus
 }
 #endif

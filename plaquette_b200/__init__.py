@@ -105,6 +105,9 @@ _SIGNATURES = {
     "plq_chain_cuda_stream": ([C.c_void_p], C.c_void_p),
     "plq_chain_launches": ([C.c_void_p], C.c_uint64),
     "plq_chain_destroy": ([C.c_void_p], None),
+    "plq_ising_metropolis_noalloc": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.c_double, C.c_double,
+                                      C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
+                                      C.POINTER(C.c_uint64)], C.c_int),
 }
 
 

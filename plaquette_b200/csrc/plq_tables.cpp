@@ -366,6 +366,38 @@ void build_jump_table(uint64_t inc_lo, uint64_t inc_hi, std::vector<AffineHost> 
     }
 }
 
+// Heap-free builders for callers that must not allocate: the q = 2
+// Metropolis cut points of every environment key, and the jump table, each
+// written into a caller-provided array.
+int64_t q2_metro53_into(const ModelParams &p, uint64_t *out, int64_t capacity) {
+    int64_t keys = env_key_count(p);
+    if (keys > capacity) return -1;
+    for (int64_t key = 0; key < keys; ++key) {
+        int cur;
+        double d64[2];
+        float d32[2];
+        out[key] = kAlways53;
+        if (env_deltas(p, key, cur, d64, d32)) out[key] = metro_cut64(p.beta, d64[1 - cur]);
+    }
+    return keys;
+}
+
+void jump_table_into(uint64_t inc_lo, uint64_t inc_hi, AffineHost *out) {
+    AffH base = {kMult, ((u128h)inc_hi << 64) | inc_lo};
+    for (int d = 0; d < 8; ++d) {
+        AffH acc = {1, 0};
+        for (int v = 0; v < 256; ++v) {
+            AffineHost &e = out[(size_t)d * 256 + v];
+            e.m_lo = (uint64_t)acc.m;
+            e.m_hi = (uint64_t)(acc.m >> 64);
+            e.p_lo = (uint64_t)acc.p;
+            e.p_hi = (uint64_t)(acc.p >> 64);
+            acc = comp(acc, base);
+        }
+        base = acc;
+    }
+}
+
 AffineHost affine_steps(const std::vector<AffineHost> &table, uint64_t n) {
     AffH acc = {1, 0};
     for (int d = 0; d < 8 && n; ++d) {

@@ -64,6 +64,11 @@ struct AffineHost {
     uint64_t m_lo, m_hi, p_lo, p_hi;
 };
 void build_jump_table(uint64_t inc_lo, uint64_t inc_hi, std::vector<AffineHost> &out);
+// Heap-free variants: q = 2 Metropolis cut points on the PCG stream for every
+// environment key (returns the key count, or -1 if `capacity` is too small),
+// and the jump table into `out` (kJumpDigits * kJumpRadix entries).
+int64_t q2_metro53_into(const ModelParams &p, uint64_t *out, int64_t capacity);
+void jump_table_into(uint64_t inc_lo, uint64_t inc_hi, AffineHost *out);
 // The affine map of n LCG steps, composed from the jump table.
 AffineHost affine_steps(const std::vector<AffineHost> &table, uint64_t n);
 
