@@ -138,6 +138,10 @@ int plq_chain_stream_position(plq_chain *chain, uint64_t *out);
 int64_t plq_chain_n_vars(plq_chain *chain);
 /* The chain's cudaStream_t, for callers that time or order work around it. */
 void *plq_chain_cuda_stream(plq_chain *chain);
+/* Which device path the chain's sweeps take: "fused3d" (both colours in one
+ * pass), "pass" (one launch per colour), "lookback" (stream Metropolis with
+ * the device-wide scan), "cluster". */
+const char *plq_chain_path(plq_chain *chain);
 /* Kernels this chain has launched so far. */
 uint64_t plq_chain_launches(plq_chain *chain);
 void plq_chain_destroy(plq_chain *chain);

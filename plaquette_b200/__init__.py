@@ -104,6 +104,7 @@ _SIGNATURES = {
     "plq_chain_n_vars": ([C.c_void_p], C.c_int64),
     "plq_chain_cuda_stream": ([C.c_void_p], C.c_void_p),
     "plq_chain_launches": ([C.c_void_p], C.c_uint64),
+    "plq_chain_path": ([C.c_void_p], C.c_char_p),
     "plq_chain_destroy": ([C.c_void_p], None),
     "plq_ising_metropolis_noalloc": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.c_double, C.c_double,
                                       C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
@@ -315,6 +316,10 @@ class GpuChain:
     @property
     def cuda_stream(self) -> int:
         return lib().plq_chain_cuda_stream(self._h) or 0
+
+    @property
+    def path(self) -> str:
+        return lib().plq_chain_path(self._h).decode()
 
     @property
     def launches(self) -> int:

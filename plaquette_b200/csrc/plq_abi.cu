@@ -645,4 +645,10 @@ extern "C" int plq_chain_stream_position(plq_chain *c, uint64_t *out) {
 extern "C" int64_t plq_chain_n_vars(plq_chain *c) { return c ? c->n_vars : 0; }
 extern "C" void *plq_chain_cuda_stream(plq_chain *c) { return c ? (void *)c->stream : nullptr; }
 extern "C" uint64_t plq_chain_launches(plq_chain *c) { return c ? c->launches : 0; }
+extern "C" const char *plq_chain_path(plq_chain *c) {
+    if (!c) return "";
+    if (c->cluster) return "cluster";
+    if (c->fused) return "fused3d";
+    return c->lookback ? "lookback" : "pass";
+}
 extern "C" void plq_chain_destroy(plq_chain *c) { chain_free(c); }

@@ -10,6 +10,7 @@ struct FusedArgs {
     const uint8_t *src;
     uint8_t *dst;
     int L0, L1, L2, tz;
+    int ty;              // rows per tile (set by the launcher)
     const void *table;   // decision table in global memory (copied to smem)
     int table_words;     // its size in 32-bit words
     uint32_t seed32, sweep32;
@@ -21,7 +22,7 @@ struct FusedArgs {
 
 bool fused3d_eligible(int model, int q, int d, const int32_t *L, int updater, int rng);
 int fused3d_default_tz(int L2);
-size_t fused3d_smem_bytes();
+size_t fused3d_smem_bytes(int L0);
 int fused3d_table_limit_bytes();
 cudaError_t launch_fused3d(const FusedArgs &a, int q, bool stream, bool hb, cudaStream_t s);
 

@@ -29,12 +29,13 @@ IDS = ["potts3-hb-stream", "potts3-hb-keyed", "ising-hb-stream", "ising-hb-keyed
        "potts2-hb-stream"]
 
 
-@pytest.mark.parametrize("shape", [(128, 16, 16), (128, 32, 24), (256, 16, 8)], ids=str)
+@pytest.mark.parametrize("shape", [(128, 64, 16), (256, 32, 24), (512, 16, 8), (512, 32, 16)], ids=str)
 @pytest.mark.parametrize("mode", MODES, ids=IDS)
 def test_fused_matches_oracle(oracle, gpu, shape, mode):
     kind, q, kernel, rng = mode
     beta = {plq.ISING: 0.2216544, plq.POTTS: 0.5505}[kind]
     got, want, chain, model, lat = run_pair(oracle, gpu, kind, q, shape, kernel, rng, beta, 5)
+    assert chain.path == "fused3d"
     assert np.array_equal(got, want)
     assert list(chain.primaries()) == list(model.primaries(lat, want))
 
@@ -50,6 +51,7 @@ def test_fused_equals_pass_kernels(gpu, mode):
         d = plq.make_desc(kind, q, shape, kernel, beta=0.4, seed=99, rng=rng, stream_offset=off,
                           sweeps_between=6, batch=1, flags=flags)
         c = plq.GpuChain(gpu, d, start)
+        assert c.path == ("fused3d" if flags == 0 else ("lookback" if kernel == plq.METROPOLIS and rng == plq.RNG_STREAM else "pass"))
         outs.append(next(c))
         if rng == plq.RNG_STREAM:
             outs.append(c.stream_position())
