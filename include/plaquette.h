@@ -54,6 +54,10 @@ enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
 /* Force the per-colour pass kernels even where the fused two-colour sweep
  * applies (both give identical results; used to check one against the other). */
 #define PLQ_FLAG_NO_FUSED 1
+/* Cap every cluster-labelling find and union at one step, so any real merge
+ * trips the cap: exercises the PLQ_ECAP path (gpu_cluster.rs:512-518) on the
+ * host side without any device fault. */
+#define PLQ_FLAG_TINY_PASS_CAP 2
 
 typedef struct plq_ctx plq_ctx;
 typedef struct plq_chain plq_chain;
@@ -138,6 +142,15 @@ int plq_chain_stream_position(plq_chain *chain, uint64_t *out);
 int64_t plq_chain_n_vars(plq_chain *chain);
 /* The chain's cudaStream_t, for callers that time or order work around it. */
 void *plq_chain_cuda_stream(plq_chain *chain);
+/* Cluster chains (Swendsen-Wang extent): the canonical label of every site in
+ * the most recent decomposition -- the minimum site index of its cluster, the
+ * fixed point of cluster_prelude.wgsl:113-147; ranked in site order it is
+ * site_clusters' compaction (cluster.rs:199-226).  n_sites int32 values. */
+int plq_chain_cluster_labels(plq_chain *chain, int32_t *out);
+/* Cluster sizes of the most recent decomposition as a histogram: bin k counts
+ * clusters with 2^k <= size < 2^(k+1) (the last bin takes the rest).  Wolff
+ * chains: the cluster of the most recent update. */
+int plq_chain_cluster_histogram(plq_chain *chain, int64_t *hist, int32_t nbins);
 /* Which device path the chain's sweeps take: "fused3d" (both colours in one
  * pass), "pass" (one launch per colour), "lookback" (stream Metropolis with
  * the device-wide scan), "cluster". */

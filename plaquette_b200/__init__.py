@@ -32,6 +32,7 @@ EXTENT_ALL, EXTENT_SEEDED = 0, 1
 RELABEL_REDRAW, RELABEL_FORCED = 0, 1
 RNG_STREAM, RNG_KEYED = 0, 1
 FLAG_NO_FUSED = 1
+FLAG_TINY_PASS_CAP = 2
 MAX_D = 8
 MAX_Q = 64
 GPU_BATCH = 64  # src/device.rs:501
@@ -105,6 +106,8 @@ _SIGNATURES = {
     "plq_chain_cuda_stream": ([C.c_void_p], C.c_void_p),
     "plq_chain_launches": ([C.c_void_p], C.c_uint64),
     "plq_chain_path": ([C.c_void_p], C.c_char_p),
+    "plq_chain_cluster_labels": ([C.c_void_p, C.c_void_p], C.c_int),
+    "plq_chain_cluster_histogram": ([C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
     "plq_chain_destroy": ([C.c_void_p], None),
     "plq_ising_metropolis_noalloc": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.c_double, C.c_double,
                                       C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p,
@@ -378,4 +381,16 @@ class GpuClusterChain(GpuChain):
     def __next__(self) -> np.ndarray:
         out = np.empty(self.n_vars, dtype=np.uint8)
         check(lib().plq_chain_next(self._h, out.ctypes.data, None))
+        return out
+
+    def labels(self) -> np.ndarray:
+        """Canonical (minimum-site) cluster label of every site, last decomposition."""
+        out = np.empty(self.n_vars, dtype=np.int32)
+        check(lib().plq_chain_cluster_labels(self._h, out.ctypes.data))
+        return out
+
+    def size_histogram(self, nbins: int = 32) -> np.ndarray:
+        """Clusters per size bin [2^k, 2^(k+1)) of the last decomposition (Wolff: last cluster)."""
+        out = np.zeros(nbins, dtype=np.int64)
+        check(lib().plq_chain_cluster_histogram(self._h, out.ctypes.data, nbins))
         return out

@@ -486,6 +486,7 @@ int local_sweep(plq_chain *c) {
 }
 
 static int run_sweeps(plq_chain *c, uint64_t sweeps) {
+    if (c->cluster) return sweeps ? cluster_sweep_n(c, sweeps) : PLQ_OK;
     for (uint64_t t = 0; t < sweeps; ++t) {
         int rc = c->cluster ? cluster_sweep(c) : local_sweep(c);
         if (rc != PLQ_OK) return rc;
@@ -645,6 +646,22 @@ extern "C" int plq_chain_stream_position(plq_chain *c, uint64_t *out) {
 extern "C" int64_t plq_chain_n_vars(plq_chain *c) { return c ? c->n_vars : 0; }
 extern "C" void *plq_chain_cuda_stream(plq_chain *c) { return c ? (void *)c->stream : nullptr; }
 extern "C" uint64_t plq_chain_launches(plq_chain *c) { return c ? c->launches : 0; }
+extern "C" int plq_chain_cluster_labels(plq_chain *c, int32_t *out) {
+    if (!c || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
+    if (!c->cluster) return plq_fail(PLQ_EINVAL, "not a cluster chain");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    int rc = cluster_labels(c, out);
+    return rc == PLQ_OK ? check_status(c) : rc;
+}
+
+extern "C" int plq_chain_cluster_histogram(plq_chain *c, int64_t *hist, int32_t nbins) {
+    if (!c || !hist) return plq_fail(PLQ_EINVAL, "NULL argument");
+    if (!c->cluster) return plq_fail(PLQ_EINVAL, "not a cluster chain");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    int rc = cluster_size_histogram(c, hist, nbins);
+    return rc == PLQ_OK ? check_status(c) : rc;
+}
+
 extern "C" const char *plq_chain_path(plq_chain *c) {
     if (!c) return "";
     if (c->cluster) return "cluster";

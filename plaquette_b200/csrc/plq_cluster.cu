@@ -1,8 +1,758 @@
-// plq_cluster.cu -- Swendsen-Wang and Wolff (placeholder until the labelling
-// kernels land).
-#include "plq_cluster.h"
+// plq_cluster.cu -- Swendsen-Wang and Wolff chains on the device.
+//
+// One cluster sweep of ClusterUpdate::sweep (src/updater.rs:541-613) /
+// GpuClusterChain::run_sweep (src/gpu_cluster.rs:492-526):
+//
+//  1. bonds  -- a forward bond (site, axis) opens iff the two sites agree and
+//               the draw is below p = 1 - exp(-beta * gap) (the host computes
+//               p as ClusterUpdate::bond_probability does).  Keyed stream: the
+//               draw is keyed by the bond index (cluster_prelude.wgsl:61-80).
+//               PCG stream: one draw per *agreeing* bond in site-major,
+//               axis-minor order (cluster.rs:44-62), placed by a device-wide
+//               exclusive scan (decoupled look-back) over agreeing bonds.
+//  2. labels -- lock-free union-find: every open bond unites its ends by
+//               hooking the larger root under the smaller with a CAS, then a
+//               flatten pass.  Roots only ever hook under smaller roots, so
+//               each component ends rooted at its minimum site: the canonical
+//               min-site label of the reference GPU (the fixed point of
+//               cluster_prelude.wgsl:113-147), and, ranked, the reference
+//               CPU's first-encounter compaction (cluster.rs:199-226).
+//  3. relabel -- keyed: per-root keyed draw (cluster_relabel.wgsl:39-90).
+//               PCG stream: clusters in root order draw next_below(q) (or the
+//               forced-change proposal) at consecutive positions; rand's
+//               range sampler occasionally takes a second draw, which shifts
+//               every later cluster -- those rare events are found and fixed
+//               up by re-running the (parallel) draw pass with the events
+//               known, in a short host loop.
+//
+// Wolff on the keyed stream: the reference relabels the cluster of a keyed
+// seed site in the full decomposition (cluster_relabel.wgsl:55-66).  Here a
+// frontier BFS from the seed site over lazily evaluated keyed bonds finds the
+// same component (work proportional to the cluster), its minimum site is the
+// root the forced change is keyed on.  One CTA runs all requested updates in
+// one launch.  Wolff on the PCG stream (draws in grow_cluster's FIFO order)
+// is sequential by definition and is not run on the device.
+//
+// Every loop that waits or retries has an iteration cap; hitting one sets a
+// status bit the host turns into PLQ_ECAP / PLQ_EDEVICE.
+#include <cuda_runtime.h>
 
-int cluster_validate(const plq_chain_desc *) { return PLQ_OK; }
-int cluster_create(plq_chain *) { return plq_fail(PLQ_EUNSUPPORTED, "cluster chains are not built yet"); }
-int cluster_sweep(plq_chain *) { return plq_fail(PLQ_EUNSUPPORTED, "cluster chains are not built yet"); }
-void cluster_free(plq_chain *) {}
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "../../include/plaquette.h"
+#include "plq_cluster.h"
+#include "plq_device.cuh"
+#include "plq_geom.cuh"
+#include "plq_local.h"
+#include "plq_tables.h"
+
+using namespace plq;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSitesPerThread = 8;
+constexpr int kChunk = kThreads * kSitesPerThread;
+constexpr int kSpinLimit = 1 << 22;
+constexpr int kMaxEvents = 64;
+constexpr int kBfsThreads = 1024;
+constexpr unsigned long long kDescAgg = 1ull, kDescPrefix = 2ull;
+
+struct ClusterArgs {
+    uint8_t *state;
+    uint8_t *bonds;
+    int32_t *parent;
+    uint8_t *fresh;
+    int32_t *rank;
+    uint32_t *stamp;
+    int32_t *queue;
+    Geom g;
+    int q;
+    int extent, relabel;
+    uint32_t seed32, sweep32;
+    uint32_t kp24;   // keyed: bond open iff k24 < kp24
+    uint64_t kp53;   // stream: bond open iff k53 < kp53
+    const Affine *jump;
+    u128 base, inc;
+    Control *ctrl;
+    unsigned long long *desc;
+    int64_t n_chunks;
+    uint64_t ticket_base;
+    uint32_t epoch;
+    int cap;          // iteration cap of finds and unions
+    const int32_t *events;  // sorted ranks of clusters that take two draws
+    int n_events;
+    int *first_new;   // device: smallest rank with an unknown second draw
+    uint64_t updates; // Wolff: updates in this launch
+};
+
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int32_t ld_relaxed32(const int32_t *p) {
+    int32_t v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long make_desc(uint32_t epoch, unsigned long long st, uint32_t value) {
+    return ((unsigned long long)(epoch & 0x3FFFFFFFu) << 34) | (st << 32) | value;
+}
+
+// Block-wide exclusive scan of `v` with decoupled look-back across chunks
+// (taken in ticket order).  Returns the thread's global exclusive prefix and,
+// through block_total / ok, the chunk total and whether the wait completed.
+__device__ uint64_t chunk_scan(const ClusterArgs &a, int64_t chunk, int v, int &block_total, bool &ok) {
+    __shared__ int warp_tot[kThreads / 32];
+    __shared__ unsigned long long s_excl;
+    __shared__ int s_fail;
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    if (threadIdx.x == 0) s_fail = 0;
+    __syncthreads();
+    int warp_excl = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        int t = warp_tot[w];
+        if (w < wid) warp_excl += t;
+        total += t;
+    }
+    if (threadIdx.x == 0) {
+        unsigned long long excl = 0;
+        if (chunk == 0) {
+            atomicExch(&a.desc[0], make_desc(a.epoch, kDescPrefix, (uint32_t)total));
+        } else {
+            atomicExch(&a.desc[chunk], make_desc(a.epoch, kDescAgg, (uint32_t)total));
+            int64_t j = chunk - 1;
+            int spins = 0;
+            while (j >= 0) {
+                unsigned long long d = ld_relaxed(&a.desc[j]);
+                uint32_t ep = (uint32_t)(d >> 34);
+                unsigned long long st = (d >> 32) & 3ull;
+                if (ep != (a.epoch & 0x3FFFFFFFu) || st == 0) {
+                    if (++spins > kSpinLimit) {
+                        s_fail = 1;
+                        atomicOr(&a.ctrl->status, kStatusLookbackTimeout);
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                excl += (uint32_t)d;
+                if (st == kDescPrefix) break;
+                --j;
+            }
+            if (!s_fail) atomicExch(&a.desc[chunk], make_desc(a.epoch, kDescPrefix, (uint32_t)(excl + total)));
+        }
+        s_excl = excl;
+    }
+    __syncthreads();
+    ok = s_fail == 0;
+    block_total = total;
+    return s_excl + (uint64_t)(warp_excl + incl - v);
+}
+
+__device__ __forceinline__ int64_t take_chunk(const ClusterArgs &a, bool lookback) {
+    if (!lookback) return blockIdx.x;
+    __shared__ unsigned long long s_ticket;
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&a.ctrl->ticket, 1ull) - a.ticket_base;
+    __syncthreads();
+    return (int64_t)s_ticket;
+}
+
+// ------------------------------------------------------------- 1. bonds
+template <int D, bool STREAM>
+__global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
+    const int64_t n = a.g.n_sites;
+    const int64_t chunk = take_chunk(a, STREAM);
+    if (chunk >= a.n_chunks) {
+        if (threadIdx.x == 0) atomicOr(&a.ctrl->status, kStatusBounds);
+        return;
+    }
+    const int64_t s0 = chunk * kChunk + (int64_t)threadIdx.x * kSitesPerThread;
+    uint8_t agree[kSitesPerThread];
+    int count = 0;
+#pragma unroll
+    for (int i = 0; i < kSitesPerThread; ++i) {
+        int64_t s = s0 + i;
+        agree[i] = 0;
+        if (s >= n) continue;
+        int32_t x[D];
+        site_coords<D>(a.g, s, x);
+        uint8_t cur = a.state[s];
+        uint8_t m = 0;
+#pragma unroll
+        for (int mu = 0; mu < D; ++mu)
+            if (a.state[nbr_plus(a.g, s, x, mu)] == cur) m |= (uint8_t)(1u << mu);
+        agree[i] = m;
+        count += __popc(m);
+        a.parent[s] = (int32_t)s;  // label init (cluster_prelude.wgsl:83-93)
+    }
+    u128 st{0, 0};
+    if (STREAM) {
+        int total;
+        bool ok;
+        uint64_t excl = chunk_scan(a, chunk, count, total, ok);
+        if (!ok) return;
+        __shared__ unsigned long long s_base;
+        if (threadIdx.x == 0) {
+            s_base = a.ctrl->pos[0];
+            if (chunk == a.n_chunks - 1) a.ctrl->pos[1] = s_base + excl + (unsigned long long)total;
+        }
+        __syncthreads();
+        if (count) st = jump(a.jump, a.base, s_base + excl);
+    }
+#pragma unroll
+    for (int i = 0; i < kSitesPerThread; ++i) {
+        int64_t s = s0 + i;
+        if (s >= n) continue;
+        uint8_t open = 0;
+#pragma unroll
+        for (int mu = 0; mu < D; ++mu) {
+            if (!((agree[i] >> mu) & 1u)) continue;
+            bool drawn;
+            if (STREAM) {
+                uint64_t k = draw53(st);
+                st = pcg_step(st, a.inc);
+                drawn = k < a.kp53;
+            } else {
+                drawn = keyed24(a.seed32 ^ kBondKey, (uint32_t)(s * D + mu), a.sweep32) < a.kp24;
+            }
+            if (drawn) open |= (uint8_t)(1u << mu);
+        }
+        a.bonds[s] = open;
+    }
+}
+
+// ------------------------------------------------------------ 2. labels
+__device__ __forceinline__ int32_t find_root(int32_t *parent, int32_t x, int cap, Control *ctrl) {
+    int32_t p = ld_relaxed32(&parent[x]);
+    int it = 0;
+    while (p != x) {
+        int32_t gp = ld_relaxed32(&parent[p]);
+        if (gp != p) parent[x] = gp;  // path halving: gp is an ancestor, never a wrong set
+        x = p;
+        p = gp;
+        if (++it > cap) {
+            atomicOr(&ctrl->status, kStatusPassCap);
+            break;
+        }
+    }
+    return x;
+}
+
+__device__ __forceinline__ void unite(int32_t *parent, int32_t a, int32_t b, int cap, Control *ctrl) {
+    for (int it = 0;; ++it) {
+        a = find_root(parent, a, cap, ctrl);
+        b = find_root(parent, b, cap, ctrl);
+        if (a == b) return;
+        if (a > b) {
+            int32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(&parent[b], b, a) == b) return;  // b was still a root: hooked under a
+        if (it > cap) {
+            atomicOr(&ctrl->status, kStatusPassCap);
+            return;
+        }
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreads) hook_kernel(ClusterArgs a) {
+    const int64_t n = a.g.n_sites;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        uint8_t b = a.bonds[s];
+        if (!b) continue;
+        int32_t x[D];
+        site_coords<D>(a.g, s, x);
+#pragma unroll
+        for (int mu = 0; mu < D; ++mu)
+            if ((b >> mu) & 1u) unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, mu), a.cap, a.ctrl);
+    }
+}
+
+// Read-only find for the flatten pass: a compressing find could overwrite a
+// site another thread has just flattened with a non-root ancestor.
+__device__ __forceinline__ int32_t find_root_ro(const int32_t *parent, int32_t x, int cap, Control *ctrl) {
+    int32_t p = ld_relaxed32(&parent[x]);
+    int it = 0;
+    while (p != x) {
+        x = p;
+        p = ld_relaxed32(&parent[x]);
+        if (++it > cap) {
+            atomicOr(&ctrl->status, kStatusPassCap);
+            break;
+        }
+    }
+    return x;
+}
+
+__global__ void flatten_kernel(ClusterArgs a) {
+    const int64_t n = a.g.n_sites;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+        a.parent[s] = find_root_ro(a.parent, (int32_t)s, a.cap, a.ctrl);
+}
+
+// ----------------------------------------------------------- 3. relabel
+// keyed (cluster_relabel.wgsl:72-89), every cluster
+__global__ void relabel_keyed_kernel(ClusterArgs a) {
+    const int64_t n = a.g.n_sites;
+    const uint32_t q = (uint32_t)a.q;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t root = (uint32_t)a.parent[s];
+        float u = __fmul_rn((float)keyed24(a.seed32 ^ kRootSalt, root, a.sweep32), 5.9604644775390625e-8f);
+        if (a.relabel == PLQ_RELABEL_FORCED) {
+            uint32_t step = __float2uint_rz(__fmul_rn(u, (float)(q - 1u)));
+            if (step >= q - 1u) step = q - 2u;
+            a.state[s] = (uint8_t)((a.state[s] + 1u + step) % q);
+        } else {
+            uint32_t draw = __float2uint_rz(__fmul_rn(u, (float)q));
+            if (draw >= q) draw = q - 1u;
+            a.state[s] = (uint8_t)draw;
+        }
+    }
+}
+
+// stream: rank of each root among roots (first-encounter order)
+template <int D>
+__global__ void __launch_bounds__(kThreads) root_rank_kernel(ClusterArgs a) {
+    const int64_t n = a.g.n_sites;
+    const int64_t chunk = take_chunk(a, true);
+    if (chunk >= a.n_chunks) {
+        if (threadIdx.x == 0) atomicOr(&a.ctrl->status, kStatusBounds);
+        return;
+    }
+    const int64_t s0 = chunk * kChunk + (int64_t)threadIdx.x * kSitesPerThread;
+    int count = 0;
+    uint32_t mask = 0;
+#pragma unroll
+    for (int i = 0; i < kSitesPerThread; ++i) {
+        int64_t s = s0 + i;
+        if (s < n && a.parent[s] == (int32_t)s) {
+            mask |= 1u << i;
+            ++count;
+        }
+    }
+    int total;
+    bool ok;
+    uint64_t excl = chunk_scan(a, chunk, count, total, ok);
+    if (!ok) return;
+    if (threadIdx.x == 0 && chunk == a.n_chunks - 1) a.ctrl->scratch[0] = excl + (unsigned long long)total;
+    int r = (int)excl;
+#pragma unroll
+    for (int i = 0; i < kSitesPerThread; ++i)
+        if ((mask >> i) & 1u) a.rank[s0 + i] = r++;
+}
+
+// rand 0.10 random_range(0..range) for range < 2^32 at stream position pos:
+// returns the value and whether a second draw was taken.
+__device__ __forceinline__ uint32_t next_below_at(const ClusterArgs &a, uint64_t pos, uint32_t range, bool &second) {
+    u128 st = jump(a.jump, a.base, pos);
+    uint32_t x = (uint32_t)xsl_rr(st);
+    uint64_t m = (uint64_t)x * range;
+    uint32_t result = (uint32_t)(m >> 32), lo = (uint32_t)m;
+    second = lo > (uint32_t)(0u - range);
+    if (second) {
+        st = pcg_step(st, a.inc);
+        uint32_t x2 = (uint32_t)xsl_rr(st);
+        uint32_t hi2 = (uint32_t)(((uint64_t)x2 * range) >> 32);
+        if ((uint64_t)lo + hi2 > 0xFFFFFFFFull) result += 1;
+    }
+    return result;
+}
+
+// stream: each root draws its cluster's fresh label (ClusterUpdate::fresh_label,
+// updater.rs:507-521) at bond_end + rank + (known second draws before it).
+__global__ void root_draw_kernel(ClusterArgs a) {
+    const int64_t n = a.g.n_sites;
+    const uint64_t bond_end = a.ctrl->pos[1];
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        if (a.parent[s] != (int32_t)s) continue;
+        int32_t r = a.rank[s];
+        int before = 0;
+        bool known = false;
+        for (int e = 0; e < a.n_events; ++e) {
+            before += a.events[e] < r;
+            known |= a.events[e] == r;
+        }
+        uint64_t pos = bond_end + (uint64_t)r + (uint64_t)before;
+        uint32_t cur = a.state[s];
+        uint32_t label;
+        bool second;
+        if (a.relabel == PLQ_RELABEL_REDRAW) {
+            label = next_below_at(a, pos, (uint32_t)a.q, second);
+        } else {  // propose (updater.rs:659-668); q >= 3 here
+            uint32_t d = next_below_at(a, pos, (uint32_t)(a.q - 1), second);
+            label = d + (d >= cur ? 1u : 0u);
+        }
+        a.fresh[s] = (uint8_t)label;
+        if (second && !known) atomicMin(a.first_new, r);
+    }
+}
+
+__global__ void apply_fresh_kernel(ClusterArgs a) {
+    const int64_t n = a.g.n_sites;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+        a.state[s] = a.fresh[a.parent[s]];
+}
+
+__global__ void finish_pos_kernel(Control *ctrl, int n_events) {
+    ctrl->pos[0] = ctrl->pos[1] + ctrl->scratch[0] + (unsigned long long)n_events;
+}
+
+// ------------------------------------------------------- Wolff (keyed BFS)
+template <int D>
+__global__ void __launch_bounds__(kBfsThreads) wolff_bfs_kernel(ClusterArgs a) {
+    __shared__ int s_tail, s_min;
+    __shared__ int s_lvl_begin, s_lvl_end;
+    const int64_t n = a.g.n_sites;
+    const uint32_t q = (uint32_t)a.q;
+    for (uint64_t up = 0; up < a.updates; ++up) {
+        const uint32_t sweep = a.sweep32 + (uint32_t)up;
+        const uint32_t epoch = sweep + 1u;
+        // seed site (cluster_relabel.wgsl:55-61)
+        float us = __fmul_rn((float)keyed24(a.seed32 ^ kSeedSalt, 0u, sweep), 5.9604644775390625e-8f);
+        uint32_t seed_site = __float2uint_rz(__fmul_rn(us, (float)(uint32_t)n));
+        if (seed_site >= (uint32_t)n) seed_site = (uint32_t)n - 1u;
+        if (threadIdx.x == 0) {
+            a.queue[0] = (int32_t)seed_site;
+            a.stamp[seed_site] = epoch;
+            s_tail = 1;
+            s_min = (int32_t)seed_site;
+            s_lvl_begin = 0;
+            s_lvl_end = 1;
+        }
+        __syncthreads();
+        const uint8_t cur = a.state[seed_site];
+        while (true) {
+            int begin = s_lvl_begin, end = s_lvl_end;
+            if (begin >= end) break;
+            for (int i = begin + threadIdx.x; i < end; i += blockDim.x) {
+                int64_t u = a.queue[i];
+                int32_t x[D];
+                site_coords<D>(a.g, u, x);
+#pragma unroll
+                for (int mu = 0; mu < D; ++mu) {
+#pragma unroll
+                    for (int sgn = 0; sgn < 2; ++sgn) {
+                        int64_t v = sgn == 0 ? nbr_plus(a.g, u, x, mu) : nbr_minus(a.g, u, x, mu);
+                        if (a.state[v] != cur) continue;
+                        uint32_t bond = (uint32_t)((sgn == 0 ? u : v) * D + mu);
+                        if (keyed24(a.seed32 ^ kBondKey, bond, sweep) >= a.kp24) continue;
+                        if (atomicExch(&a.stamp[v], epoch) == epoch) continue;  // already a member
+                        int slot = atomicAdd(&s_tail, 1);
+                        a.queue[slot] = (int32_t)v;
+                        atomicMin(&s_min, (int32_t)v);
+                    }
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_lvl_begin = end;
+                s_lvl_end = s_tail;
+            }
+            __syncthreads();
+        }
+        const int members = s_tail;
+        const uint32_t root = (uint32_t)s_min;
+        float u = __fmul_rn((float)keyed24(a.seed32 ^ kRootSalt, root, sweep), 5.9604644775390625e-8f);
+        uint8_t next;
+        if (a.relabel == PLQ_RELABEL_FORCED) {
+            uint32_t step = __float2uint_rz(__fmul_rn(u, (float)(q - 1u)));
+            if (step >= q - 1u) step = q - 2u;
+            next = (uint8_t)((cur + 1u + step) % q);
+        } else {
+            uint32_t draw = __float2uint_rz(__fmul_rn(u, (float)q));
+            if (draw >= q) draw = q - 1u;
+            next = (uint8_t)draw;
+        }
+        for (int i = threadIdx.x; i < members; i += blockDim.x) a.state[a.queue[i]] = next;
+        if (threadIdx.x == 0) a.ctrl->scratch[1] = (unsigned long long)members;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ sizes
+__global__ void sizes_kernel(const int32_t *parent, int32_t *size, int64_t n) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&size[parent[s]], 1);
+}
+__global__ void size_hist_kernel(const int32_t *parent, const int32_t *size, int64_t n, long long *hist, int nbins) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        if (parent[s] != (int32_t)s) continue;
+        int bin = 31 - __clz(size[s]);
+        if (bin >= nbins) bin = nbins - 1;
+        atomicAdd((unsigned long long *)&hist[bin], 1ull);
+    }
+}
+
+// ------------------------------------------------------------ host side
+struct ClusterDev {
+    uint8_t *bonds = nullptr;
+    int32_t *parent = nullptr;
+    uint8_t *fresh = nullptr;
+    int32_t *rank = nullptr;
+    uint32_t *stamp = nullptr;
+    int32_t *queue = nullptr;
+    unsigned long long *desc = nullptr;
+    int64_t n_chunks = 0;
+    int32_t *events = nullptr;
+    int *first_new = nullptr;
+    int32_t *sizes = nullptr;
+    uint32_t kp24 = 0;
+    uint64_t kp53 = 0;
+    uint64_t lookback_launches = 0;
+    std::vector<int32_t> host_events;
+    bool decomposed = false;
+};
+
+unsigned grid_stride_blocks(int64_t n) {
+    int64_t b = (n + kThreads - 1) / kThreads;
+    if (b > 148 * 16) b = 148 * 16;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+ClusterArgs cluster_args(plq_chain *c) {
+    ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
+    ClusterArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.state = c->d_state;
+    a.bonds = cd->bonds;
+    a.parent = cd->parent;
+    a.fresh = cd->fresh;
+    a.rank = cd->rank;
+    a.stamp = cd->stamp;
+    a.queue = cd->queue;
+    a.g = c->g;
+    a.q = c->q;
+    a.extent = c->desc.extent;
+    a.relabel = c->desc.relabel;
+    a.seed32 = c->seed32;
+    a.sweep32 = (uint32_t)c->sweeps_done;
+    a.kp24 = cd->kp24;
+    a.kp53 = cd->kp53;
+    a.jump = c->d_jump;
+    a.base = c->base;
+    a.inc = c->inc;
+    a.ctrl = c->d_ctrl;
+    a.desc = cd->desc;
+    a.n_chunks = cd->n_chunks;
+    a.cap = (c->desc.flags & PLQ_FLAG_TINY_PASS_CAP) ? 1 : (int)std::min<int64_t>(c->n_sites + 64, 1 << 30);
+    a.events = cd->events;
+    a.first_new = cd->first_new;
+    return a;
+}
+
+template <int D>
+int sweep_d(plq_chain *c, uint64_t sweeps) {
+    ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
+    const bool stream = c->desc.rng == PLQ_RNG_STREAM;
+    const int64_t n = c->n_sites;
+    const unsigned gs = grid_stride_blocks(n);
+    if (c->desc.extent == PLQ_EXTENT_SEEDED) {
+        ClusterArgs a = cluster_args(c);
+        a.updates = sweeps;
+        wolff_bfs_kernel<D><<<1, kBfsThreads, 0, c->stream>>>(a);
+        c->launches++;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, std::string("wolff launch: ") + cudaGetErrorString(e));
+        c->sweeps_done += sweeps;
+        cd->decomposed = false;
+        return PLQ_OK;
+    }
+    for (uint64_t t = 0; t < sweeps; ++t) {
+        ClusterArgs a = cluster_args(c);
+        auto lookback = [&](ClusterArgs &x) {
+            x.epoch = (uint32_t)(cd->lookback_launches + 1);
+            x.ticket_base = cd->lookback_launches * (uint64_t)cd->n_chunks;
+            cd->lookback_launches++;
+        };
+        if (stream) {
+            lookback(a);
+            bonds_kernel<D, true><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
+        } else {
+            bonds_kernel<D, false><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
+        }
+        hook_kernel<D><<<gs, kThreads, 0, c->stream>>>(a);
+        flatten_kernel<<<gs, kThreads, 0, c->stream>>>(a);
+        c->launches += 3;
+        if (!stream) {
+            relabel_keyed_kernel<<<gs, kThreads, 0, c->stream>>>(a);
+            c->launches++;
+        } else {
+            lookback(a);
+            root_rank_kernel<D><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
+            c->launches++;
+            cd->host_events.clear();
+            for (int round = 0;; ++round) {
+                a.n_events = (int)cd->host_events.size();
+                int none = 0x7FFFFFFF;
+                cudaMemcpyAsync(cd->first_new, &none, sizeof none, cudaMemcpyHostToDevice, c->stream);
+                if (a.n_events)
+                    cudaMemcpyAsync(cd->events, cd->host_events.data(), sizeof(int32_t) * a.n_events,
+                                    cudaMemcpyHostToDevice, c->stream);
+                root_draw_kernel<<<gs, kThreads, 0, c->stream>>>(a);
+                c->launches++;
+                int first = none;
+                cudaMemcpyAsync(&first, cd->first_new, sizeof first, cudaMemcpyDeviceToHost, c->stream);
+                cudaError_t e = cudaStreamSynchronize(c->stream);
+                if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, std::string("root draws: ") + cudaGetErrorString(e));
+                if (first == none) break;
+                if ((int)cd->host_events.size() >= kMaxEvents)
+                    return plq_fail(PLQ_EDEVICE, "too many two-draw label events in one sweep");
+                cd->host_events.insert(std::upper_bound(cd->host_events.begin(), cd->host_events.end(), first), first);
+            }
+            apply_fresh_kernel<<<gs, kThreads, 0, c->stream>>>(a);
+            finish_pos_kernel<<<1, 1, 0, c->stream>>>(c->d_ctrl, (int)cd->host_events.size());
+            c->launches += 2;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, std::string("cluster sweep: ") + cudaGetErrorString(e));
+        c->sweeps_done++;
+        cd->decomposed = true;
+    }
+    return PLQ_OK;
+}
+
+}  // namespace
+
+int cluster_validate(const plq_chain_desc *d) {
+    if (d->extent == PLQ_EXTENT_SEEDED && d->rng == PLQ_RNG_STREAM)
+        return plq_fail(PLQ_EUNSUPPORTED,
+                        "Wolff on the PCG stream draws in grow_cluster's sequential FIFO order; this device path "
+                        "runs the seeded extent on the keyed stream only");
+    return PLQ_OK;
+}
+
+int cluster_create(plq_chain *c) {
+    ClusterDev *cd = new ClusterDev();
+    c->cl = cd;
+    const int64_t n = c->n_sites;
+    double p = plq_bond_probability(c->desc.model, c->desc.j, c->desc.beta);
+    // bond open iff u < p: keyed in f32 (cluster_prelude.wgsl:77), stream in f64 (updater.rs:570-572)
+    float p32 = (float)p;
+    uint32_t lo = 0, hi = 1u << 24;
+    while (lo < hi) {
+        uint32_t mid = lo + (hi - lo) / 2;
+        if ((float)mid * (1.0f / 16777216.0f) < p32) lo = mid + 1;
+        else hi = mid;
+    }
+    cd->kp24 = lo;
+    uint64_t lo53 = 0, hi53 = 1ull << 53;
+    while (lo53 < hi53) {
+        uint64_t mid = lo53 + (hi53 - lo53) / 2;
+        if ((double)mid * (1.0 / 9007199254740992.0) < p) lo53 = mid + 1;
+        else hi53 = mid;
+    }
+    cd->kp53 = lo53;
+    c->pass_cap = (c->desc.flags & PLQ_FLAG_TINY_PASS_CAP) ? 1 : std::min<int64_t>(n + 64, 1 << 30);
+    cd->n_chunks = (n + kChunk - 1) / kChunk;
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    if (c->desc.extent == PLQ_EXTENT_SEEDED) {
+        alloc((void **)&cd->stamp, sizeof(uint32_t) * (size_t)n);
+        alloc((void **)&cd->queue, sizeof(int32_t) * (size_t)n);
+        if (e == cudaSuccess) e = cudaMemsetAsync(cd->stamp, 0, sizeof(uint32_t) * (size_t)n, c->stream);
+    } else {
+        alloc((void **)&cd->bonds, (size_t)n);
+        alloc((void **)&cd->parent, sizeof(int32_t) * (size_t)n);
+        alloc((void **)&cd->desc, sizeof(unsigned long long) * (size_t)cd->n_chunks);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(cd->desc, 0, sizeof(unsigned long long) * (size_t)cd->n_chunks, c->stream);
+        if (c->desc.rng == PLQ_RNG_STREAM) {
+            alloc((void **)&cd->fresh, (size_t)n);
+            alloc((void **)&cd->rank, sizeof(int32_t) * (size_t)n);
+            alloc((void **)&cd->events, sizeof(int32_t) * kMaxEvents);
+            alloc((void **)&cd->first_new, sizeof(int));
+        }
+    }
+    if (e != cudaSuccess)
+        return plq_fail(e == cudaErrorMemoryAllocation ? PLQ_ENOMEM : PLQ_ECUDA,
+                        std::string("cluster buffers: ") + cudaGetErrorString(e));
+    return PLQ_OK;
+}
+
+int cluster_sweep_n(plq_chain *c, uint64_t sweeps) {
+    switch (c->d) {
+        case 1: return sweep_d<1>(c, sweeps);
+        case 2: return sweep_d<2>(c, sweeps);
+        case 3: return sweep_d<3>(c, sweeps);
+        case 4: return sweep_d<4>(c, sweeps);
+        case 5: return sweep_d<5>(c, sweeps);
+        case 6: return sweep_d<6>(c, sweeps);
+        case 7: return sweep_d<7>(c, sweeps);
+        case 8: return sweep_d<8>(c, sweeps);
+        default: return plq_fail(PLQ_EINVAL, "dimension out of range");
+    }
+}
+
+int cluster_sweep(plq_chain *c) { return cluster_sweep_n(c, 1); }
+
+void cluster_free(plq_chain *c) {
+    ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
+    if (!cd) return;
+    void *ptrs[] = {cd->bonds, cd->parent, cd->fresh, cd->rank, cd->stamp, cd->queue,
+                    cd->desc, cd->events, cd->first_new, cd->sizes};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    delete cd;
+    c->cl = nullptr;
+}
+
+int cluster_labels(plq_chain *c, int32_t *out) {
+    ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
+    if (!cd || !cd->decomposed) return plq_fail(PLQ_EINVAL, "no decomposition yet (run a Swendsen-Wang sweep first)");
+    cudaError_t e = cudaMemcpyAsync(out, cd->parent, sizeof(int32_t) * (size_t)c->n_sites, cudaMemcpyDeviceToHost,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, std::string("labels read: ") + cudaGetErrorString(e));
+    return PLQ_OK;
+}
+
+int cluster_size_histogram(plq_chain *c, int64_t *hist, int32_t nbins) {
+    ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
+    if (!cd || nbins <= 0) return plq_fail(PLQ_EINVAL, "bad arguments");
+    std::vector<long long> h((size_t)nbins, 0);
+    if (c->desc.extent == PLQ_EXTENT_SEEDED) {
+        unsigned long long members = 0;
+        cudaMemcpyAsync(&members, &c->d_ctrl->scratch[1], sizeof members, cudaMemcpyDeviceToHost, c->stream);
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, cudaGetErrorString(e));
+        if (members) {
+            int bin = 63 - __builtin_clzll(members);
+            h[(size_t)std::min(bin, nbins - 1)] = 1;
+        }
+    } else {
+        if (!cd->decomposed) return plq_fail(PLQ_EINVAL, "no decomposition yet (run a Swendsen-Wang sweep first)");
+        const int64_t n = c->n_sites;
+        cudaError_t e = cudaSuccess;
+        if (!cd->sizes) e = cudaMalloc((void **)&cd->sizes, sizeof(int32_t) * (size_t)n);
+        long long *dh = nullptr;
+        if (e == cudaSuccess) e = cudaMalloc((void **)&dh, sizeof(long long) * (size_t)nbins);
+        if (e != cudaSuccess) return plq_fail(PLQ_ENOMEM, cudaGetErrorString(e));
+        cudaMemsetAsync(cd->sizes, 0, sizeof(int32_t) * (size_t)n, c->stream);
+        cudaMemsetAsync(dh, 0, sizeof(long long) * (size_t)nbins, c->stream);
+        sizes_kernel<<<grid_stride_blocks(n), kThreads, 0, c->stream>>>(cd->parent, cd->sizes, n);
+        size_hist_kernel<<<grid_stride_blocks(n), kThreads, 0, c->stream>>>(cd->parent, cd->sizes, n, dh, nbins);
+        c->launches += 2;
+        cudaMemcpyAsync(h.data(), dh, sizeof(long long) * (size_t)nbins, cudaMemcpyDeviceToHost, c->stream);
+        e = cudaStreamSynchronize(c->stream);
+        cudaFree(dh);
+        if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, cudaGetErrorString(e));
+    }
+    for (int i = 0; i < nbins; ++i) hist[i] = h[(size_t)i];
+    return PLQ_OK;
+}
