@@ -159,6 +159,43 @@ const char *plq_chain_path(plq_chain *chain);
 uint64_t plq_chain_launches(plq_chain *chain);
 void plq_chain_destroy(plq_chain *chain);
 
+/* -------------------------------------------------------- ensembles */
+/* No counterpart in the reference (which runs one chain per GpuChain): many
+ * chains -- any mix of models, dimensions <= 4, uneven shapes, betas and
+ * seeds, local updaters on the keyed stream or heat bath on the PCG stream --
+ * advanced together.  Member m evolves exactly as plq_chain_create(desc[m],
+ * starts[m]) would; starts may be NULL (all members cold) or hold NULLs. */
+typedef struct plq_ensemble plq_ensemble;
+int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc *members, const uint8_t *const *starts,
+                        plq_ensemble **out);
+/* Parallel tempering over k members of identical model, shape and updater
+ * (no field, no offsets): slot i runs at betas[i] (member member_ids[i]
+ * starts there); every `every` sweeps adjacent slots attempt swaps (even
+ * pairs, then odd pairs) with min(1, exp((b_i - b_i+1)(E_i - E_i+1))). */
+int plq_ensemble_add_ladder(plq_ensemble *e, int32_t k, const int32_t *member_ids, const double *betas,
+                            int32_t every, uint64_t seed);
+/* `sweeps` sweeps of every member (and the swaps they reach) in one
+ * persistent cooperative launch, captured once into a CUDA graph and replayed. */
+int plq_ensemble_advance(plq_ensemble *e, uint64_t sweeps);
+/* The same sweeps with one launch per member per colour pass (the
+ * per-lattice baseline); identical results. */
+int plq_ensemble_advance_unbatched(plq_ensemble *e, uint64_t sweeps);
+/* Work-item shape of the persistent launch: ranks per thread (2, 4, 8) and
+ * CTAs per SM; the autotuner times the candidates on a snapshot of the
+ * ensemble (restored afterwards) and keeps the fastest. */
+int plq_ensemble_set_config(plq_ensemble *e, int32_t ranks_per_thread, int32_t ctas_per_sm);
+int plq_ensemble_tune(plq_ensemble *e, int32_t trial_sweeps, int32_t *ranks_out, int32_t *ctas_out,
+                      double *ms_per_sweep_out);
+int plq_ensemble_sync(plq_ensemble *e);
+int plq_ensemble_read(plq_ensemble *e, int32_t member, uint8_t *out_states);
+int plq_ensemble_primaries(plq_ensemble *e, int32_t member, int64_t *out, int32_t *n_out);
+/* Current beta of every member (parallel tempering moves them). */
+int plq_ensemble_betas(plq_ensemble *e, double *beta_of_member);
+int64_t plq_ensemble_n_vars(plq_ensemble *e);
+void *plq_ensemble_cuda_stream(plq_ensemble *e);
+uint64_t plq_ensemble_launches(plq_ensemble *e);
+void plq_ensemble_destroy(plq_ensemble *e);
+
 /* ------------------------------------------- allocation-free sweep */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a host that owns the device memory and lends this library one buffer, or

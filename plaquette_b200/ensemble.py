@@ -1,0 +1,115 @@
+"""Batched ensembles: many chains advanced by one persistent launch.
+
+``Ensemble`` wraps the ``plq_ensemble_*`` entry points of include/plaquette.h:
+members are chain descriptors (any mix of models, shapes, betas, seeds),
+optionally grouped into parallel-tempering ladders; ``advance`` runs every
+member in one cooperative, graph-captured launch and ``advance_unbatched``
+runs the same sweeps one launch per member per colour pass (the per-lattice
+baseline, identical results).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import ChainDesc, check, extra_signatures, lib
+
+_P = C.POINTER
+extra_signatures({
+    "plq_ensemble_create": ([C.c_void_p, C.c_int32, _P(ChainDesc), _P(C.c_void_p), _P(C.c_void_p)], C.c_int),
+    "plq_ensemble_add_ladder": ([C.c_void_p, C.c_int32, _P(C.c_int32), _P(C.c_double), C.c_int32, C.c_uint64],
+                                C.c_int),
+    "plq_ensemble_advance": ([C.c_void_p, C.c_uint64], C.c_int),
+    "plq_ensemble_advance_unbatched": ([C.c_void_p, C.c_uint64], C.c_int),
+    "plq_ensemble_set_config": ([C.c_void_p, C.c_int32, C.c_int32], C.c_int),
+    "plq_ensemble_tune": ([C.c_void_p, C.c_int32, _P(C.c_int32), _P(C.c_int32), _P(C.c_double)], C.c_int),
+    "plq_ensemble_sync": ([C.c_void_p], C.c_int),
+    "plq_ensemble_read": ([C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
+    "plq_ensemble_primaries": ([C.c_void_p, C.c_int32, C.c_void_p, _P(C.c_int32)], C.c_int),
+    "plq_ensemble_betas": ([C.c_void_p, C.c_void_p], C.c_int),
+    "plq_ensemble_n_vars": ([C.c_void_p], C.c_int64),
+    "plq_ensemble_cuda_stream": ([C.c_void_p], C.c_void_p),
+    "plq_ensemble_launches": ([C.c_void_p], C.c_uint64),
+    "plq_ensemble_destroy": ([C.c_void_p], None),
+})
+
+
+class Ensemble:
+    def __init__(self, gpu, descs: list[ChainDesc], starts: list[np.ndarray | None] | None = None):
+        self.gpu = gpu
+        self.descs = list(descs)
+        n = len(self.descs)
+        arr = (ChainDesc * n)(*self.descs)
+        self._keep = []
+        ptrs = (C.c_void_p * n)()
+        if starts is not None:
+            for i, s in enumerate(starts):
+                if s is not None:
+                    s = np.ascontiguousarray(s, dtype=np.uint8)
+                    self._keep.append(s)
+                    ptrs[i] = s.ctypes.data
+        self._h = C.c_void_p()
+        check(lib().plq_ensemble_create(gpu._h, n, arr, ptrs, C.byref(self._h)))
+        self.n = n
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().plq_ensemble_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def add_ladder(self, member_ids, betas, every: int, seed: int = 0):
+        k = len(member_ids)
+        ids = (C.c_int32 * k)(*member_ids)
+        bs = (C.c_double * k)(*betas)
+        check(lib().plq_ensemble_add_ladder(self._h, k, ids, bs, every, seed))
+
+    def advance(self, sweeps: int):
+        check(lib().plq_ensemble_advance(self._h, sweeps))
+
+    def advance_unbatched(self, sweeps: int):
+        check(lib().plq_ensemble_advance_unbatched(self._h, sweeps))
+
+    def set_config(self, ranks_per_thread: int, ctas_per_sm: int):
+        check(lib().plq_ensemble_set_config(self._h, ranks_per_thread, ctas_per_sm))
+
+    def tune(self, trial_sweeps: int = 10):
+        r, c, ms = C.c_int32(), C.c_int32(), C.c_double()
+        check(lib().plq_ensemble_tune(self._h, trial_sweeps, C.byref(r), C.byref(c), C.byref(ms)))
+        return r.value, c.value, ms.value
+
+    def sync(self):
+        check(lib().plq_ensemble_sync(self._h))
+
+    def n_vars(self, m: int | None = None) -> int:
+        if m is None:
+            return int(lib().plq_ensemble_n_vars(self._h))
+        d = self.descs[m]
+        n = int(np.prod([d.shape[i] for i in range(d.d)]))
+        return n * d.d if d.model == 2 else n
+
+    def read(self, m: int) -> np.ndarray:
+        out = np.empty(self.n_vars(m), dtype=np.uint8)
+        check(lib().plq_ensemble_read(self._h, m, out.ctypes.data))
+        return out
+
+    def primaries(self, m: int) -> np.ndarray:
+        out = np.zeros(66, dtype=np.int64)
+        n = C.c_int32()
+        check(lib().plq_ensemble_primaries(self._h, m, out.ctypes.data, C.byref(n)))
+        return out[: n.value].copy()
+
+    def betas(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        check(lib().plq_ensemble_betas(self._h, out.ctypes.data))
+        return out
+
+    @property
+    def cuda_stream(self) -> int:
+        return lib().plq_ensemble_cuda_stream(self._h) or 0
+
+    @property
+    def launches(self) -> int:
+        return int(lib().plq_ensemble_launches(self._h))

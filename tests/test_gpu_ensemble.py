@@ -1,0 +1,105 @@
+"""Batched ensembles: every member evolves exactly as its own chain would,
+batched (one persistent graph-captured launch) or unbatched (one launch per
+member per colour pass); parallel tempering gives identical results on both
+paths; the autotuner leaves the ensemble's state untouched."""
+import numpy as np
+import pytest
+
+import plaquette_b200 as plq
+from plaquette_b200.ensemble import Ensemble
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    g = plq.Gpu.new()
+    if g is None:
+        pytest.fail("no CUDA device")
+    return g
+
+
+def _members():
+    specs = [
+        (plq.ISING, 2, (16, 16, 16), plq.METROPOLIS, plq.RNG_KEYED, 0.2216544, 1),
+        (plq.ISING, 2, (24, 24, 24), plq.HEATBATH, plq.RNG_KEYED, 0.21, 2),
+        (plq.POTTS, 3, (8, 8, 8), plq.HEATBATH, plq.RNG_STREAM, 0.5505, 3),
+        (plq.GAUGE, 2, (4, 4, 4, 4), plq.HEATBATH, plq.RNG_KEYED, 0.44, 4),
+        (plq.GAUGE, 2, (6, 6, 6, 6), plq.HEATBATH, plq.RNG_STREAM, 0.40, 5),
+        (plq.ISING, 2, (32, 16), plq.METROPOLIS, plq.RNG_KEYED, 0.4406868, 6),
+        (plq.POTTS, 4, (8, 6, 4), plq.METROPOLIS, plq.RNG_KEYED, 0.62, 7),
+    ]
+    descs, starts = [], []
+    for kind, q, shape, upd, rng, beta, seed in specs:
+        n = int(np.prod(shape)) * (len(shape) if kind == plq.GAUGE else 1)
+        start, off = plq.hot_start(seed, q, n)
+        descs.append(plq.make_desc(kind, q, shape, upd, beta=beta, seed=seed, rng=rng, stream_offset=off,
+                                   sweeps_between=1, batch=1))
+        starts.append(start)
+    return descs, starts
+
+
+def test_members_match_their_own_chains(gpu):
+    descs, starts = _members()
+    ens = Ensemble(gpu, descs, starts)
+    chains = [plq.GpuChain(gpu, d, s) for d, s in zip(descs, starts)]
+    ens.advance(7)
+    for c in chains:
+        c.advance(7)
+    for m, c in enumerate(chains):
+        assert np.array_equal(ens.read(m), c.read()), m
+        assert list(ens.primaries(m)) == list(c.primaries()), m
+    ens.advance_unbatched(5)
+    for c in chains:
+        c.advance(5)
+    for m, c in enumerate(chains):
+        assert np.array_equal(ens.read(m), c.read()), m
+    ens.advance(3)
+    ens.advance(3)  # graph replay
+    for c in chains:
+        c.advance(6)
+    for m, c in enumerate(chains):
+        assert np.array_equal(ens.read(m), c.read()), m
+
+
+def _ladder_ensemble(gpu, L=8, k=8, every=2):
+    betas = list(np.geomspace(0.20, 0.24, k))
+    descs, starts = [], []
+    for i in range(k):
+        start, _ = plq.hot_start(100 + i, 2, L ** 3)
+        descs.append(plq.make_desc(plq.ISING, 2, (L, L, L), plq.METROPOLIS, beta=betas[i], seed=100 + i,
+                                   rng=plq.RNG_KEYED, sweeps_between=1, batch=1))
+        starts.append(start)
+    ens = Ensemble(gpu, descs, starts)
+    ens.add_ladder(list(range(k)), betas, every, seed=42)
+    return ens, betas
+
+
+def test_tempering_batched_equals_unbatched(gpu):
+    a, betas = _ladder_ensemble(gpu)
+    b, _ = _ladder_ensemble(gpu)
+    a.advance(20)
+    b.advance_unbatched(20)
+    assert np.array_equal(a.betas(), b.betas())
+    for m in range(8):
+        assert np.array_equal(a.read(m), b.read(m)), m
+    ba = a.betas()
+    assert sorted(ba.tolist()) == sorted(betas)
+    assert not np.array_equal(ba, np.array(betas)), "no swap was accepted in 10 attempts"
+
+
+def test_tune_keeps_state(gpu):
+    descs, starts = _members()
+    ens = Ensemble(gpu, descs, starts)
+    ens.advance(2)
+    before = [ens.read(m) for m in range(len(descs))]
+    r, c, ms = ens.tune(3)
+    assert r in (2, 4, 8) and c >= 1 and ms > 0
+    after = [ens.read(m) for m in range(len(descs))]
+    for x, y in zip(before, after):
+        assert np.array_equal(x, y)
+    chains = [plq.GpuChain(gpu, d, s) for d, s in zip(descs, starts)]
+    ens.advance(4)
+    for m, ch in enumerate(chains):
+        ch.advance(6)
+        assert np.array_equal(ens.read(m), ch.read()), m
