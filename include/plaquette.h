@@ -196,6 +196,37 @@ void *plq_ensemble_cuda_stream(plq_ensemble *e);
 uint64_t plq_ensemble_launches(plq_ensemble *e);
 void plq_ensemble_destroy(plq_ensemble *e);
 
+/* ---------------------------------------------------------- serving */
+/* No counterpart in the reference.  A request loop for simulation jobs
+ * (model, shape, beta, sweeps, ...): a worker thread admits queued jobs
+ * first-fit while their device footprint fits `budget_bytes` (0 = 80 % of
+ * free device memory) and fewer than `max_slots` run; keeps each job's state
+ * resident on the device; and batches every running job into one persistent
+ * launch per tick (about `tick_ms` of work), so jobs that arrive while others
+ * run join at the next tick and share its launches.  A job's result is the
+ * same alone or in any mix (its keyed sweep counter and stream position are
+ * its own).  Jobs: local updaters, d <= 4, keyed or heat bath on the PCG stream. */
+typedef struct plq_server plq_server;
+enum plq_job_state { PLQ_JOB_QUEUED = 0, PLQ_JOB_ACTIVE = 1, PLQ_JOB_DONE = 2, PLQ_JOB_FAILED = 3,
+                     PLQ_JOB_CANCELLED = 4 };
+int plq_server_create(plq_ctx *ctx, uint64_t budget_bytes, int32_t max_slots, double tick_ms, plq_server **out);
+/* Queue a job of `sweeps` sweeps from `start` (NULL = cold); returns at once.
+ * PLQ_ENOMEM if it could never fit the budget. */
+int plq_server_submit(plq_server *s, const plq_chain_desc *desc, const uint8_t *start, uint64_t sweeps,
+                      int32_t want_states, int64_t *job_id);
+/* Wait until the job left the queue and the device (timeout_s < 0: forever). */
+int plq_server_wait(plq_server *s, int64_t job_id, double timeout_s, int32_t *state_out);
+int plq_server_cancel(plq_server *s, int64_t job_id);
+/* Final configuration (if submitted with want_states), int64 primaries as
+ * plq_chain_primaries, timing {queue ms, latency ms} (each may be NULL). */
+int plq_server_result(plq_server *s, int64_t job_id, uint8_t *out_states, int64_t *out_primaries,
+                      double *timing_out);
+int plq_server_release(plq_server *s, int64_t job_id);
+/* {completed, p50 ms, p99 ms, site updates/ns while busy, ticks, queued,
+ * running, device bytes in use}; returns a device error if one occurred. */
+int plq_server_stats(plq_server *s, double *out8);
+void plq_server_destroy(plq_server *s);
+
 /* ------------------------------------------- allocation-free sweep */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a host that owns the device memory and lends this library one buffer, or

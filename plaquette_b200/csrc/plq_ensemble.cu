@@ -23,9 +23,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/plaquette.h"
@@ -84,6 +90,7 @@ struct EnsArgs {
     TableSet *tsets;
     int32_t *ts_of_member;
     unsigned long long *pos;  // stream heat bath: per-member stream position (relative)
+    unsigned long long *msweep;  // per-member sweep counters (serving), or null: all share ls->sweep
     const int32_t *item_member;
     const int32_t *item_chunk;
     const int64_t *sp_begin;
@@ -163,7 +170,7 @@ __device__ void item_args(const EnsArgs &e, int m, int sp, unsigned long long sw
     sa.metro24 = ts.metro24;
     sa.dir = mem.link ? sp >> 1 : 0;
     sa.color = sp & 1;
-    sa.sweep32 = (uint32_t)(e.ls->sweep + sweep_in_launch);
+    sa.sweep32 = (uint32_t)((e.msweep ? e.msweep[m] : e.ls->sweep) + sweep_in_launch);
     if (sa.jump)
         sa.pass_offset = e.pos[m] + sweep_in_launch * (unsigned long long)mem.n_vars +
                          (unsigned long long)sp * (unsigned long long)(mem.a.g.n_sites / 2);
@@ -299,8 +306,10 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     // advance the device-resident launch state (block 0, after every CTA left the loop)
     grid_barrier(e);
     if (blockIdx.x == 0) {
-        for (int m = threadIdx.x; m < e.n_members; m += blockDim.x)
+        for (int m = threadIdx.x; m < e.n_members; m += blockDim.x) {
             if (e.members[m].a.jump) e.pos[m] += e.sweeps * (unsigned long long)e.members[m].n_vars;
+            if (e.msweep) e.msweep[m] += e.sweeps;
+        }
         __syncthreads();
         if (threadIdx.x == 0) e.ls->sweep += e.sweeps;
     }
@@ -977,4 +986,634 @@ extern "C" void plq_ensemble_destroy(plq_ensemble *E) {
     for (void *p : E->allocs) cudaFree(p);
     if (E->stream) cudaStreamDestroy(E->stream);
     delete E;
+}
+
+// ====================================================================
+// Serving: continuous batching of simulation jobs.
+//
+// A worker thread owns the device.  Each tick it (1) admits queued jobs,
+// first-fit, while their device footprint fits the memory budget and a slot
+// is free -- a job's lattice, tables and jump table are allocated once and
+// stay resident until it finishes; (2) launches the persistent ensemble
+// kernel over every active job for a quantum of sweeps sized so a tick takes
+// about `tick_ms`; (3) retires finished jobs: final primaries (and, if asked,
+// the configuration) are read back and their memory freed.  Jobs that arrive
+// while others run join at the next tick; their sweeps share launches with
+// whatever else is active.  Each job keeps its own keyed sweep counter and
+// stream position, so its result is the same alone or in any mix.
+// ====================================================================
+
+struct ServerJob {
+    int64_t id = 0;
+    plq_chain_desc desc;
+    std::vector<uint8_t> start;
+    bool has_start = false;
+    uint64_t sweeps = 0, done = 0;
+    bool want_states = false;
+    int state = PLQ_JOB_QUEUED;
+    int error = PLQ_OK;
+    std::string message;
+    double t_submit = 0, t_admit = 0, t_finish = 0;
+    uint64_t footprint = 0;
+    // device state while active
+    EnsMember mem;
+    TableSet ts;
+    std::vector<void *> allocs;
+    unsigned long long pos = 0, msweep = 0;
+    // results
+    std::vector<uint8_t> final_states;
+    std::vector<int64_t> primaries;
+};
+
+struct plq_server {
+    plq_ctx *ctx = nullptr;
+    uint64_t budget = 0, used = 0;
+    int max_slots = 0;
+    double tick_ms = 10.0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread worker;
+    bool stop = false;
+    int64_t next_id = 1;
+    std::deque<ServerJob *> queue;
+    std::vector<ServerJob *> active;
+    std::map<int64_t, ServerJob *> jobs;
+    // statistics
+    std::vector<double> latencies_ms;
+    double updates = 0, busy_s = 0;
+    uint64_t ticks = 0, launches = 0;
+    double last_ms_per_sweep = 1.0;
+    int device_error = PLQ_OK;
+    std::string device_message;
+};
+
+namespace {
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Device bytes a job holds while active.
+uint64_t job_footprint(const plq_chain_desc &d) {
+    int64_t n = 1;
+    for (int i = 0; i < d.d; ++i) n *= d.shape[i];
+    int64_t n_vars = d.model == PLQ_GAUGE ? n * d.d : n;
+    ModelParams p;
+    std::memset(&p, 0, sizeof p);
+    p.model = d.model;
+    p.q = d.model == PLQ_POTTS ? d.q : 2;
+    p.d = d.d;
+    int64_t keys = d.updater == PLQ_METROPOLIS && p.q > 2 ? potts_metro_key_count(p) : env_key_count(p);
+    uint64_t table = (uint64_t)keys * (uint64_t)std::max(1, p.q - 1) * 8ull;
+    uint64_t jump = d.rng == PLQ_RNG_STREAM ? 65536ull : 0ull;
+    return (uint64_t)n_vars + table + jump + 4096ull;
+}
+
+void job_release(ServerJob *j) {
+    for (void *p : j->allocs) cudaFree(p);
+    j->allocs.clear();
+}
+
+// Allocate and upload a job's resident state (worker thread, device current).
+int job_admit(plq_server *S, ServerJob *j, cudaStream_t stream) {
+    const plq_chain_desc &d = j->desc;
+    EnsMember &mem = j->mem;
+    std::memset(&mem, 0, sizeof mem);
+    LocalArgs &a = mem.a;
+    const int q = d.model == PLQ_POTTS ? d.q : 2;
+    a.g.d = d.d;
+    int64_t ns = 1;
+    for (int i = 0; i < kMaxD; ++i) {
+        a.g.L[i] = i < d.d ? (int32_t)d.shape[i] : 1;
+        a.g.stride[i] = ns;
+        if (i < d.d) ns *= d.shape[i];
+    }
+    a.g.n_sites = ns;
+    mem.link = d.model == PLQ_GAUGE;
+    mem.passes = mem.link ? 2 * d.d : 2;
+    mem.n_vars = mem.link ? ns * d.d : ns;
+    mem.j = d.j;
+    mem.ladder = -1;
+    a.q = q;
+    a.kernel = d.updater;
+    a.model = d.model;
+    int32_t w = 1;
+    for (int s = 1; s < q; ++s) {
+        a.pw[s] = w;
+        w *= 2 * d.d + 1;
+    }
+    a.seed32 = plq_fold_seed(d.seed);
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) j->allocs.push_back(*p);
+    };
+    uint8_t *st = nullptr;
+    alloc((void **)&st, (size_t)mem.n_vars);
+    a.state = st;
+    if (e == cudaSuccess) {
+        if (j->has_start) {
+            if (mem.link) {
+                uint8_t *tmp = nullptr;
+                e = cudaMalloc((void **)&tmp, (size_t)mem.n_vars);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(tmp, j->start.data(), (size_t)mem.n_vars, cudaMemcpyHostToDevice, stream);
+                if (e == cudaSuccess) e = launch_links_to_planes(tmp, st, ns, d.d, stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+                if (tmp) cudaFree(tmp);
+            } else {
+                e = cudaMemcpyAsync(st, j->start.data(), (size_t)mem.n_vars, cudaMemcpyHostToDevice, stream);
+            }
+        } else {
+            e = cudaMemsetAsync(st, 0, (size_t)mem.n_vars, stream);
+        }
+    }
+    if (e == cudaSuccess && d.rng == PLQ_RNG_STREAM) {
+        uint64_t slo, shi, ilo, ihi;
+        pcg_seed_from_u64(d.seed, slo, shi, ilo, ihi);
+        std::vector<AffineHost> tab;
+        build_jump_table(ilo, ihi, tab);
+        a.inc = u128{ilo, ihi};
+        u128 s0 = jump(reinterpret_cast<const Affine *>(tab.data()), u128{slo, shi}, d.stream_offset);
+        a.base = pcg_step(s0, a.inc);
+        void *dj = nullptr;
+        alloc(&dj, tab.size() * sizeof(AffineHost));
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dj, tab.data(), tab.size() * sizeof(AffineHost), cudaMemcpyHostToDevice, stream);
+        a.jump = reinterpret_cast<const Affine *>(dj);
+    }
+    if (e != cudaSuccess) {
+        job_release(j);
+        return plq_fail(e == cudaErrorMemoryAllocation ? PLQ_ENOMEM : PLQ_ECUDA, cudaGetErrorString(e));
+    }
+    ModelParams p;
+    std::memset(&p, 0, sizeof p);
+    p.model = d.model;
+    p.q = q;
+    p.d = d.d;
+    p.beta = d.beta;
+    p.j = d.j;
+    p.h = d.h;
+    for (int k = 0; k < PLQ_MAX_Q; ++k) p.offsets[k] = d.offsets[k];
+    Tables t;
+    std::string err;
+    if (!build_tables(p, d.updater, d.rng, t, err)) {
+        job_release(j);
+        return plq_fail(PLQ_EUNSUPPORTED, err);
+    }
+    std::memset(&j->ts, 0, sizeof j->ts);
+    j->ts.beta = d.beta;
+    auto up = [&](const void *host, size_t bytes) -> void * {
+        if (!bytes || e != cudaSuccess) return nullptr;
+        void *p2 = nullptr;
+        alloc(&p2, bytes);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p2, host, bytes, cudaMemcpyHostToDevice, stream);
+        return p2;
+    };
+    j->ts.hb53 = (const uint64_t *)up(t.hb53.data(), t.hb53.size() * 8);
+    j->ts.hb24 = (const uint32_t *)up(t.hb24.data(), t.hb24.size() * 4);
+    j->ts.metro53 = (const uint64_t *)up(t.metro53.data(), t.metro53.size() * 8);
+    j->ts.metro24 = (const uint32_t *)up(t.metro24.data(), t.metro24.size() * 4);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        job_release(j);
+        return plq_fail(e == cudaErrorMemoryAllocation ? PLQ_ENOMEM : PLQ_ECUDA, cudaGetErrorString(e));
+    }
+    return PLQ_OK;
+}
+
+// Device buffers of one tick's launch; grown, never shrunk.
+struct TickBuffers {
+    EnsMember *members = nullptr;
+    TableSet *tsets = nullptr;
+    int32_t *ts = nullptr;
+    unsigned long long *pos = nullptr, *msweep = nullptr;
+    int32_t *im = nullptr, *ic = nullptr;
+    int64_t *spb = nullptr;
+    LaunchState *ls = nullptr;
+    Control *ctrl = nullptr;
+    size_t cap_members = 0, cap_items = 0;
+    void release() {
+        void *ps[] = {members, tsets, ts, pos, msweep, im, ic, spb, ls, ctrl};
+        for (void *p : ps)
+            if (p) cudaFree(p);
+        *this = TickBuffers();
+    }
+};
+
+int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps) {
+    const size_t n = S->active.size();
+    std::vector<EnsMember> mems(n);
+    std::vector<TableSet> tss(n);
+    std::vector<int32_t> ts(n);
+    std::vector<unsigned long long> pos(n), msw(n);
+    int max_passes = 0;
+    for (size_t m = 0; m < n; ++m) {
+        mems[m] = S->active[m]->mem;
+        tss[m] = S->active[m]->ts;
+        ts[m] = (int32_t)m;
+        pos[m] = S->active[m]->pos;
+        msw[m] = S->active[m]->msweep;
+        max_passes = std::max(max_passes, mems[m].passes);
+    }
+    const int ranks = 8;
+    const int64_t chunk = (int64_t)kEnsThreads * ranks;
+    std::vector<int32_t> im, ic;
+    std::vector<int64_t> spb;
+    for (int sp = 0; sp < max_passes; ++sp) {
+        spb.push_back((int64_t)im.size());
+        for (size_t m = 0; m < n; ++m) {
+            if (sp >= mems[m].passes) continue;
+            int64_t nc = (mems[m].a.g.n_sites / 2 + chunk - 1) / chunk;
+            for (int64_t c = 0; c < nc; ++c) {
+                im.push_back((int32_t)m);
+                ic.push_back((int32_t)c);
+            }
+        }
+    }
+    spb.push_back((int64_t)im.size());
+    cudaError_t e = cudaSuccess;
+    if (!B.ls) {
+        e = cudaMalloc((void **)&B.ls, sizeof(LaunchState));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.ctrl, sizeof(Control));
+        if (e == cudaSuccess) e = cudaMemsetAsync(B.ls, 0, sizeof(LaunchState), stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(B.ctrl, 0, sizeof(Control), stream);
+    }
+    if (e == cudaSuccess && B.cap_members < n) {
+        cudaFree(B.members);
+        cudaFree(B.tsets);
+        cudaFree(B.ts);
+        cudaFree(B.pos);
+        cudaFree(B.msweep);
+        size_t c = std::max<size_t>(n, 2 * B.cap_members);
+        e = cudaMalloc((void **)&B.members, c * sizeof(EnsMember));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.tsets, c * sizeof(TableSet));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.ts, c * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.pos, c * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.msweep, c * sizeof(unsigned long long));
+        B.cap_members = c;
+    }
+    if (e == cudaSuccess && B.cap_items < im.size() + 1) {
+        cudaFree(B.im);
+        cudaFree(B.ic);
+        cudaFree(B.spb);
+        size_t c = std::max<size_t>(im.size() + 1, 2 * B.cap_items);
+        e = cudaMalloc((void **)&B.im, c * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.ic, c * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.spb, 64 * sizeof(int64_t));
+        B.cap_items = c;
+    }
+    if (e != cudaSuccess) return plq_fail(PLQ_ENOMEM, std::string("tick buffers: ") + cudaGetErrorString(e));
+    cudaMemcpyAsync(B.members, mems.data(), n * sizeof(EnsMember), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(B.tsets, tss.data(), n * sizeof(TableSet), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(B.ts, ts.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(B.pos, pos.data(), n * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(B.msweep, msw.data(), n * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(B.im, im.data(), im.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(B.ic, ic.data(), ic.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(B.spb, spb.data(), spb.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream);
+    EnsArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.members = B.members;
+    a.n_members = (int)n;
+    a.tsets = B.tsets;
+    a.ts_of_member = B.ts;
+    a.pos = B.pos;
+    a.msweep = B.msweep;
+    a.item_member = B.im;
+    a.item_chunk = B.ic;
+    a.sp_begin = B.spb;
+    a.n_sp = max_passes;
+    a.ls = B.ls;
+    a.ctrl = B.ctrl;
+    a.sweeps = sweeps;
+    a.ranks = ranks;
+    void *params[] = {&a};
+    int ctas = std::max(1, std::min(2, max_ctas_per_sm(ranks)));
+    dim3 grid((unsigned)(S->ctx->sm_count * ctas));
+    e = cudaLaunchCooperativeKernel(kernel_ptr(ranks), grid, dim3(kEnsThreads), params, 0, stream);
+    S->launches++;
+    unsigned int status = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &B.ctrl->status, sizeof status, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, std::string("serving launch: ") + cudaGetErrorString(e));
+    if (status) return plq_fail(PLQ_EDEVICE, "serving kernel status word " + std::to_string(status));
+    for (size_t m = 0; m < n; ++m) {
+        ServerJob *j = S->active[m];
+        j->done += sweeps;
+        j->msweep += sweeps;
+        if (j->mem.a.jump) j->pos += sweeps * (unsigned long long)j->mem.n_vars;
+    }
+    return PLQ_OK;
+}
+
+void retire(plq_server *S, ServerJob *j, cudaStream_t stream) {
+    const EnsMember &mem = j->mem;
+    int np = primaries_count(mem.a.model, mem.a.q);
+    std::vector<long long> prim((size_t)np, 0);
+    long long *d = nullptr;
+    cudaError_t e = cudaMalloc((void **)&d, sizeof(long long) * (size_t)np);
+    if (e == cudaSuccess) e = launch_primaries(mem.a.state, mem.a.g, mem.a.model, mem.a.q, d, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(prim.data(), d, sizeof(long long) * (size_t)np, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && j->want_states) {
+        j->final_states.resize((size_t)mem.n_vars);
+        if (mem.link) {
+            uint8_t *tmp = nullptr;
+            e = cudaMalloc((void **)&tmp, (size_t)mem.n_vars);
+            if (e == cudaSuccess) e = launch_planes_to_links(mem.a.state, tmp, mem.a.g.n_sites, mem.a.g.d, stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(j->final_states.data(), tmp, (size_t)mem.n_vars, cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (tmp) cudaFree(tmp);
+        } else {
+            e = cudaMemcpyAsync(j->final_states.data(), mem.a.state, (size_t)mem.n_vars, cudaMemcpyDeviceToHost,
+                                stream);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (d) cudaFree(d);
+    job_release(j);
+    std::lock_guard<std::mutex> lock(S->mu);
+    S->used -= j->footprint;
+    j->t_finish = now_s();
+    if (e != cudaSuccess) {
+        j->state = PLQ_JOB_FAILED;
+        j->error = PLQ_ECUDA;
+        j->message = cudaGetErrorString(e);
+    } else {
+        j->primaries.assign(prim.begin(), prim.end());
+        j->state = PLQ_JOB_DONE;
+        S->latencies_ms.push_back((j->t_finish - j->t_submit) * 1e3);
+    }
+}
+
+void worker_loop(plq_server *S) {
+    cudaSetDevice(S->ctx->device);
+    cudaStream_t stream = nullptr;
+    cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    TickBuffers B;
+    for (;;) {
+        // 1. admit (first fit by footprint and slots)
+        std::vector<ServerJob *> admit;
+        {
+            std::unique_lock<std::mutex> lock(S->mu);
+            S->cv_work.wait(lock, [&] { return S->stop || !S->queue.empty() || !S->active.empty(); });
+            if (S->stop) break;
+            for (auto it = S->queue.begin(); it != S->queue.end();) {
+                ServerJob *j = *it;
+                if ((int)(S->active.size() + admit.size()) >= S->max_slots) break;
+                if (S->used + j->footprint <= S->budget) {
+                    S->used += j->footprint;
+                    admit.push_back(j);
+                    it = S->queue.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        }
+        for (ServerJob *j : admit) {
+            int rc = job_admit(S, j, stream);
+            std::lock_guard<std::mutex> lock(S->mu);
+            if (rc != PLQ_OK) {
+                S->used -= j->footprint;
+                j->state = PLQ_JOB_FAILED;
+                j->error = rc;
+                j->message = plq_last_error();
+                j->t_finish = now_s();
+                S->cv_done.notify_all();
+            } else {
+                j->state = PLQ_JOB_ACTIVE;
+                j->t_admit = now_s();
+                S->active.push_back(j);
+            }
+        }
+        // jobs with nothing left to run (zero sweeps) retire before the tick
+        {
+            std::vector<ServerJob *> still;
+            for (ServerJob *j : S->active) {
+                if (j->done >= j->sweeps)
+                    retire(S, j, stream);
+                else
+                    still.push_back(j);
+            }
+            S->active.swap(still);
+            S->cv_done.notify_all();
+        }
+        if (S->active.empty()) continue;
+        // 2. one tick: a quantum of sweeps for every active job
+        uint64_t remaining = ~0ull;
+        for (ServerJob *j : S->active) remaining = std::min(remaining, j->sweeps - j->done);
+        uint64_t quantum = (uint64_t)std::max(1.0, S->tick_ms / std::max(1e-3, S->last_ms_per_sweep));
+        quantum = std::max<uint64_t>(1, std::min(quantum, remaining));
+        double t0 = now_s();
+        int rc = remaining ? run_tick(S, B, stream, quantum) : PLQ_OK;
+        double dt = now_s() - t0;
+        if (remaining) S->last_ms_per_sweep = std::max(1e-3, dt * 1e3 / (double)quantum);
+        {
+            std::lock_guard<std::mutex> lock(S->mu);
+            S->ticks++;
+            S->busy_s += dt;
+            if (rc != PLQ_OK) {
+                S->device_error = rc;
+                S->device_message = plq_last_error();
+                for (ServerJob *j : S->active) {
+                    j->state = PLQ_JOB_FAILED;
+                    j->error = rc;
+                    j->message = S->device_message;
+                    S->used -= j->footprint;
+                }
+            } else if (remaining) {
+                for (ServerJob *j : S->active) {
+                    int64_t nv = j->mem.n_vars;
+                    S->updates += (double)nv * (double)quantum;
+                }
+            }
+        }
+        if (rc != PLQ_OK) {
+            for (ServerJob *j : S->active) job_release(j);
+            S->active.clear();
+            S->cv_done.notify_all();
+            continue;
+        }
+        // 3. retire finished jobs
+        std::vector<ServerJob *> still;
+        for (ServerJob *j : S->active) {
+            if (j->done >= j->sweeps)
+                retire(S, j, stream);
+            else
+                still.push_back(j);
+        }
+        S->active.swap(still);
+        S->cv_done.notify_all();
+    }
+    for (ServerJob *j : S->active) job_release(j);
+    S->active.clear();
+    B.release();
+    cudaStreamDestroy(stream);
+}
+
+}  // namespace
+
+extern "C" int plq_server_create(plq_ctx *ctx, uint64_t budget_bytes, int32_t max_slots, double tick_ms,
+                                 plq_server **out) {
+    if (!ctx || !out || max_slots <= 0) return plq_fail(PLQ_EINVAL, "bad server arguments");
+    *out = nullptr;
+    plq_server *S = new plq_server();
+    S->ctx = ctx;
+    S->max_slots = max_slots;
+    S->tick_ms = tick_ms > 0 ? tick_ms : 10.0;
+    if (budget_bytes == 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaSetDevice(ctx->device);
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            delete S;
+            return plq_fail(PLQ_ECUDA, "cudaMemGetInfo failed");
+        }
+        budget_bytes = (uint64_t)(0.8 * (double)free_b);
+    }
+    S->budget = budget_bytes;
+    S->worker = std::thread(worker_loop, S);
+    *out = S;
+    return PLQ_OK;
+}
+
+extern "C" int plq_server_submit(plq_server *S, const plq_chain_desc *desc, const uint8_t *start, uint64_t sweeps,
+                                 int32_t want_states, int64_t *job_id) {
+    if (!S || !desc || !job_id) return plq_fail(PLQ_EINVAL, "bad arguments");
+    int rc = plq_chain_validate(desc);
+    if (rc != PLQ_OK) return rc;
+    if (desc->updater == PLQ_CLUSTER || desc->d > 4 ||
+        (desc->rng == PLQ_RNG_STREAM && desc->updater == PLQ_METROPOLIS))
+        return plq_fail(PLQ_EUNSUPPORTED,
+                        "served jobs are local updaters in at most 4 dimensions (keyed, or heat bath on the PCG "
+                        "stream)");
+    ServerJob *j = new ServerJob();
+    j->desc = *desc;
+    j->sweeps = sweeps;
+    j->want_states = want_states != 0;
+    j->footprint = job_footprint(*desc);
+    int64_t n = 1;
+    for (int i = 0; i < desc->d; ++i) n *= desc->shape[i];
+    int64_t n_vars = desc->model == PLQ_GAUGE ? n * desc->d : n;
+    const int q = desc->model == PLQ_POTTS ? desc->q : 2;
+    if (start) {
+        for (int64_t i = 0; i < n_vars; ++i)
+            if (start[i] >= q) {
+                delete j;
+                return plq_fail(PLQ_EINVAL, "start state out of range");
+            }
+        j->start.assign(start, start + n_vars);
+        j->has_start = true;
+    }
+    std::lock_guard<std::mutex> lock(S->mu);
+    if (j->footprint > S->budget) {
+        delete j;
+        return plq_fail(PLQ_ENOMEM, "the job's device footprint exceeds the server's memory budget");
+    }
+    j->id = S->next_id++;
+    j->t_submit = now_s();
+    S->jobs[j->id] = j;
+    if (sweeps == 0) {
+        // nothing to run: still a job, resolved at the next tick with its start state
+        j->sweeps = 0;
+    }
+    S->queue.push_back(j);
+    *job_id = j->id;
+    S->cv_work.notify_one();
+    return PLQ_OK;
+}
+
+extern "C" int plq_server_wait(plq_server *S, int64_t job_id, double timeout_s, int32_t *state_out) {
+    if (!S) return plq_fail(PLQ_EINVAL, "NULL server");
+    std::unique_lock<std::mutex> lock(S->mu);
+    auto it = S->jobs.find(job_id);
+    if (it == S->jobs.end()) return plq_fail(PLQ_EINVAL, "unknown job");
+    ServerJob *j = it->second;
+    auto finished = [&] { return j->state == PLQ_JOB_DONE || j->state == PLQ_JOB_FAILED || j->state == PLQ_JOB_CANCELLED; };
+    if (timeout_s < 0)
+        S->cv_done.wait(lock, finished);
+    else
+        S->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), finished);
+    if (state_out) *state_out = j->state;
+    return PLQ_OK;
+}
+
+extern "C" int plq_server_cancel(plq_server *S, int64_t job_id) {
+    if (!S) return plq_fail(PLQ_EINVAL, "NULL server");
+    std::lock_guard<std::mutex> lock(S->mu);
+    auto it = S->jobs.find(job_id);
+    if (it == S->jobs.end()) return plq_fail(PLQ_EINVAL, "unknown job");
+    ServerJob *j = it->second;
+    if (j->state != PLQ_JOB_QUEUED) return plq_fail(PLQ_EBUSY, "only a queued job can be cancelled");
+    S->queue.erase(std::remove(S->queue.begin(), S->queue.end(), j), S->queue.end());
+    j->state = PLQ_JOB_CANCELLED;
+    j->t_finish = now_s();
+    S->cv_done.notify_all();
+    return PLQ_OK;
+}
+
+extern "C" int plq_server_result(plq_server *S, int64_t job_id, uint8_t *out_states, int64_t *out_primaries,
+                                 double *timing_out) {
+    if (!S) return plq_fail(PLQ_EINVAL, "NULL server");
+    std::lock_guard<std::mutex> lock(S->mu);
+    auto it = S->jobs.find(job_id);
+    if (it == S->jobs.end()) return plq_fail(PLQ_EINVAL, "unknown job");
+    ServerJob *j = it->second;
+    if (j->state == PLQ_JOB_FAILED) return plq_fail(j->error, j->message);
+    if (j->state != PLQ_JOB_DONE) return plq_fail(PLQ_EBUSY, "job not finished");
+    if (out_states) {
+        if (!j->want_states) return plq_fail(PLQ_EINVAL, "the job was submitted without want_states");
+        std::memcpy(out_states, j->final_states.data(), j->final_states.size());
+    }
+    if (out_primaries) std::copy(j->primaries.begin(), j->primaries.end(), out_primaries);
+    if (timing_out) {
+        timing_out[0] = (j->t_admit - j->t_submit) * 1e3;
+        timing_out[1] = (j->t_finish - j->t_submit) * 1e3;
+    }
+    return PLQ_OK;
+}
+
+extern "C" int plq_server_release(plq_server *S, int64_t job_id) {
+    if (!S) return plq_fail(PLQ_EINVAL, "NULL server");
+    std::lock_guard<std::mutex> lock(S->mu);
+    auto it = S->jobs.find(job_id);
+    if (it == S->jobs.end()) return plq_fail(PLQ_EINVAL, "unknown job");
+    ServerJob *j = it->second;
+    if (j->state == PLQ_JOB_QUEUED || j->state == PLQ_JOB_ACTIVE) return plq_fail(PLQ_EBUSY, "job still running");
+    S->jobs.erase(it);
+    delete j;
+    return PLQ_OK;
+}
+
+extern "C" int plq_server_stats(plq_server *S, double *out) {
+    if (!S || !out) return plq_fail(PLQ_EINVAL, "bad arguments");
+    std::lock_guard<std::mutex> lock(S->mu);
+    std::vector<double> lat = S->latencies_ms;
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&](double p) {
+        if (lat.empty()) return 0.0;
+        size_t k = (size_t)std::min<double>((double)lat.size() - 1, std::ceil(p * (double)lat.size()) - 1);
+        return lat[k];
+    };
+    out[0] = (double)lat.size();
+    out[1] = pct(0.50);
+    out[2] = pct(0.99);
+    out[3] = S->busy_s > 0 ? S->updates / S->busy_s / 1e9 : 0.0;
+    out[4] = (double)S->ticks;
+    out[5] = (double)S->queue.size();
+    out[6] = (double)S->active.size();
+    out[7] = (double)S->used;
+    return S->device_error;
+}
+
+extern "C" void plq_server_destroy(plq_server *S) {
+    if (!S) return;
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        S->stop = true;
+        S->cv_work.notify_all();
+    }
+    if (S->worker.joinable()) S->worker.join();
+    for (auto &kv : S->jobs) delete kv.second;
+    delete S;
 }
