@@ -281,6 +281,7 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
         if (i < desc->d) n *= desc->shape[i];
     }
     c->g.n_sites = n;
+    geom_init(c->g, desc->d, desc->shape);
     c->n_sites = n;
     c->n_vars = c->link ? n * desc->d : n;
     c->seed32 = plq_fold_seed(desc->seed);

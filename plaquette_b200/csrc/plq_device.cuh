@@ -16,13 +16,51 @@ constexpr uint32_t kStatusPassCap = 1u << 1;
 constexpr uint32_t kStatusBounds = 1u << 2;
 constexpr uint32_t kStatusQueueOverflow = 1u << 3;
 
-// Lattice geometry by value: extents, strides, site count.
+// Lattice geometry by value: extents, strides, site count, and the magic
+// numbers that divide a site index (< 2^31) by each extent.
 struct Geom {
     int d;
     int32_t L[kMaxD];
     int64_t stride[kMaxD];
     int64_t n_sites;
+    uint32_t dm[kMaxD];  // division by L[mu]: multiplier
+    int32_t dl[kMaxD];   // ... and ceil(log2 L[mu])
 };
+
+// Division by an invariant integer with one multiply-high (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", 1994,
+// the unsigned multiply-add form): exact for every 32-bit n.
+PLQ_HD uint32_t fdiv(uint32_t n, uint32_t m, int l) {
+    if (l == 0) return n;
+#if defined(__CUDA_ARCH__)
+    uint32_t t1 = __umulhi(m, n);
+#else
+    uint32_t t1 = (uint32_t)(((uint64_t)m * n) >> 32);
+#endif
+    return (t1 + ((n - t1) >> 1)) >> (l - 1);
+}
+
+// Fill extents, strides and division constants from a shape.
+inline void geom_init(Geom &g, int d, const int64_t *shape) {
+    g.d = d;
+    int64_t n = 1;
+    for (int i = 0; i < kMaxD; ++i) {
+        g.L[i] = i < d ? (int32_t)shape[i] : 1;
+        g.stride[i] = n;
+        if (i < d) n *= shape[i];
+        uint32_t L = (uint32_t)g.L[i];
+        if (L <= 1) {
+            g.dm[i] = 0;
+            g.dl[i] = 0;
+        } else {
+            int l = 0;
+            while ((1ull << l) < L) ++l;
+            g.dm[i] = (uint32_t)((((1ull << 32) * ((1ull << l) - L)) / L) + 1);
+            g.dl[i] = l;
+        }
+    }
+    g.n_sites = n;
+}
 
 // Per-chain device control block (in device memory).
 struct Control {

@@ -529,6 +529,7 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
             if (i < d.d) ns *= d.shape[i];
         }
         a.g.n_sites = ns;
+    geom_init(a.g, d.d, d.shape);
         mem.link = d.model == PLQ_GAUGE;
         mem.passes = mem.link ? 2 * d.d : 2;
         mem.n_vars = mem.link ? ns * d.d : ns;
@@ -1089,6 +1090,7 @@ int job_admit(plq_server *S, ServerJob *j, cudaStream_t stream) {
         if (i < d.d) ns *= d.shape[i];
     }
     a.g.n_sites = ns;
+    geom_init(a.g, d.d, d.shape);
     mem.link = d.model == PLQ_GAUGE;
     mem.passes = mem.link ? 2 * d.d : 2;
     mem.n_vars = mem.link ? ns * d.d : ns;

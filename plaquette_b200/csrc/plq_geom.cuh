@@ -9,10 +9,12 @@ namespace plq {
 
 template <int D>
 __device__ __forceinline__ void site_coords(const Geom &g, int64_t s, int32_t *x) {
+    uint32_t t = (uint32_t)s;  // site indices are below 2^31
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) {
-        x[mu] = (int32_t)(s % g.L[mu]);
-        s /= g.L[mu];
+        uint32_t q = fdiv(t, g.dm[mu], g.dl[mu]);
+        x[mu] = (int32_t)(t - q * (uint32_t)g.L[mu]);
+        t = q;
     }
 }
 

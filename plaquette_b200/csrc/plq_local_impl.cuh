@@ -31,10 +31,12 @@ __device__ __forceinline__ unsigned long long make_desc(uint32_t epoch, unsigned
 
 template <int D>
 __device__ __forceinline__ void coords_of(const Geom &g, int64_t s, int32_t *x) {
+    uint32_t t = (uint32_t)s;
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) {
-        x[mu] = (int32_t)(s % g.L[mu]);
-        s /= g.L[mu];
+        uint32_t q = fdiv(t, g.dm[mu], g.dl[mu]);
+        x[mu] = (int32_t)(t - q * (uint32_t)g.L[mu]);
+        t = q;
     }
 }
 
@@ -51,21 +53,22 @@ __device__ __forceinline__ int64_t step_minus(const Geom &g, int64_t s, const in
 // (extent 0 even): s = 2r + b, b fixed by the parity of the row.
 template <int D>
 __device__ __forceinline__ int64_t site_of_rank(const Geom &g, int64_t r, int color, int32_t *x) {
-    int64_t even = 2 * r;
-    int64_t row = even / g.L[0];
+    const uint32_t even = 2u * (uint32_t)r;  // < 2^31: a site index
+    const uint32_t row = fdiv(even, g.dm[0], g.dl[0]);
     int par = 0;
-    int64_t rr = row;
+    uint32_t rr = row;
 #pragma unroll
     for (int mu = 1; mu < D; ++mu) {
-        int32_t c = (int32_t)(rr % g.L[mu]);
-        rr /= g.L[mu];
+        uint32_t q = fdiv(rr, g.dm[mu], g.dl[mu]);
+        int32_t c = (int32_t)(rr - q * (uint32_t)g.L[mu]);
+        rr = q;
         x[mu] = c;
         par += c;
     }
     int b = (color ^ par) & 1;
-    int64_t s = even + b;
-    x[0] = (int32_t)(s - row * g.L[0]);
-    return s;
+    uint32_t s = even + (uint32_t)b;
+    x[0] = (int32_t)(s - row * (uint32_t)g.L[0]);
+    return (int64_t)s;
 }
 
 // Environment of a variable: key into the decision tables, plus the two

@@ -142,6 +142,7 @@ extern "C" int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int
         if (i < d) stride *= shape[i];
     }
     a.g.n_sites = n;
+    geom_init(a.g, d, shape);
     a.q = 2;
     a.kernel = PLQ_METROPOLIS;
     a.model = PLQ_ISING;

@@ -36,11 +36,12 @@ primaries_kernel(const uint8_t *state, Geom g, int model, int q, long long *out)
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
          s += (int64_t)gridDim.x * blockDim.x) {
         int32_t x[D];
-        int64_t t = s;
+        uint32_t t = (uint32_t)s;
 #pragma unroll
         for (int mu = 0; mu < D; ++mu) {
-            x[mu] = (int32_t)(t % g.L[mu]);
-            t /= g.L[mu];
+            uint32_t qq = fdiv(t, g.dm[mu], g.dl[mu]);
+            x[mu] = (int32_t)(t - qq * (uint32_t)g.L[mu]);
+            t = qq;
         }
         if (model == PLQ_GAUGE) {
             // plaquettes (s, mu, nu), mu < nu: U_mu(s) U_nu(s+mu) U_mu(s+nu) U_nu(s)
