@@ -1,12 +1,13 @@
 """Throughput benchmark of the lattice Monte Carlo hot path on B200.
 
-Workload (one GPU): 3D q=3 Potts, 512^3 periodic, u8 states drawn uniformly
-from the seed exactly as the reference's hot start does (RandRng +
+Default workload (one GPU): 3D q=3 Potts, 512^3 periodic, u8 states drawn
+uniformly from the seed exactly as the reference's hot start does (RandRng +
 Configuration::hot), beta = 0.5505, checkerboard heat bath on the reference
 CPU stream (PCG64) -- bit-exact with the reference's CPU path.  One step =
 one sweep of the lattice (134,217,728 site updates).  Under torchrun each rank
 runs its own lattice (independent replicas, weak scaling; no collective on the
-data path).
+data path).  `--workload` selects the other 512^3 single-lattice cases (3D
+Ising Metropolis on the keyed or the PCG stream, q=3 Potts heat bath keyed).
 
 Prints one JSON line (rank 0).  ``--impl reference`` times the reference's
 CPU algorithm (the C restatement in oracle/, single thread -- the reference
@@ -27,13 +28,27 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SHAPE = (512, 512, 512)
-Q = 3
-BETA = 0.5505
 SEED = 20260718
-WORKLOAD = ("3D q=3 Potts 512^3 periodic, checkerboard heat bath, beta=0.5505, PCG64 reference stream "
-            "(bit-exact with the reference CPU path), uniform random u8 start from seed 20260718")
 N_SITES = SHAPE[0] * SHAPE[1] * SHAPE[2]
 BYTES_PER_UPDATE = 2  # each site read once and written once per sweep
+
+# name -> (model, q, updater, rng, beta, description, dominant kernel, launches per sweep)
+WORKLOADS = {
+    "potts3-512-hb-stream": ("potts", 3, "heatbath", "stream", 0.5505,
+                             "3D q=3 Potts 512^3 periodic, checkerboard heat bath, beta=0.5505, PCG64 reference "
+                             "stream (bit-exact with the reference CPU path), uniform random u8 start from seed "
+                             "20260718", "fused3d_kernel<3,true,true>", 1),
+    "potts3-512-hb-keyed": ("potts", 3, "heatbath", "keyed", 0.5505,
+                            "3D q=3 Potts 512^3 periodic, checkerboard heat bath, beta=0.5505, keyed reference GPU "
+                            "stream, uniform random u8 start from seed 20260718", "fused3d_kernel<3,false,true>", 1),
+    "ising-512-metro-keyed": ("ising", 2, "metropolis", "keyed", 0.2216544,
+                              "3D Ising 512^3 periodic, checkerboard Metropolis, beta=0.2216544, keyed reference GPU "
+                              "stream, uniform random start from seed 20260718", "fused3d_kernel<2,false,false>", 1),
+    "ising-512-metro-stream": ("ising", 2, "metropolis", "stream", 0.2216544,
+                               "3D Ising 512^3 periodic, checkerboard Metropolis, beta=0.2216544, PCG64 reference "
+                               "stream (bit-exact with the reference CPU path; device-wide scan per colour pass), "
+                               "uniform random start from seed 20260718", "local_pass_kernel<3,false,true>", 2),
+}
 
 
 def _env_int(name, default):
@@ -72,7 +87,6 @@ class ClockSampler:
         self.device = device
         self.samples = []
         self.proc = None
-        self.thread = None
 
     def start(self):
         try:
@@ -82,8 +96,7 @@ class ClockSampler:
         except Exception:
             self.proc = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
-        self.thread.start()
+        threading.Thread(target=self._read, daemon=True).start()
         time.sleep(0.3)
 
     def _read(self):
@@ -112,7 +125,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(inside)}
 
 
-def dist_setup(n_gpus):
+def dist_setup():
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local = _env_int("LOCAL_RANK", 0)
@@ -122,7 +135,7 @@ def dist_setup(n_gpus):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=None)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -145,23 +158,32 @@ def barrier(pg, device):
         pg.barrier()
 
 
+def _desc(plq, w, seed, offset):
+    model, q, upd, rng, beta = w[:5]
+    return plq.make_desc({"potts": plq.POTTS, "ising": plq.ISING}[model], q, SHAPE,
+                         {"heatbath": plq.HEATBATH, "metropolis": plq.METROPOLIS}[upd], beta=beta, seed=seed,
+                         rng={"stream": plq.RNG_STREAM, "keyed": plq.RNG_KEYED}[rng], stream_offset=offset,
+                         sweeps_between=1, batch=plq.GPU_BATCH)
+
+
 def run_product(args):
     import numpy as np
     import torch
 
     import plaquette_b200 as plq
 
-    world, rank, local, pg = dist_setup(args.gpus)
+    w = WORKLOADS[args.workload]
+    world, rank, local, pg = dist_setup()
     torch.cuda.set_device(local)
     gpu = plq.Gpu.new(local)
     if gpu is None:
         raise RuntimeError("no CUDA device")
     seed = SEED + rank
-    start, offset = plq.hot_start(seed, Q, N_SITES)
+    q = w[1]
+    start, offset = plq.hot_start(seed, q, N_SITES)
 
     # ---- device-resident throughput: K sweeps timed with CUDA events on the chain's stream
-    desc = plq.make_desc(plq.POTTS, Q, SHAPE, plq.HEATBATH, beta=BETA, seed=seed, rng=plq.RNG_STREAM,
-                         stream_offset=offset, sweeps_between=1, batch=plq.GPU_BATCH)
+    desc = _desc(plq, w, seed, offset)
     chain = plq.GpuChain(gpu, desc, start)
     stream = torch.cuda.ExternalStream(chain.cuda_stream, device=f"cuda:{local}")
     chain.advance(args.warmup)
@@ -189,10 +211,10 @@ def run_product(args):
     value = sites_total / (dev_ms_max * 1e6)  # site updates per ns
     ms_per_step = dev_ms_max / args.steps
     per_launch_ms = dev_ms / max(1, launches)
-    alg_bytes = BYTES_PER_UPDATE * N_SITES
+    alg_bytes = BYTES_PER_UPDATE * N_SITES // w[7]  # per launch
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic = profiled_traffic().get("fused3d_potts3_heatbath_stream_512", {}).get("dram_bytes_per_launch")
+    prof = profiled_traffic().get(args.workload, {})
 
     # ---- end to end through the public API: pinned host start in, samples and final state out
     pinned = torch.empty(N_SITES, dtype=torch.uint8).pin_memory()
@@ -202,11 +224,11 @@ def run_product(args):
     t0 = time.perf_counter()
     echain = plq.GpuChain(gpu, desc, pinned.numpy())
     _, prims = echain.next_batch(args.steps, states=False)
-    rc = plq.lib().plq_chain_read(echain._h, out_pinned.data_ptr())
-    plq.check(rc)
+    plq.check(plq.lib().plq_chain_read(echain._h, out_pinned.data_ptr()))
     t1 = time.perf_counter()
     e2e_s = max_over_ranks(pg, t1 - t0, local)
     e2e_value = sites_total / (e2e_s * 1e9)
+    n_prim = len(prims[0])
     echain.close()
 
     line = {
@@ -222,23 +244,24 @@ def run_product(args):
         "vs_baseline": None,
         "dtype": "u8",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sites_per_gpu": N_SITES, "step": "one sweep",
-                   "l2": "inputs larger than L2 (two 134 MB state buffers, out-of-place sweep)",
-                   "parallelism": f"independent lattice per GPU x{world}"},
+        "config": {"workload": w[5], "name": args.workload, "sites_per_gpu": N_SITES, "step": "one sweep",
+                   "l2": "inputs larger than L2 (134 MB state per lattice, two buffers for the out-of-place sweep)",
+                   "parallelism": f"independent lattice per GPU x{world}", "path": chain.path},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": alg_bytes, "kernel": "fused3d_kernel<3,true,true>"},
+                     "frac": round(achieved / peak, 4), "traffic": prof.get("dram_bytes_per_launch"),
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes, "kernel": w[6],
+                     "note": "instruction-issue bound: the reference's per-site RNG costs more issue slots than "
+                             "HBM allows at 2 B/update (see DESIGN.md)"},
         "e2e": {"value": round(e2e_value, 3), "unit": "site updates/ns",
                 "h2d_bytes_per_step": N_SITES / args.steps,
-                "d2h_bytes_per_step": 8 * (1 + Q) + N_SITES / args.steps,
-                "what": "chain create from pinned host start, K samples of one sweep each with device "
-                        "primaries read back (GPU_BATCH at a time), final configuration read back"},
+                "d2h_bytes_per_step": 8 * n_prim + N_SITES / args.steps,
+                "what": "chain create from a pinned host start, K samples of one sweep each with their device "
+                        "primaries read back (GPU_BATCH per round-trip), final configuration read back"},
         "gpu_launches": launches,
         "clocks": clock_info,
     }
     if rank == 0 and args.cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     chain.close()
@@ -246,39 +269,37 @@ def run_product(args):
         pg.destroy_process_group()
 
 
-def cpu_baseline(seconds: float, steps: int = 1):
-    """The reference CPU path (oracle restatement) on a bounded sample of the
-    same workload: colour-0 heat-bath updates over a slice of the 512^3
-    lattice, one thread (the reference has no threading)."""
-    import numpy as np
-
+def _oracle_setup(name):
     from oracle import oracle as o
 
+    w = WORKLOADS[name]
     lat = o.Lattice(SHAPE)
-    model = o.Model.potts(Q, 1.0)
+    model = o.Model.potts(w[1], 1.0) if w[0] == "potts" else o.Model.ising(1.0, 0.0)
+    kernel = o.HEATBATH if w[2] == "heatbath" else o.METROPOLIS
     rng = o.PcgStream(SEED)
-    cfg = o.hot_start(N_SITES, Q, rng)
-    # warm-up slice
-    o.local_site_slice(model, lat, cfg, o.HEATBATH, BETA, rng, 0, 0, 1 << 18)
-    lo = 1 << 18
-    chunk = 1 << 21
+    cfg = o.hot_start(N_SITES, w[1], rng)
+    return o, w, lat, model, kernel, rng, cfg
+
+
+def cpu_baseline(name: str, seconds: float):
+    """The reference CPU path (oracle restatement) on a bounded sample of the
+    same workload: colour-0 updates over slices of the 512^3 lattice, one
+    thread (the reference has no threading)."""
+    o, w, lat, model, kernel, rng, cfg = _oracle_setup(name)
+    o.local_site_slice(model, lat, cfg, kernel, w[4], rng, 0, 0, 1 << 18)  # warm-up
+    lo, chunk = 1 << 18, 1 << 21
     total_updates, total_t = 0, 0.0
-    times = []
-    while total_t < seconds or len(times) < steps:
+    while total_t < seconds:
         t0 = time.perf_counter()
-        n = o.local_site_slice(model, lat, cfg, o.HEATBATH, BETA, rng, 0, lo, lo + chunk)
-        dt = time.perf_counter() - t0
+        n = o.local_site_slice(model, lat, cfg, kernel, w[4], rng, 0, lo, lo + chunk)
+        total_t += time.perf_counter() - t0
         total_updates += n
-        total_t += dt
-        times.append(n / dt / 1e9)
         lo += chunk
         if lo + chunk > N_SITES:
             lo = 1 << 18
-    del lat
-    return {"value": round(total_updates / total_t / 1e9, 6), "unit": "site updates/ns", "cores": 1,
-            "kind": "port",
-            "sample": f"{total_updates} colour-0 heat-bath site updates of the 512^3 q=3 Potts lattice "
-                      f"in slices of {chunk} sites ({total_t:.1f} s)"}
+    return {"value": round(total_updates / total_t / 1e9, 6), "unit": "site updates/ns", "cores": 1, "kind": "port",
+            "sample": f"{total_updates} colour-0 site updates of the {name} workload in slices of {chunk} sites "
+                      f"({total_t:.1f} s, one thread)"}
 
 
 def run_reference(args):
@@ -286,20 +307,13 @@ def run_reference(args):
     rank = _env_int("RANK", 0)
     if rank != 0:
         return
-    import numpy as np
-
-    from oracle import oracle as o
-
-    lat = o.Lattice(SHAPE)
-    model = o.Model.potts(Q, 1.0)
-    rng = o.PcgStream(SEED)
-    cfg = o.hot_start(N_SITES, Q, rng)
+    o, w, lat, model, kernel, rng, cfg = _oracle_setup(args.workload)
     chunk = 1 << 20  # site indices per step: one bounded sample of a sweep
     lo = 0
 
     def step():
         nonlocal lo
-        n = o.local_site_slice(model, lat, cfg, o.HEATBATH, BETA, rng, 0, lo, lo + 2 * chunk)
+        n = o.local_site_slice(model, lat, cfg, kernel, w[4], rng, 0, lo, lo + 2 * chunk)
         lo = (lo + 2 * chunk) % (N_SITES - 2 * chunk)
         return n
 
@@ -314,10 +328,11 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "step": f"heat-bath updates of the colour-0 sites among {2 * chunk} "
-                                                 "consecutive site indices (a bounded sample of one sweep)"},
+        "config": {"workload": w[5], "name": args.workload,
+                   "step": f"updates of the colour-0 sites among {2 * chunk} consecutive site indices "
+                           "(a bounded sample of one sweep)"},
         "cpu_baseline": {"value": round(value, 6), "unit": "site updates/ns", "cores": 1, "kind": "port",
-                         "sample": f"{updates} site updates in {args.steps} steps"},
+                         "sample": f"{updates} site updates in {args.steps} steps, one thread"},
         "e2e": {"value": round(value, 6), "unit": "site updates/ns", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -330,6 +345,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--workload", default="potts3-512-hb-stream", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
