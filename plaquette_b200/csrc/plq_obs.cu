@@ -81,6 +81,94 @@ primaries_kernel(const uint8_t *state, Geom g, int model, int q, long long *out)
     }
 }
 
+// Fast path for site models with extent 0 a multiple of 16 and q <= 8: a
+// thread takes 16 consecutive sites as one 16-byte vector and counts with
+// SWAR popcounts -- disagreeing forward bonds (states differ in their low 3
+// bits), ones (Ising spin sum), and per-label counts.
+__device__ __forceinline__ uint32_t differ_bytes(uint32_t a, uint32_t b) {
+    uint32_t t = a ^ b;
+    return (t | (t >> 1) | (t >> 2)) & 0x01010101u;  // 1 per byte whose states differ (states < 8)
+}
+
+template <int D>
+__global__ void __launch_bounds__(kObsThreads)
+primaries_runs_kernel(const uint8_t *state, Geom g, int model, int q, long long *out) {
+    __shared__ long long s_acc[2 + 8];
+    if (threadIdx.x < 10) s_acc[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t n = g.n_sites;
+    const int64_t runs = n / 16;
+    long long disagree = 0, ones = 0;
+    long long cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < runs; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = r * 16;
+        int32_t x[D];
+        uint32_t t = (uint32_t)s;
+#pragma unroll
+        for (int mu = 0; mu < D; ++mu) {
+            uint32_t qq = fdiv(t, g.dm[mu], g.dl[mu]);
+            x[mu] = (int32_t)(t - qq * (uint32_t)g.L[mu]);
+            t = qq;
+        }
+        const uint4 C = *reinterpret_cast<const uint4 *>(state + s);
+        // +x: the byte after the run wraps to the row start at the end of a row
+        const int64_t nx = x[0] + 16 < g.L[0] ? s + 16 : s + 16 - g.L[0];
+        const uint32_t N0 = *reinterpret_cast<const uint32_t *>(state + nx);
+        const uint32_t w[5] = {C.x, C.y, C.z, C.w, N0};
+        int dif = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dif += __popc(differ_bytes(w[k], __funnelshift_r(w[k], w[k + 1], 8)));
+#pragma unroll
+        for (int mu = 1; mu < D; ++mu) {
+            const int64_t sp = x[mu] + 1 < g.L[mu] ? s + g.stride[mu] : s - (int64_t)(g.L[mu] - 1) * g.stride[mu];
+            const uint4 F = *reinterpret_cast<const uint4 *>(state + sp);
+            dif += __popc(differ_bytes(C.x, F.x)) + __popc(differ_bytes(C.y, F.y)) + __popc(differ_bytes(C.z, F.z)) +
+                   __popc(differ_bytes(C.w, F.w));
+        }
+        disagree += dif;
+        if (model == PLQ_ISING) {
+            ones += __popc(C.x) + __popc(C.y) + __popc(C.z) + __popc(C.w);
+        } else {
+            for (int a = 0; a < q; ++a) {
+                const uint32_t A = 0x01010101u * (uint32_t)a;
+                cnt[a] += 16 - __popc(differ_bytes(C.x, A)) - __popc(differ_bytes(C.y, A)) -
+                          __popc(differ_bytes(C.z, A)) - __popc(differ_bytes(C.w, A));
+            }
+        }
+    }
+    disagree = warp_sum(disagree);
+    ones = warp_sum(ones);
+    for (int a = 0; a < 8; ++a) cnt[a] = warp_sum(cnt[a]);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd((unsigned long long *)&s_acc[0], (unsigned long long)disagree);
+        atomicAdd((unsigned long long *)&s_acc[1], (unsigned long long)ones);
+        for (int a = 0; a < 8; ++a) atomicAdd((unsigned long long *)&s_acc[2 + a], (unsigned long long)cnt[a]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // per block: bonds = D * sites covered; out holds partial sums in the reference's form after the
+        // final fix-up kernel, so accumulate raw disagreements and ones here
+        atomicAdd((unsigned long long *)&out[0], (unsigned long long)s_acc[0]);
+        if (model == PLQ_ISING) {
+            atomicAdd((unsigned long long *)&out[1], (unsigned long long)s_acc[1]);
+        } else {
+            for (int a = 0; a < q; ++a) atomicAdd((unsigned long long *)&out[1 + a], (unsigned long long)s_acc[2 + a]);
+        }
+    }
+}
+
+// Raw counts -> the reference's integers: Ising bond_sum = bonds - 2*disagree,
+// spin_sum = n - 2*ones; Potts agree = bonds - disagree.
+__global__ void primaries_fixup_kernel(long long *out, int model, long long n_sites, int d) {
+    const long long bonds = n_sites * d;
+    if (model == PLQ_ISING) {
+        out[0] = bonds - 2 * out[0];
+        out[1] = n_sites - 2 * out[1];
+    } else {
+        out[0] = bonds - out[0];
+    }
+}
+
 int primaries_count(int model, int q) {
     if (model == PLQ_ISING) return 2;
     if (model == PLQ_POTTS) return 1 + q;
@@ -91,6 +179,18 @@ cudaError_t launch_primaries(const uint8_t *state, const Geom &g, int model, int
                              cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(long long) * primaries_count(model, q), stream);
     if (e != cudaSuccess) return e;
+    if (model != PLQ_GAUGE && q <= 8 && (g.d == 2 || g.d == 3) && g.L[0] % 16 == 0) {
+        const int64_t runs = g.n_sites / 16;
+        int64_t blocks = (runs + kObsThreads - 1) / kObsThreads;
+        if (blocks > 148 * 16) blocks = 148 * 16;
+        if (blocks < 1) blocks = 1;
+        if (g.d == 2)
+            primaries_runs_kernel<2><<<(unsigned)blocks, kObsThreads, 0, stream>>>(state, g, model, q, out);
+        else
+            primaries_runs_kernel<3><<<(unsigned)blocks, kObsThreads, 0, stream>>>(state, g, model, q, out);
+        primaries_fixup_kernel<<<1, 1, 0, stream>>>(out, model, (long long)g.n_sites, g.d);
+        return cudaGetLastError();
+    }
     int64_t blocks = (g.n_sites + kObsThreads - 1) / kObsThreads;
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
