@@ -141,13 +141,19 @@ def dist_setup():
 
 
 def max_over_ranks(pg, value, device):
+    """Max of a per-rank time over all ranks (device None: a CPU tensor, for gloo)."""
     if pg is None:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{device}")
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{device}" if device is not None else "cpu")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(world, sites_per_rank, steps, max_ms):
+    """Whole-job site updates per ns: every rank's sites over the slowest rank's time."""
+    return sites_per_rank * world * steps / (max_ms * 1e6)
 
 
 def barrier(pg, device):
@@ -208,7 +214,7 @@ def run_product(args):
     barrier(pg, local)
 
     sites_total = N_SITES * world * args.steps
-    value = sites_total / (dev_ms_max * 1e6)  # site updates per ns
+    value = whole_job_rate(world, N_SITES, args.steps, dev_ms_max)
     ms_per_step = dev_ms_max / args.steps
     per_launch_ms = dev_ms / max(1, launches)
     alg_bytes = BYTES_PER_UPDATE * N_SITES // w[7]  # per launch
