@@ -19,6 +19,7 @@
 #include "plq_device.cuh"
 #include "plq_fused.h"
 #include "plq_local.h"
+#include "plq_scan.h"
 #include "plq_tables.h"
 
 using namespace plq;
@@ -477,7 +478,33 @@ int local_sweep(plq_chain *c) {
         } else if (c->desc.rng == PLQ_RNG_STREAM) {
             a.pass_offset = c->host_pos + (uint64_t)pass * (uint64_t)half;
         }
-        cudaError_t e = launch_local_pass(a, c->link, c->lookback, c->stream);
+        cudaError_t e;
+        if (c->lookback && !c->link && c->q == 2 && !(c->desc.flags & PLQ_FLAG_NO_FUSED) &&
+            scan_metro_eligible(c->d, c->g.L)) {
+            // q = 2 sites in 2D/3D: the vectorised look-back pass (same draws, same result)
+            ScanArgs s;
+            std::memset(&s, 0, sizeof s);
+            s.state = c->d_state;
+            s.n_sites = c->n_sites;
+            s.L0 = c->g.L[0];
+            s.L1 = c->g.L[1];
+            s.L2 = c->g.L[2];
+            s.color = a.color;
+            s.metro53 = c->d_metro53;
+            s.table_entries = (int)env_key_count(model_params(&c->desc));
+            s.jump = c->d_jump;
+            s.base = c->base;
+            s.inc = c->inc;
+            s.ctrl = c->d_ctrl;
+            s.desc = c->d_desc;
+            s.n_chunks = c->n_chunks;
+            s.ticket_base = a.ticket_base;
+            s.epoch = a.epoch;
+            s.pos_in = a.pos_in;
+            e = launch_scan_metro(s, c->d, c->stream);
+        } else {
+            e = launch_local_pass(a, c->link, c->lookback, c->stream);
+        }
         c->launches++;
         if (e != cudaSuccess) return cuda_fail(e, "local pass launch");
     }

@@ -1,0 +1,211 @@
+// plq_scan.cu -- one colour pass of q = 2 checkerboard Metropolis on the PCG
+// stream for 2D/3D site lattices with extent 0 a multiple of 16.
+//
+// Same semantics as the generic look-back pass (plq_local_impl.cuh): a
+// variable draws only when its move is uphill (src/updater.rs:90), so its draw
+// position is the count of uphill variables of the colour before it in index
+// order -- a device-wide exclusive scan, done in one pass with decoupled
+// look-back over chunks taken in ticket order.  What this kernel changes is
+// the cost per site:
+//   * a thread owns 16 consecutive sites (one 16-byte vector, 8 of the pass's
+//     colour); neighbour words come as vectors (+-y, +-z) and 4-byte words
+//     (+-x across the vector's ends), and the table keys of all 16 sites are
+//     computed four at a time in 32-bit words (SWAR: key = cur + 2 * sum of
+//     neighbour states, no byte ever carries);
+//   * the chunk's first thread jumps the PCG stream to the chunk's position
+//     once (8 radix-256 digits); every thread then jumps from there by its
+//     local exclusive count (< 2^16: at most 2 digits) and steps the LCG.
+#include <cuda_runtime.h>
+
+#include "../../include/plaquette.h"
+#include "plq_device.cuh"
+#include "plq_scan.h"
+
+namespace plq {
+
+constexpr int SThreads = 256;
+constexpr int SSites = 16;  // sites per thread
+constexpr int SChunkSites = SThreads * SSites;
+constexpr int SSpinLimit = 1 << 22;
+
+__device__ __forceinline__ unsigned long long s_ld_relaxed(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long s_make_desc(uint32_t epoch, unsigned long long st, uint32_t value) {
+    return ((unsigned long long)(epoch & 0x3FFFFFFFu) << 34) | (st << 32) | value;
+}
+
+// jump by a small count (< 2^16): the two low radix-256 digits
+__device__ __forceinline__ u128 jump_small(const Affine *table, u128 s, uint32_t n) {
+    uint32_t v0 = n & 255u, v1 = (n >> 8) & 255u;
+    if (v0) s = apply(table[v0], s);
+    if (v1) s = apply(table[kJumpRadix + v1], s);
+    return s;
+}
+
+template <int D>
+__global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
+    __shared__ unsigned long long s_ticket;
+    __shared__ uint64_t s_tab[64];
+    __shared__ int warp_tot[SThreads / 32];
+    __shared__ unsigned long long s_excl, s_base;
+    __shared__ u128 s_chunk_state;
+    __shared__ int s_fail;
+
+    if (threadIdx.x < a.table_entries) s_tab[threadIdx.x] = a.metro53[threadIdx.x];
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&a.ctrl->ticket, 1ull) - a.ticket_base;
+    __syncthreads();
+    const int64_t chunk = (int64_t)s_ticket;
+    if (chunk >= a.n_chunks) {
+        if (threadIdx.x == 0) atomicOr(&a.ctrl->status, kStatusBounds);
+        return;
+    }
+    const int64_t n = a.n_sites;
+    const int64_t s0 = chunk * SChunkSites + (int64_t)threadIdx.x * SSites;
+    const bool active = s0 < n;
+
+    // ---- keys of the 16 sites
+    uint32_t C[4] = {0, 0, 0, 0}, K[4] = {0, 0, 0, 0};
+    uint32_t need_mask = 0;  // bit i: colour site i (0..7) draws
+    uint64_t entry[8];
+    int b = 0;
+    if (active) {
+        // coordinates of the vector's first site (x multiple of 16)
+        const uint32_t row = (uint32_t)(s0 / a.L0);
+        const uint32_t x0 = (uint32_t)(s0 - (int64_t)row * a.L0);
+        uint32_t y = row, z = 0;
+        if (D == 3) {
+            z = row / (uint32_t)a.L1;
+            y = row - z * (uint32_t)a.L1;
+        }
+        const uint4 c4 = *reinterpret_cast<const uint4 *>(a.state + s0);
+        C[0] = c4.x;
+        C[1] = c4.y;
+        C[2] = c4.z;
+        C[3] = c4.w;
+        const int64_t rs = s0 - x0;  // row start
+        const uint32_t Lw = *reinterpret_cast<const uint32_t *>(a.state + rs + (x0 == 0 ? a.L0 - 4 : x0 - 4));
+        const uint32_t Rw = *reinterpret_cast<const uint32_t *>(a.state + rs + (x0 + 16 == (uint32_t)a.L0 ? 0 : x0 + 16));
+        const int64_t sy = (int64_t)a.L0;
+        const uint4 up = *reinterpret_cast<const uint4 *>(a.state + (y + 1 < (uint32_t)a.L1 ? s0 + sy : s0 - sy * (a.L1 - 1)));
+        const uint4 dn = *reinterpret_cast<const uint4 *>(a.state + (y > 0 ? s0 - sy : s0 + sy * (a.L1 - 1)));
+        uint32_t U[4] = {up.x, up.y, up.z, up.w}, Dn[4] = {dn.x, dn.y, dn.z, dn.w};
+        uint32_t Zp[4] = {0, 0, 0, 0}, Zm[4] = {0, 0, 0, 0};
+        if (D == 3) {
+            const int64_t sz = (int64_t)a.L0 * a.L1;
+            const uint4 zp = *reinterpret_cast<const uint4 *>(a.state + (z + 1 < (uint32_t)a.L2 ? s0 + sz : s0 - sz * (a.L2 - 1)));
+            const uint4 zm = *reinterpret_cast<const uint4 *>(a.state + (z > 0 ? s0 - sz : s0 + sz * (a.L2 - 1)));
+            Zp[0] = zp.x; Zp[1] = zp.y; Zp[2] = zp.z; Zp[3] = zp.w;
+            Zm[0] = zm.x; Zm[1] = zm.y; Zm[2] = zm.z; Zm[3] = zm.w;
+        }
+        const uint32_t W[6] = {Lw, C[0], C[1], C[2], C[3], Rw};
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            uint32_t l = __funnelshift_l(W[w], W[w + 1], 8);
+            uint32_t r = __funnelshift_r(W[w + 1], W[w + 2], 8);
+            uint32_t s = l + r + U[w] + Dn[w] + Zp[w] + Zm[w];
+            K[w] = C[w] + 2u * s;
+        }
+        // the pass's colour sits at byte offsets b, b+2, ... (x0 even)
+        b = (int)((a.color + y + z) & 1u);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int j = b + 2 * i;
+            const uint32_t key = (K[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+            entry[i] = s_tab[key];
+            if (entry[i] != ~0ull) need_mask |= 1u << i;
+        }
+    }
+    const int need = __popc(need_mask);
+
+    // ---- block scan + decoupled look-back
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = need;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    if (threadIdx.x == 0) s_fail = 0;
+    __syncthreads();
+    int warp_excl = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < SThreads / 32; ++w) {
+        int t = warp_tot[w];
+        if (w < wid) warp_excl += t;
+        total += t;
+    }
+    const int thread_excl = warp_excl + incl - need;
+    if (threadIdx.x == 0) {
+        unsigned long long excl = 0;
+        if (chunk == 0) {
+            atomicExch(&a.desc[0], s_make_desc(a.epoch, 2ull, (uint32_t)total));
+        } else {
+            atomicExch(&a.desc[chunk], s_make_desc(a.epoch, 1ull, (uint32_t)total));
+            int64_t j = chunk - 1;
+            int spins = 0;
+            while (j >= 0) {
+                unsigned long long d = s_ld_relaxed(&a.desc[j]);
+                uint32_t ep = (uint32_t)(d >> 34);
+                unsigned long long st = (d >> 32) & 3ull;
+                if (ep != (a.epoch & 0x3FFFFFFFu) || st == 0) {
+                    if (++spins > SSpinLimit) {
+                        s_fail = 1;
+                        atomicOr(&a.ctrl->status, kStatusLookbackTimeout);
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                excl += (uint32_t)d;
+                if (st == 2ull) break;
+                --j;
+            }
+            if (!s_fail) atomicExch(&a.desc[chunk], s_make_desc(a.epoch, 2ull, (uint32_t)(excl + total)));
+        }
+        s_excl = excl;
+        s_base = a.ctrl->pos[a.pos_in];
+        if (chunk == a.n_chunks - 1 && !s_fail) a.ctrl->pos[a.pos_in ^ 1] = s_base + excl + (unsigned long long)total;
+        if (!s_fail) s_chunk_state = jump(a.jump, a.base, s_base + excl);
+    }
+    __syncthreads();
+    if (s_fail || !active) return;
+
+    // ---- draws and decisions
+    u128 st = jump_small(a.jump, s_chunk_state, (uint32_t)thread_excl);
+    uint32_t flip[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int j = b + 2 * i;
+        bool accept;
+        if ((need_mask >> i) & 1u) {
+            uint64_t k = draw53(st);
+            st = pcg_step(st, a.inc);
+            accept = k < entry[i];
+        } else {
+            accept = true;  // downhill: accept without a draw
+        }
+        flip[j >> 2] |= (accept ? 1u : 0u) << (8 * (j & 3));
+    }
+    uint4 out = make_uint4(C[0] ^ flip[0], C[1] ^ flip[1], C[2] ^ flip[2], C[3] ^ flip[3]);
+    *reinterpret_cast<uint4 *>(a.state + s0) = out;
+}
+
+bool scan_metro_eligible(int d, const int32_t *L) {
+    return (d == 2 || d == 3) && L[0] % 16 == 0 && L[0] >= 16;
+}
+
+int64_t scan_chunks(int64_t n_sites) { return (n_sites + SChunkSites - 1) / SChunkSites; }
+
+cudaError_t launch_scan_metro(const ScanArgs &a, int d, cudaStream_t stream) {
+    if (d == 2)
+        scan_metro_kernel<2><<<(unsigned)a.n_chunks, SThreads, 0, stream>>>(a);
+    else
+        scan_metro_kernel<3><<<(unsigned)a.n_chunks, SThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace plq

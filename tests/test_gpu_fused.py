@@ -58,3 +58,20 @@ def test_fused_equals_pass_kernels(gpu, mode):
     assert np.array_equal(outs[0], outs[2 if rng == plq.RNG_STREAM else 1])
     if rng == plq.RNG_STREAM:
         assert outs[1] == outs[3] == off + 6 * n
+
+
+@pytest.mark.parametrize("shape,beta", [((512, 64, 32), 0.2216544), ((1024, 512), 0.4406868), ((48, 32, 16), 0.3)],
+                         ids=str)
+def test_vector_scan_pass_equals_generic_lookback(gpu, shape, beta):
+    """The vectorised stream-Metropolis pass (plq_scan.cu) against the
+    generic look-back pass: same configurations, same stream position."""
+    n = int(np.prod(shape))
+    start, off = plq.hot_start(5, 2, n)
+    outs = []
+    for flags in (0, plq.FLAG_NO_FUSED):
+        d = plq.make_desc(plq.ISING, 2, shape, plq.METROPOLIS, beta=beta, h=0.05, seed=5, rng=plq.RNG_STREAM,
+                          stream_offset=off, sweeps_between=4, batch=1, flags=flags)
+        c = plq.GpuChain(gpu, d, start)
+        outs.append((next(c), c.stream_position()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1]
