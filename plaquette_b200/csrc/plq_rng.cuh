@@ -58,7 +58,7 @@ struct Affine {
     u128 m, p;
 };
 
-PLQ_HD u128 apply(const Affine &f, u128 s) { return add128(mul128(f.m, s), f.p); }
+PLQ_HD u128 apply(const Affine &f, u128 s);
 
 // g after f: s -> g(f(s)).
 PLQ_HD Affine compose(const Affine &f, const Affine &g) {
@@ -73,11 +73,87 @@ PLQ_HD uint64_t rotr64(uint64_t x, unsigned r) {
     return r ? (x >> r) | (x << (64u - r)) : x;
 }
 
+#if defined(__CUDA_ARCH__)
+// Device forms of the two per-draw operations, written on 32-bit limbs: the
+// generic 64-bit expressions above compile to wide-multiply-high sequences and
+// compare-based carries that load the integer ALU pipe.
+
+// m*s + p (mod 2^128) as carry chains of 32-bit multiply-adds: the ten limb
+// products s_i*m_j with i + j <= 3 (high halves where i + j <= 2), with p as
+// the initial accumulator.
+__device__ __forceinline__ u128 muladd128_limbs(u128 m, u128 s, u128 p) {
+    const uint32_t s0 = (uint32_t)s.lo, s1 = (uint32_t)(s.lo >> 32), s2 = (uint32_t)s.hi,
+                   s3 = (uint32_t)(s.hi >> 32);
+    const uint32_t m0 = (uint32_t)m.lo, m1 = (uint32_t)(m.lo >> 32), m2 = (uint32_t)m.hi,
+                   m3 = (uint32_t)(m.hi >> 32);
+    const uint32_t i0 = (uint32_t)p.lo, i1 = (uint32_t)(p.lo >> 32), i2 = (uint32_t)p.hi,
+                   i3 = (uint32_t)(p.hi >> 32);
+    uint32_t r0, r1, r2, r3;
+    asm("{\n\t"
+        "mad.lo.cc.u32  %0, %4, %8, %12;\n\t"   // s0*m0 + p (cols 0..1), s0*m2 (cols 2..3)
+        "madc.hi.cc.u32 %1, %4, %8, %13;\n\t"
+        "madc.lo.cc.u32 %2, %4, %10, %14;\n\t"
+        "madc.hi.u32    %3, %4, %10, %15;\n\t"
+        "mad.lo.cc.u32  %1, %4, %9, %1;\n\t"    // s0*m1 (cols 1..2), s0*m3 (col 3)
+        "madc.hi.cc.u32 %2, %4, %9, %2;\n\t"
+        "madc.lo.u32    %3, %4, %11, %3;\n\t"
+        "mad.lo.cc.u32  %1, %5, %8, %1;\n\t"    // s1*m0 (cols 1..2), s1*m2 (col 3)
+        "madc.hi.cc.u32 %2, %5, %8, %2;\n\t"
+        "madc.lo.u32    %3, %5, %10, %3;\n\t"
+        "mad.lo.cc.u32  %2, %5, %9, %2;\n\t"    // s1*m1 (cols 2..3)
+        "madc.hi.u32    %3, %5, %9, %3;\n\t"
+        "mad.lo.cc.u32  %2, %6, %8, %2;\n\t"    // s2*m0 (cols 2..3)
+        "madc.hi.u32    %3, %6, %8, %3;\n\t"
+        "mad.lo.u32     %3, %6, %9, %3;\n\t"    // s2*m1 (col 3)
+        "mad.lo.u32     %3, %7, %8, %3;\n\t"    // s3*m0 (col 3)
+        "}"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"(s0), "r"(s1), "r"(s2), "r"(s3), "r"(m0), "r"(m1), "r"(m2), "r"(m3), "r"(i0), "r"(i1), "r"(i2),
+          "r"(i3));
+    u128 r;
+    r.lo = ((uint64_t)r1 << 32) | r0;
+    r.hi = ((uint64_t)r3 << 32) | r2;
+    return r;
+}
+
+// XSL-RR with the 64-bit rotation as two funnel shifts: rotating by r >= 32
+// is a word swap followed by a rotation by r - 32.
+__device__ __forceinline__ uint64_t xsl_rr_limbs(u128 s) {
+    const uint32_t x0 = (uint32_t)s.lo ^ (uint32_t)s.hi;
+    const uint32_t x1 = (uint32_t)(s.lo >> 32) ^ (uint32_t)(s.hi >> 32);
+    const uint32_t r = (uint32_t)(s.hi >> 58);
+    const bool swap = (r & 32u) != 0;
+    const uint32_t a = swap ? x1 : x0, b = swap ? x0 : x1;
+    const uint32_t o0 = __funnelshift_r(a, b, r), o1 = __funnelshift_r(b, a, r);
+    return ((uint64_t)o1 << 32) | o0;
+}
+#endif
+
+PLQ_HD u128 apply(const Affine &f, u128 s) {
+#if defined(__CUDA_ARCH__)
+    return muladd128_limbs(f.m, s, f.p);
+#else
+    return add128(mul128(f.m, s), f.p);
+#endif
+}
+
 // XSL-RR output of a 128-bit state.
-PLQ_HD uint64_t xsl_rr(u128 s) { return rotr64(s.hi ^ s.lo, (unsigned)(s.hi >> 58)); }
+PLQ_HD uint64_t xsl_rr(u128 s) {
+#if defined(__CUDA_ARCH__)
+    return xsl_rr_limbs(s);
+#else
+    return rotr64(s.hi ^ s.lo, (unsigned)(s.hi >> 58));
+#endif
+}
 
 // One LCG step.
-PLQ_HD u128 pcg_step(u128 s, u128 inc) { return add128(mul128(s, pcg_mult()), inc); }
+PLQ_HD u128 pcg_step(u128 s, u128 inc) {
+#if defined(__CUDA_ARCH__)
+    return muladd128_limbs(pcg_mult(), s, inc);
+#else
+    return add128(mul128(s, pcg_mult()), inc);
+#endif
+}
 
 // 53-bit integer behind rand's next_f64: the draw is (k * 2^-53).
 PLQ_HD uint64_t draw53(u128 state_after_step) { return xsl_rr(state_after_step) >> 11; }
