@@ -56,21 +56,21 @@ __device__ __forceinline__ uint32_t gw(uint32_t w) {
     return w;
 }
 
-// Keys of the 4 sites of word C given its six neighbour words.
+// Keys of the 4 sites of word C given its six neighbour words.  For q = 3,
+// sum g = raw + 5*hi with hi the per-byte count of state-2 neighbours; the
+// masked bits (value 2 per state-2 neighbour) are summed first and the key is
+// C + 3*raw + 15*hi2/2, where each byte of 15*hi2 is even and at most 180, so
+// the final shift moves no bit across a byte boundary.
 template <int Q>
 __device__ __forceinline__ uint32_t key_word(uint32_t C, uint32_t l, uint32_t r, uint32_t u, uint32_t d,
                                              uint32_t m, uint32_t p) {
-    uint32_t s;
+    const uint32_t raw = l + r + u + d + m + p;
     if (Q == 3) {
-        const uint32_t M = 0x01010101u;
-        uint32_t raw = l + r + u + d + m + p;
-        uint32_t hi = ((l >> 1) & M) + ((r >> 1) & M) + ((u >> 1) & M) + ((d >> 1) & M) + ((m >> 1) & M) +
-                      ((p >> 1) & M);
-        s = raw + hi * 5u;
-    } else {
-        s = l + r + u + d + m + p;
+        const uint32_t M2 = 0x02020202u;
+        const uint32_t hi2 = (l & M2) + (r & M2) + (u & M2) + (d & M2) + (m & M2) + (p & M2);
+        return C + raw * 3u + ((hi2 * 15u) >> 1);
     }
-    return C + s * (uint32_t)Q;
+    return C + raw * (uint32_t)Q;
 }
 
 // Table decision for one site; returns the new state.
@@ -78,10 +78,11 @@ template <int Q, bool STREAM, bool HB>
 __device__ __forceinline__ uint32_t decide(const uint8_t *tab, uint32_t key, uint32_t cur, uint64_t k) {
     if (HB) {
         if (STREAM) {
-            const uint64_t *cut = reinterpret_cast<const uint64_t *>(tab) + key * (Q - 1);
-            uint32_t ch = k >= cut[0] ? 1u : 0u;
-            if (Q == 3) ch += k >= cut[1] ? 1u : 0u;
-            return ch;
+            if (Q == 3) {  // both cut points of a key in one 16-byte load
+                const ulonglong2 cut = reinterpret_cast<const ulonglong2 *>(tab)[key];
+                return (k >= cut.x ? 1u : 0u) + (k >= cut.y ? 1u : 0u);
+            }
+            return k >= reinterpret_cast<const uint64_t *>(tab)[key] ? 1u : 0u;
         } else {
             const uint32_t *cut = reinterpret_cast<const uint32_t *>(tab) + key * (Q - 1);
             uint32_t k32 = (uint32_t)k;
@@ -95,16 +96,19 @@ __device__ __forceinline__ uint32_t decide(const uint8_t *tab, uint32_t key, uin
     }
 }
 
-// Updates the colour-c sites (byte offsets b, b+2) of one 32-bit word in place.
+// Updates the colour-c sites (byte offsets b, b+2) of one 32-bit word in place:
+// the word and its keys are shifted by b bytes once, so both sites sit at fixed
+// byte offsets 0 and 2.
 template <int Q, bool STREAM, bool HB>
 __device__ __forceinline__ uint32_t update_word(const FusedArgs &a, const uint8_t *tab, uint32_t C, uint32_t K,
                                                 int b, uint32_t var0, u128 &st) {
-    uint32_t out = C;
+    const uint32_t sh = 8u * (uint32_t)b;
+    const uint32_t Cs = C >> sh, Ks = K >> sh;
+    uint32_t delta = 0;
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-        uint32_t sh = 8u * (uint32_t)(b + 2 * i);
-        uint32_t key = (K >> sh) & 0xFFu;
-        uint32_t cur = (C >> sh) & 0xFFu;
+        const uint32_t key = (Ks >> (16 * i)) & 0xFFu;
+        const uint32_t cur = (Cs >> (16 * i)) & 0xFFu;
         uint64_t k;
         if (STREAM) {
             k = draw53(st);
@@ -112,10 +116,10 @@ __device__ __forceinline__ uint32_t update_word(const FusedArgs &a, const uint8_
         } else {
             k = keyed24(a.seed32, var0 + (uint32_t)(b + 2 * i), a.sweep32);
         }
-        uint32_t nv = decide<Q, STREAM, HB>(tab, key, cur, k);
-        out ^= (nv ^ cur) << sh;
+        const uint32_t nv = decide<Q, STREAM, HB>(tab, key, cur, k);
+        delta |= (nv ^ cur) << (16 * i);
     }
-    return out;
+    return C ^ (delta << sh);
 }
 
 // A run of 16 bytes at x offset xr of smem row `row` (plane c, neighbours in
