@@ -83,23 +83,28 @@ primaries_kernel(const uint8_t *state, Geom g, int model, int q, long long *out)
 
 // Fast path for site models with extent 0 a multiple of 16 and q <= 8: a
 // thread takes 16 consecutive sites as one 16-byte vector and counts with
-// SWAR popcounts -- disagreeing forward bonds (states differ in their low 3
-// bits), ones (Ising spin sum), and per-label counts.
+// SWAR popcounts -- disagreeing forward bonds, ones (Ising spin sum), and
+// per-label counts -- in 32-bit per-thread registers (Q = 0: Ising; Q = 2..8:
+// Potts with q = Q; the label counts come from the state bits for Q <= 4).
+template <int Q>
 __device__ __forceinline__ uint32_t differ_bytes(uint32_t a, uint32_t b) {
-    uint32_t t = a ^ b;
-    return (t | (t >> 1) | (t >> 2)) & 0x01010101u;  // 1 per byte whose states differ (states < 8)
+    const uint32_t t = a ^ b;
+    if (Q <= 2) return t;                                  // states 0/1: bit 0 only
+    if (Q <= 4) return (t | (t >> 1)) & 0x01010101u;       // states < 4
+    return (t | (t >> 1) | (t >> 2)) & 0x01010101u;        // states < 8
 }
 
-template <int D>
-__global__ void __launch_bounds__(kObsThreads)
-primaries_runs_kernel(const uint8_t *state, Geom g, int model, int q, long long *out) {
-    __shared__ long long s_acc[2 + 8];
-    if (threadIdx.x < 10) s_acc[threadIdx.x] = 0;
+template <int D, int Q>
+__global__ void __launch_bounds__(kObsThreads) primaries_runs_kernel(const uint8_t *state, Geom g, long long *out) {
+    constexpr int NC = Q == 0 ? 1 : Q;  // Ising: ones; Potts: one count per label
+    __shared__ unsigned long long s_acc[1 + NC];
+    if (threadIdx.x < 1 + NC) s_acc[threadIdx.x] = 0;
     __syncthreads();
-    const int64_t n = g.n_sites;
-    const int64_t runs = n / 16;
-    long long disagree = 0, ones = 0;
-    long long cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int64_t runs = g.n_sites / 16;
+    uint32_t disagree = 0;
+    uint32_t cnt[NC];
+#pragma unroll
+    for (int a = 0; a < NC; ++a) cnt[a] = 0;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < runs; r += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = r * 16;
         int32_t x[D];
@@ -115,45 +120,73 @@ primaries_runs_kernel(const uint8_t *state, Geom g, int model, int q, long long 
         const int64_t nx = x[0] + 16 < g.L[0] ? s + 16 : s + 16 - g.L[0];
         const uint32_t N0 = *reinterpret_cast<const uint32_t *>(state + nx);
         const uint32_t w[5] = {C.x, C.y, C.z, C.w, N0};
-        int dif = 0;
+        uint32_t dif = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) dif += __popc(differ_bytes(w[k], __funnelshift_r(w[k], w[k + 1], 8)));
+        for (int k = 0; k < 4; ++k) dif += __popc(differ_bytes<Q>(w[k], __funnelshift_r(w[k], w[k + 1], 8)));
 #pragma unroll
         for (int mu = 1; mu < D; ++mu) {
             const int64_t sp = x[mu] + 1 < g.L[mu] ? s + g.stride[mu] : s - (int64_t)(g.L[mu] - 1) * g.stride[mu];
             const uint4 F = *reinterpret_cast<const uint4 *>(state + sp);
-            dif += __popc(differ_bytes(C.x, F.x)) + __popc(differ_bytes(C.y, F.y)) + __popc(differ_bytes(C.z, F.z)) +
-                   __popc(differ_bytes(C.w, F.w));
+            dif += __popc(differ_bytes<Q>(C.x, F.x)) + __popc(differ_bytes<Q>(C.y, F.y)) +
+                   __popc(differ_bytes<Q>(C.z, F.z)) + __popc(differ_bytes<Q>(C.w, F.w));
         }
         disagree += dif;
-        if (model == PLQ_ISING) {
-            ones += __popc(C.x) + __popc(C.y) + __popc(C.z) + __popc(C.w);
+        const uint32_t M = 0x01010101u;
+        if (Q <= 2) {  // Ising ones, or Potts q = 2 label 1; label 0 is the rest
+            const uint32_t ones = __popc(C.x) + __popc(C.y) + __popc(C.z) + __popc(C.w);
+            cnt[NC - 1] += ones;
+            if (Q == 2) cnt[0] += 16u - ones;
+        } else if (Q <= 4) {
+            const uint32_t b0 = __popc(C.x & M) + __popc(C.y & M) + __popc(C.z & M) + __popc(C.w & M);
+            const uint32_t b1 = __popc((C.x >> 1) & M) + __popc((C.y >> 1) & M) + __popc((C.z >> 1) & M) +
+                                __popc((C.w >> 1) & M);
+            uint32_t c3 = 0;
+            if (Q == 4)
+                c3 = __popc(C.x & (C.x >> 1) & M) + __popc(C.y & (C.y >> 1) & M) + __popc(C.z & (C.z >> 1) & M) +
+                     __popc(C.w & (C.w >> 1) & M);
+            cnt[1] += b0 - c3;
+            cnt[2] += b1 - c3;
+            if (Q == 4) cnt[3 % NC] += c3;
+            cnt[0] += 16u - b0 - b1 + c3;
         } else {
-            for (int a = 0; a < q; ++a) {
-                const uint32_t A = 0x01010101u * (uint32_t)a;
-                cnt[a] += 16 - __popc(differ_bytes(C.x, A)) - __popc(differ_bytes(C.y, A)) -
-                          __popc(differ_bytes(C.z, A)) - __popc(differ_bytes(C.w, A));
+#pragma unroll
+            for (int a = 0; a < Q; ++a) {
+                const uint32_t A = M * (uint32_t)a;
+                cnt[a] += 16u - __popc(differ_bytes<Q>(C.x, A)) - __popc(differ_bytes<Q>(C.y, A)) -
+                          __popc(differ_bytes<Q>(C.z, A)) - __popc(differ_bytes<Q>(C.w, A));
             }
         }
     }
-    disagree = warp_sum(disagree);
-    ones = warp_sum(ones);
-    for (int a = 0; a < 8; ++a) cnt[a] = warp_sum(cnt[a]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) disagree += __shfl_down_sync(0xffffffffu, disagree, off);
+#pragma unroll
+    for (int a = 0; a < NC; ++a)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) cnt[a] += __shfl_down_sync(0xffffffffu, cnt[a], off);
     if ((threadIdx.x & 31) == 0) {
-        atomicAdd((unsigned long long *)&s_acc[0], (unsigned long long)disagree);
-        atomicAdd((unsigned long long *)&s_acc[1], (unsigned long long)ones);
-        for (int a = 0; a < 8; ++a) atomicAdd((unsigned long long *)&s_acc[2 + a], (unsigned long long)cnt[a]);
+        atomicAdd(&s_acc[0], (unsigned long long)disagree);
+#pragma unroll
+        for (int a = 0; a < NC; ++a) atomicAdd(&s_acc[1 + a], (unsigned long long)cnt[a]);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        // per block: bonds = D * sites covered; out holds partial sums in the reference's form after the
-        // final fix-up kernel, so accumulate raw disagreements and ones here
-        atomicAdd((unsigned long long *)&out[0], (unsigned long long)s_acc[0]);
-        if (model == PLQ_ISING) {
-            atomicAdd((unsigned long long *)&out[1], (unsigned long long)s_acc[1]);
-        } else {
-            for (int a = 0; a < q; ++a) atomicAdd((unsigned long long *)&out[1 + a], (unsigned long long)s_acc[2 + a]);
-        }
+    if (threadIdx.x < 1 + NC) atomicAdd((unsigned long long *)&out[threadIdx.x], s_acc[threadIdx.x]);
+}
+
+template <int D>
+static void launch_runs(unsigned blocks, cudaStream_t stream, const uint8_t *state, const Geom &g, int model, int q,
+                        long long *out) {
+    if (model == PLQ_ISING) {
+        primaries_runs_kernel<D, 0><<<blocks, kObsThreads, 0, stream>>>(state, g, out);
+        return;
+    }
+    switch (q) {
+        case 2: primaries_runs_kernel<D, 2><<<blocks, kObsThreads, 0, stream>>>(state, g, out); break;
+        case 3: primaries_runs_kernel<D, 3><<<blocks, kObsThreads, 0, stream>>>(state, g, out); break;
+        case 4: primaries_runs_kernel<D, 4><<<blocks, kObsThreads, 0, stream>>>(state, g, out); break;
+        case 5: primaries_runs_kernel<D, 5><<<blocks, kObsThreads, 0, stream>>>(state, g, out); break;
+        case 6: primaries_runs_kernel<D, 6><<<blocks, kObsThreads, 0, stream>>>(state, g, out); break;
+        case 7: primaries_runs_kernel<D, 7><<<blocks, kObsThreads, 0, stream>>>(state, g, out); break;
+        default: primaries_runs_kernel<D, 8><<<blocks, kObsThreads, 0, stream>>>(state, g, out); break;
     }
 }
 
@@ -185,9 +218,9 @@ cudaError_t launch_primaries(const uint8_t *state, const Geom &g, int model, int
         if (blocks > 148 * 16) blocks = 148 * 16;
         if (blocks < 1) blocks = 1;
         if (g.d == 2)
-            primaries_runs_kernel<2><<<(unsigned)blocks, kObsThreads, 0, stream>>>(state, g, model, q, out);
+            launch_runs<2>((unsigned)blocks, stream, state, g, model, q, out);
         else
-            primaries_runs_kernel<3><<<(unsigned)blocks, kObsThreads, 0, stream>>>(state, g, model, q, out);
+            launch_runs<3>((unsigned)blocks, stream, state, g, model, q, out);
         primaries_fixup_kernel<<<1, 1, 0, stream>>>(out, model, (long long)g.n_sites, g.d);
         return cudaGetLastError();
     }

@@ -159,6 +159,24 @@ def test_primaries_match_oracle(oracle, gpu):
         assert list(chain.primaries()) == list(model.primaries(lat, want))
 
 
+@pytest.mark.parametrize("shape", [(32, 6), (16, 4, 6), (48, 2, 2)])
+@pytest.mark.parametrize("q", [0, 2, 3, 4, 5, 6, 7, 8])
+def test_vector_primaries_match_oracle(oracle, gpu, q, shape):
+    # extent 0 a multiple of 16: the 16-site vector counting path, every label count
+    n = int(np.prod(shape))
+    rng = np.random.default_rng(100 + q)
+    for trial in range(3):
+        if q == 0:
+            kind, qq, model = plq.ISING, 2, oracle.Model.ising(1.0, 0.0)
+        else:
+            kind, qq, model = plq.POTTS, q, oracle.Model.potts(q, 1.0)
+        start = rng.integers(0, qq, n).astype(np.uint8) if trial else np.full(n, qq - 1, np.uint8)
+        d = plq.make_desc(kind, qq, shape, plq.METROPOLIS, beta=0.5, seed=1, rng=plq.RNG_KEYED)
+        chain = plq.GpuChain(gpu, d, start)
+        assert list(chain.primaries()) == list(model.primaries(oracle.Lattice(shape), start)), (q, shape, trial)
+        chain.close()
+
+
 def test_energy_matches_oracle_energy(oracle, gpu):
     # E from the integer primaries, as Ising::energy forms it (ising/mod.rs:116)
     got, want, chain, model, lat = run_pair(oracle, gpu, plq.ISING, 2, (12, 8), plq.METROPOLIS, plq.RNG_STREAM, 0.3,
