@@ -367,6 +367,11 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
             c->fused_tz = fused3d_default_tz(c->g.L[2]);
             e = cudaMalloc((void **)&c->d_state_alt, (size_t)c->n_vars);
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(state_alt)"));
+            for (int k = 0; k < 2; ++k) {
+                c->fused_map_buf[k] = k ? c->d_state_alt : c->d_state;
+                e = fused3d_make_maps(c->fused_map_buf[k], c->g.L[0], c->g.L[1], c->g.L[2], &c->fused_maps[k]);
+                if (e != cudaSuccess) return fail(cuda_fail(e, "tensor map of the state buffer"));
+            }
         }
         if (c->lookback) {
             c->n_chunks = local_chunks(n);
@@ -450,7 +455,9 @@ static int fused_sweep(plq_chain *c) {
         f.off1 = c->host_pos + (uint64_t)(c->n_sites / 2);
         f.plane = to_affine(affine_steps(c->h_jump, (uint64_t)f.L0 * (uint64_t)f.L1 / 2));
     }
-    cudaError_t e = launch_fused3d(f, c->q, stream, hb, c->stream);
+    f.status = &c->d_ctrl->status;
+    const FusedMaps &maps = c->fused_maps[f.src == c->fused_map_buf[0] ? 0 : 1];
+    cudaError_t e = launch_fused3d(f, maps, c->q, stream, hb, c->stream);
     c->launches++;
     if (e != cudaSuccess) return cuda_fail(e, "fused sweep launch");
     std::swap(c->d_state, c->d_state_alt);
@@ -540,7 +547,8 @@ static int check_status(plq_chain *c) {
                                       "so this is a bug rather than a hard lattice");
     if (st)
         return plq_fail(PLQ_EDEVICE, "device status word " + std::to_string(st) +
-                                         " (1 = look-back wait limit, 4 = bounds, 8 = queue overflow)");
+                                         " (1 = look-back wait limit, 4 = bounds, 8 = queue overflow, "
+                                         "16 = tile copy wait limit)");
     return PLQ_OK;
 }
 

@@ -8,6 +8,7 @@
 
 #include "../../include/plaquette.h"
 #include "plq_device.cuh"
+#include "plq_fused.h"
 #include "plq_tables.h"
 
 struct plq_ctx {
@@ -31,6 +32,8 @@ struct plq_chain {
     uint8_t *d_state_alt = nullptr;  // second buffer of the out-of-place fused sweep
     bool fused = false;
     int fused_tz = 0;
+    plq::FusedMaps fused_maps[2];          // TMA descriptors of the two state buffers
+    const uint8_t *fused_map_buf[2] = {nullptr, nullptr};
     std::vector<plq::AffineHost> h_jump;  // host copy of the jump table
     uint8_t *d_io = nullptr;     // host-order staging on the device
     uint64_t *d_hb53 = nullptr, *d_metro53 = nullptr;

@@ -15,6 +15,7 @@ constexpr uint32_t kStatusLookbackTimeout = 1u << 0;
 constexpr uint32_t kStatusPassCap = 1u << 1;
 constexpr uint32_t kStatusBounds = 1u << 2;
 constexpr uint32_t kStatusQueueOverflow = 1u << 3;
+constexpr uint32_t kStatusCopyTimeout = 1u << 4;
 
 // Lattice geometry by value: extents, strides, site count, and the magic
 // numbers that divide a site index (< 2^31) by each extent.

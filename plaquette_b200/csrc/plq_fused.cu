@@ -9,7 +9,8 @@
 // A CTA owns full x-rows (L0 = 128, 256 or 512, so x wraps inside
 // shared memory) for TY = 8192/L0 rows of y, and marches along z through a
 // ring of shared-memory planes with a y halo of 2.  At step z:
-//   1. plane z+2 has landed (prefetched FPREF steps ahead by cp.async);
+//   1. plane z+2 has landed (prefetched FPREF steps ahead as three TMA boxes
+//      -- TY interior rows and two wrapped 2-row halos -- on the slot's mbarrier);
 //   2. colour 0 of plane z+1 is updated in shared memory on the interior rows
 //      and on the two ring rows y0-1 and y0+TY (recomputed by the
 //      neighbouring tile too -- same inputs, same draws, same result);
@@ -22,7 +23,11 @@
 // Neighbour keys are computed four sites per 32-bit word (SWAR): states are
 // bytes and the per-byte neighbour sum of g(state) never carries (g = state
 // for q = 2; g = 0,1,7 for q = 3), giving the table key cur + q*sum(g).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+
+#include <climits>
 
 #include "../../include/plaquette.h"
 #include "plq_device.cuh"
@@ -38,13 +43,42 @@ constexpr int FPREF = 3, FNS = FPREF + 5;     // ring of 8 planes
 constexpr int FTABLE_BYTES = 4096;
 constexpr int FMAX_L0 = 512;  // 2 ring rows of L0/4 words: one word per thread
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+constexpr int kFusedWaitLimit = 1 << 21;  // polls of a plane's barrier before the launch gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_pref() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(FPREF) : "memory");
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Waits for the phase of the given parity to complete; false after the poll limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (int i = 0; i < kFusedWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// One TMA box of full rows (x = 0, rows from y, plane z) into shared memory,
+// completing on `bar` with its byte count.  No multicast.
+__device__ __forceinline__ void tma_rows(void *dst, const CUtensorMap *map, int y, int z, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
 }
 
 __device__ __forceinline__ int wrapi(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
@@ -149,37 +183,52 @@ __device__ __forceinline__ uint4 update_run(const FusedArgs &a, const uint8_t *t
 }
 
 template <int Q, bool STREAM, bool HB>
-__global__ void __launch_bounds__(FTHREADS, 2) fused3d_kernel(FusedArgs a) {
-    extern __shared__ __align__(16) uint8_t smem[];
+__global__ void __launch_bounds__(FTHREADS, 2)
+    fused3d_kernel(const FusedArgs a, const __grid_constant__ CUtensorMap tm_rows,
+                   const __grid_constant__ CUtensorMap tm_halo) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // TMA destinations start on 128-byte boundaries: align the base here
+    // (the launch reserves 128 bytes for it) rather than trust the window's.
+    uint8_t *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
     const int L0 = a.L0, L1 = a.L1, L2 = a.L2, TY = a.ty;
     const int plane_bytes = L0 * (TY + 4);
     uint8_t *ring = smem;
     uint8_t *tab = smem + FNS * plane_bytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(tab + FTABLE_BYTES);
     const int t = threadIdx.x;
     const int y0 = blockIdx.x * TY, z0 = blockIdx.y * a.tz;
 
+    if (t == 0) {
+        for (int i = 0; i < FNS; ++i) mbar_init(&bars[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     {
         const uint32_t *src = reinterpret_cast<const uint32_t *>(a.table);
         uint32_t *dst = reinterpret_cast<uint32_t *>(tab);
         for (int i = t; i < a.table_words; i += FTHREADS) dst[i] = src[i];
     }
+    __syncthreads();
 
-    const int zlast = z0 + a.tz + 1;
-    const int chunks_per_row = L0 / 16;
-    const int chunks = chunks_per_row * (TY + 4);
+    // Plane zp (zfirst <= zp <= zlast) lives in ring slot (zp - zfirst) % FNS;
+    // its fill is that slot's use number (zp - zfirst) / FNS, whose parity the
+    // waits name.  Thread 0 issues every plane as three TMA boxes: the TY
+    // interior rows and the two 2-row y halos (wrapped, so each is contiguous).
+    const int zfirst = z0 - 2, zlast = z0 + a.tz + 1;
+    auto slot = [&](int zp) { return (zp - zfirst) % FNS; };
+    auto parity = [&](int zp) { return (uint32_t)(((zp - zfirst) / FNS) & 1); };
     auto issue = [&](int zp) {
         if (zp <= zlast) {
             const int gz = wrapi(zp, L2);
-            uint8_t *slot = ring + ((zp + 2 * FNS) % FNS) * plane_bytes;
-            for (int c = t; c < chunks; c += FTHREADS) {
-                int row = c / chunks_per_row, cx = c - row * chunks_per_row;
-                int gy = wrapi(y0 - 2 + row, L1);
-                cp_async16(slot + row * L0 + 16 * cx, a.src + ((size_t)gz * L1 + gy) * L0 + 16 * cx);
-            }
+            uint8_t *dst = ring + slot(zp) * plane_bytes;
+            uint64_t *bar = &bars[slot(zp)];
+            mbar_expect_tx(bar, (uint32_t)plane_bytes);
+            tma_rows(dst + 2 * L0, &tm_rows, y0, gz, bar);
+            tma_rows(dst, &tm_halo, wrapi(y0 - 2, L1), gz, bar);
+            tma_rows(dst + (TY + 2) * L0, &tm_halo, wrapi(y0 + TY, L1), gz, bar);
         }
-        cp_commit();
     };
-    for (int zp = z0 - 2; zp <= z0 + FPREF; ++zp) issue(zp);
+    if (t == 0)
+        for (int zp = zfirst; zp <= z0 + FPREF; ++zp) issue(zp);
 
     // interior runs u = t + 256k: smem row 2 + u / runs_per_row, x = 16 * (u % runs_per_row)
     const int runs_per_row = L0 / FRUN;
@@ -201,15 +250,26 @@ __global__ void __launch_bounds__(FTHREADS, 2) fused3d_kernel(FusedArgs a) {
     u128 st0[FRUNS_PER_THREAD], st1[FRUNS_PER_THREAD], stR;
     const size_t plane_sites = (size_t)L0 * L1;
 
-    for (int z = z0 - 2; z < z0 + a.tz; ++z) {
-        cp_wait_pref();
-        __syncthreads();
-        issue(z + FPREF + 3);
+    int z_abort = INT_MAX;
+    for (int z = zfirst; z < z0 + a.tz; ++z) {
+        // planes z and z+1 landed at earlier steps (both at the first), z+2 now
+        bool landed = true;
+        if (z == zfirst) landed = mbar_wait(&bars[slot(z)], parity(z)) && mbar_wait(&bars[slot(z + 1)], parity(z + 1));
+        landed = landed && mbar_wait(&bars[slot(z + 2)], parity(z + 2));
+        if (__syncthreads_or(!landed)) {
+            z_abort = z;
+            break;
+        }
+        if (t == 0) {
+            // every thread's reads and writes of the slot refilled next are done
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(z + FPREF + 3);
+        }
 
         const int gz1 = wrapi(z + 1, L2), gz0 = wrapi(z, L2);
-        const uint8_t *sM = ring + ((z + 2 * FNS) % FNS) * plane_bytes;      // plane z
-        uint8_t *sC = ring + ((z + 1 + 2 * FNS) % FNS) * plane_bytes;        // plane z+1
-        const uint8_t *sP = ring + ((z + 2 + 2 * FNS) % FNS) * plane_bytes;  // plane z+2
+        const uint8_t *sM = ring + slot(z) * plane_bytes;      // plane z
+        uint8_t *sC = ring + slot(z + 1) * plane_bytes;        // plane z+1
+        const uint8_t *sP = ring + slot(z + 2) * plane_bytes;  // plane z+2
         const size_t zoff1 = (size_t)gz1 * plane_sites;
 
         // ---- colour 0 of plane z+1: interior runs and the ring word
@@ -255,7 +315,7 @@ __global__ void __launch_bounds__(FTHREADS, 2) fused3d_kernel(FusedArgs a) {
         // ---- colour 1 of plane z: interior runs, stored to dst
         if (z >= z0) {
             const size_t zoff0 = (size_t)gz0 * plane_sites;
-            const uint8_t *zM = ring + ((z - 1 + 2 * FNS) % FNS) * plane_bytes;
+            const uint8_t *zM = ring + slot(z - 1) * plane_bytes;
 #pragma unroll
             for (int k = 0; k < FRUNS_PER_THREAD; ++k) {
                 if (STREAM)
@@ -269,7 +329,12 @@ __global__ void __launch_bounds__(FTHREADS, 2) fused3d_kernel(FusedArgs a) {
             }
         }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (z_abort != INT_MAX && t == 0) {
+        // a plane never landed: report, and let the copies already issued finish (bounded) before exit
+        atomicOr(a.status, kStatusCopyTimeout);
+        const int last = min(zlast, z_abort + FPREF + 2);
+        for (int zp = z_abort; zp <= last; ++zp) mbar_wait(&bars[slot(zp)], parity(zp));
+    }
 }
 
 static int fused_ty(int L0) { return FPLANE_SITES / L0; }
@@ -291,28 +356,57 @@ int fused3d_default_tz(int L2) {
 }
 
 size_t fused3d_smem_bytes(int L0) {
-    return (size_t)FNS * (size_t)L0 * (size_t)(fused_ty(L0) + 4) + FTABLE_BYTES;
+    return 128 + (size_t)FNS * (size_t)L0 * (size_t)(fused_ty(L0) + 4) + FTABLE_BYTES + FNS * sizeof(uint64_t);
 }
 int fused3d_table_limit_bytes() { return FTABLE_BYTES; }
 
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+}
+
+cudaError_t fused3d_make_maps(const uint8_t *buf, int L0, int L1, int L2, FusedMaps *out) {
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return cudaErrorNotSupported;
+    // u8 [L2][L1][L0/X][X]: rows of L0 bytes land densely in shared memory
+    const cuuint32_t X = (cuuint32_t)(L0 < 256 ? L0 : 256);
+    const cuuint64_t dims[4] = {X, (cuuint64_t)(L0 / (int)X), (cuuint64_t)L1, (cuuint64_t)L2};
+    const cuuint64_t strides[3] = {X, (cuuint64_t)L0, (cuuint64_t)L0 * (cuuint64_t)L1};
+    const cuuint32_t elem[4] = {1, 1, 1, 1};
+    const cuuint32_t box_rows[4] = {X, (cuuint32_t)(L0 / (int)X), (cuuint32_t)fused_ty(L0), 1};
+    const cuuint32_t box_halo[4] = {X, (cuuint32_t)(L0 / (int)X), 2, 1};
+    for (int k = 0; k < 2; ++k) {
+        CUresult r = encode(k ? &out->halo : &out->rows, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t *>(buf),
+                            dims, strides, k ? box_halo : box_rows, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
 template <int Q, bool STREAM, bool HB>
-static cudaError_t launch_t(FusedArgs a, cudaStream_t s) {
+static cudaError_t launch_t(FusedArgs a, const FusedMaps &m, cudaStream_t s) {
     auto kern = fused3d_kernel<Q, STREAM, HB>;
     size_t smem = fused3d_smem_bytes(a.L0);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     a.ty = fused_ty(a.L0);
     dim3 grid(a.L1 / a.ty, a.L2 / a.tz);
-    kern<<<grid, FTHREADS, smem, s>>>(a);
+    kern<<<grid, FTHREADS, smem, s>>>(a, m.rows, m.halo);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fused3d(const FusedArgs &a, int q, bool stream, bool hb, cudaStream_t s) {
+cudaError_t launch_fused3d(const FusedArgs &a, const FusedMaps &m, int q, bool stream, bool hb, cudaStream_t s) {
     if (q == 2) {
-        if (hb) return stream ? launch_t<2, true, true>(a, s) : launch_t<2, false, true>(a, s);
-        return launch_t<2, false, false>(a, s);
+        if (hb) return stream ? launch_t<2, true, true>(a, m, s) : launch_t<2, false, true>(a, m, s);
+        return launch_t<2, false, false>(a, m, s);
     }
-    if (q == 3 && hb) return stream ? launch_t<3, true, true>(a, s) : launch_t<3, false, true>(a, s);
+    if (q == 3 && hb) return stream ? launch_t<3, true, true>(a, m, s) : launch_t<3, false, true>(a, m, s);
     return cudaErrorInvalidValue;
 }
 

@@ -1,5 +1,6 @@
 // plq_fused.h -- the fused two-colour 3D site sweep (plq_fused.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "plq_device.cuh"
@@ -18,12 +19,21 @@ struct FusedArgs {
     u128 base, inc;
     uint64_t off0, off1; // stream positions of rank 0 of colours 0 and 1
     Affine plane;        // stream jump by one z-plane of one colour (L0*L1/2 draws)
+    unsigned int *status;  // chain status word (copy wait limit)
+};
+
+// TMA descriptors of one state buffer viewed as u8 [L2][L1][L0/X][X] (X =
+// min(L0, 256)): boxes of TY full rows (a tile's interior) and of 2 rows (a
+// y halo), one z-plane deep.
+struct FusedMaps {
+    CUtensorMap rows, halo;
 };
 
 bool fused3d_eligible(int model, int q, int d, const int32_t *L, int updater, int rng);
 int fused3d_default_tz(int L2);
 size_t fused3d_smem_bytes(int L0);
 int fused3d_table_limit_bytes();
-cudaError_t launch_fused3d(const FusedArgs &a, int q, bool stream, bool hb, cudaStream_t s);
+cudaError_t fused3d_make_maps(const uint8_t *buf, int L0, int L1, int L2, FusedMaps *out);
+cudaError_t launch_fused3d(const FusedArgs &a, const FusedMaps &maps, int q, bool stream, bool hb, cudaStream_t s);
 
 }  // namespace plq
