@@ -58,6 +58,12 @@ enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
  * trips the cap: exercises the PLQ_ECAP path (gpu_cluster.rs:512-518) on the
  * host side without any device fault. */
 #define PLQ_FLAG_TINY_PASS_CAP 2
+/* Fused 3D sweep only: never issue the tile copies of one z-plane and wait
+ * for them at most 1024 polls, so every tile's bounded wait runs out and the
+ * launch reports PLQ_EDEVICE (status bit 16) -- exercises the copy-wait limit
+ * without any device fault.  No reference counterpart (the reference has no
+ * staged tiles). */
+#define PLQ_FLAG_TEST_COPY_STALL 4
 
 typedef struct plq_ctx plq_ctx;
 typedef struct plq_chain plq_chain;

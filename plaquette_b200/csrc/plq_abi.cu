@@ -456,6 +456,8 @@ static int fused_sweep(plq_chain *c) {
         f.plane = to_affine(affine_steps(c->h_jump, (uint64_t)f.L0 * (uint64_t)f.L1 / 2));
     }
     f.status = &c->d_ctrl->status;
+    f.stall = (c->desc.flags & PLQ_FLAG_TEST_COPY_STALL) ? 1 : 0;
+    f.wait_limit = f.stall ? 1024 : (1 << 21);
     const FusedMaps &maps = c->fused_maps[f.src == c->fused_map_buf[0] ? 0 : 1];
     cudaError_t e = launch_fused3d(f, maps, c->q, stream, hb, c->stream);
     c->launches++;

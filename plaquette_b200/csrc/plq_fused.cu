@@ -43,8 +43,6 @@ constexpr int FPREF = 3, FNS = FPREF + 5;     // ring of 8 planes
 constexpr int FTABLE_BYTES = 4096;
 constexpr int FMAX_L0 = 512;  // 2 ring rows of L0/4 words: one word per thread
 
-constexpr int kFusedWaitLimit = 1 << 21;  // polls of a plane's barrier before the launch gives up
-
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
@@ -65,9 +63,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return done != 0;
 }
-// Waits for the phase of the given parity to complete; false after the poll limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (int i = 0; i < kFusedWaitLimit; ++i)
+// Waits for the phase of the given parity to complete; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int limit) {
+    for (int i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -217,7 +215,7 @@ __global__ void __launch_bounds__(FTHREADS, 2)
     auto slot = [&](int zp) { return (zp - zfirst) % FNS; };
     auto parity = [&](int zp) { return (uint32_t)(((zp - zfirst) / FNS) & 1); };
     auto issue = [&](int zp) {
-        if (zp <= zlast) {
+        if (zp <= zlast && !(a.stall && zp == zfirst + 4)) {
             const int gz = wrapi(zp, L2);
             uint8_t *dst = ring + slot(zp) * plane_bytes;
             uint64_t *bar = &bars[slot(zp)];
@@ -254,8 +252,10 @@ __global__ void __launch_bounds__(FTHREADS, 2)
     for (int z = zfirst; z < z0 + a.tz; ++z) {
         // planes z and z+1 landed at earlier steps (both at the first), z+2 now
         bool landed = true;
-        if (z == zfirst) landed = mbar_wait(&bars[slot(z)], parity(z)) && mbar_wait(&bars[slot(z + 1)], parity(z + 1));
-        landed = landed && mbar_wait(&bars[slot(z + 2)], parity(z + 2));
+        if (z == zfirst)
+            landed = mbar_wait(&bars[slot(z)], parity(z), a.wait_limit) &&
+                      mbar_wait(&bars[slot(z + 1)], parity(z + 1), a.wait_limit);
+        landed = landed && mbar_wait(&bars[slot(z + 2)], parity(z + 2), a.wait_limit);
         if (__syncthreads_or(!landed)) {
             z_abort = z;
             break;
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(FTHREADS, 2)
         // a plane never landed: report, and let the copies already issued finish (bounded) before exit
         atomicOr(a.status, kStatusCopyTimeout);
         const int last = min(zlast, z_abort + FPREF + 2);
-        for (int zp = z_abort; zp <= last; ++zp) mbar_wait(&bars[slot(zp)], parity(zp));
+        for (int zp = z_abort; zp <= last; ++zp) mbar_wait(&bars[slot(zp)], parity(zp), a.wait_limit);
     }
 }
 

@@ -20,6 +20,8 @@ struct FusedArgs {
     uint64_t off0, off1; // stream positions of rank 0 of colours 0 and 1
     Affine plane;        // stream jump by one z-plane of one colour (L0*L1/2 draws)
     unsigned int *status;  // chain status word (copy wait limit)
+    int wait_limit;        // polls of a plane's barrier before the launch gives up
+    int stall;             // test only: plane zfirst + 4 of every tile is never issued
 };
 
 // TMA descriptors of one state buffer viewed as u8 [L2][L1][L0/X][X] (X =

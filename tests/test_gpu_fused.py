@@ -75,3 +75,20 @@ def test_vector_scan_pass_equals_generic_lookback(gpu, shape, beta):
         outs.append((next(c), c.stream_position()))
     assert np.array_equal(outs[0][0], outs[1][0])
     assert outs[0][1] == outs[1][1]
+
+
+def test_tile_copy_wait_limit_reports_and_context_survives(oracle, gpu):
+    # every tile waits for a z-plane whose copies are never issued: the bounded
+    # wait runs out, the launch reports status bit 16, and the device stays usable
+    shape = (128, 64, 16)
+    start = np.zeros(int(np.prod(shape)), dtype=np.uint8)
+    d = plq.make_desc(plq.ISING, 2, shape, plq.METROPOLIS, beta=0.3, seed=3, rng=plq.RNG_KEYED, batch=1,
+                      flags=plq.FLAG_TEST_COPY_STALL)
+    chain = plq.GpuChain(gpu, d, start)
+    assert chain.path == "fused3d"
+    with pytest.raises(plq.PlaquetteError, match="16 = tile copy wait limit") as info:
+        next(chain)
+    assert info.value.code == plq.PLQ_EDEVICE
+    chain.close()
+    got, want, *_ = run_pair(oracle, gpu, plq.ISING, 2, shape, plq.METROPOLIS, plq.RNG_KEYED, 0.3, 2)
+    assert np.array_equal(got, want)
