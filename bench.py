@@ -33,6 +33,8 @@ N_SITES = SHAPE[0] * SHAPE[1] * SHAPE[2]
 BYTES_PER_UPDATE = 2  # each site read once and written once per sweep
 
 # name -> (model, q, updater, rng, beta, description, dominant kernel, launches per sweep)
+HIST_BINS = 1024
+
 WORKLOADS = {
     "potts3-512-hb-stream": ("potts", 3, "heatbath", "stream", 0.5505,
                              "3D q=3 Potts 512^3 periodic, checkerboard heat bath, beta=0.5505, PCG64 reference "
@@ -47,7 +49,7 @@ WORKLOADS = {
     "ising-512-metro-stream": ("ising", 2, "metropolis", "stream", 0.2216544,
                                "3D Ising 512^3 periodic, checkerboard Metropolis, beta=0.2216544, PCG64 reference "
                                "stream (bit-exact with the reference CPU path; device-wide scan per colour pass), "
-                               "uniform random start from seed 20260718", "local_pass_kernel<3,false,true>", 2),
+                               "uniform random start from seed 20260718", "scan_metro_kernel<3>", 2),
 }
 
 
@@ -177,6 +179,7 @@ def run_product(args):
     import torch
 
     import plaquette_b200 as plq
+    from plaquette_b200 import observables as obs
 
     w = WORKLOADS[args.workload]
     world, rank, local, pg = dist_setup()
@@ -231,7 +234,13 @@ def run_product(args):
     echain = plq.GpuChain(gpu, desc, pinned.numpy())
     _, prims = echain.next_batch(args.steps, states=False)
     plq.check(plq.lib().plq_chain_read(echain._h, out_pinned.data_ptr()))
+    # per-sweep energy and order-parameter histograms (1024 bins) from the exact primaries
+    model = obs.POTTS if w[0] == "potts" else obs.ISING
+    ser = obs.series(model, prims, N_SITES)
+    hist_e = obs.histogram(ser["e"], HIST_BINS, -3.0, 3.0)
+    hist_m = obs.histogram(ser["m"], HIST_BINS, 0.0, 1.0)
     t1 = time.perf_counter()
+    assert int(hist_e.sum()) == int(hist_m.sum()) == args.steps
     e2e_s = max_over_ranks(pg, t1 - t0, local)
     e2e_value = sites_total / (e2e_s * 1e9)
     n_prim = len(prims[0])
@@ -262,7 +271,8 @@ def run_product(args):
                 "h2d_bytes_per_step": N_SITES / args.steps,
                 "d2h_bytes_per_step": 8 * n_prim + N_SITES / args.steps,
                 "what": "chain create from a pinned host start, K samples of one sweep each with their device "
-                        "primaries read back (GPU_BATCH per round-trip), final configuration read back"},
+                        "primaries read back, per-sweep E/N and order-parameter histograms "
+                        f"({HIST_BINS} bins), final configuration read back"},
         "gpu_launches": launches,
         "clocks": clock_info,
     }
