@@ -50,7 +50,6 @@ __global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
     __shared__ unsigned long long s_ticket;
     __shared__ uint64_t s_tab[64];
     __shared__ int warp_tot[SThreads / 32];
-    __shared__ unsigned long long s_excl, s_base;
     __shared__ u128 s_chunk_state;
     __shared__ int s_fail;
 
@@ -120,7 +119,7 @@ __global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
     }
     const int need = __popc(need_mask);
 
-    // ---- block scan + decoupled look-back
+    // ---- block scan + decoupled look-back (warp 0 reads 32 predecessors at a time)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int incl = need;
 #pragma unroll
@@ -129,7 +128,6 @@ __global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
         if (lane >= off) incl += v;
     }
     if (lane == 31) warp_tot[wid] = incl;
-    if (threadIdx.x == 0) s_fail = 0;
     __syncthreads();
     int warp_excl = 0, total = 0;
 #pragma unroll
@@ -139,37 +137,69 @@ __global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
         total += t;
     }
     const int thread_excl = warp_excl + incl - need;
-    if (threadIdx.x == 0) {
+    if (wid == 0) {
+        const uint32_t ep = a.epoch & 0x3FFFFFFFu;
         unsigned long long excl = 0;
+        bool fail = false;
         if (chunk == 0) {
-            atomicExch(&a.desc[0], s_make_desc(a.epoch, 2ull, (uint32_t)total));
+            if (lane == 0) atomicExch(&a.desc[0], s_make_desc(a.epoch, 2ull, (uint32_t)total));
         } else {
-            atomicExch(&a.desc[chunk], s_make_desc(a.epoch, 1ull, (uint32_t)total));
-            int64_t j = chunk - 1;
+            if (lane == 0) atomicExch(&a.desc[chunk], s_make_desc(a.epoch, 1ull, (uint32_t)total));
+            int64_t top = chunk - 1;  // lane l reads chunk top - l
             int spins = 0;
-            while (j >= 0) {
-                unsigned long long d = s_ld_relaxed(&a.desc[j]);
-                uint32_t ep = (uint32_t)(d >> 34);
-                unsigned long long st = (d >> 32) & 3ull;
-                if (ep != (a.epoch & 0x3FFFFFFFu) || st == 0) {
+            while (true) {
+                const int64_t idx = top - lane;
+                const unsigned long long d = idx >= 0 ? s_ld_relaxed(&a.desc[idx]) : s_make_desc(a.epoch, 2ull, 0u);
+                const unsigned long long st = (uint32_t)(d >> 34) == ep ? (d >> 32) & 3ull : 0ull;
+                const unsigned incl_lanes = __ballot_sync(0xffffffffu, st == 2ull);
+                const unsigned ready = __ballot_sync(0xffffffffu, st != 0ull);
+                // lanes up to the nearest inclusive prefix (all 32 when none is in this window)
+                const unsigned span = incl_lanes ? (((incl_lanes & (0u - incl_lanes)) << 1) - 1u) : 0xffffffffu;
+                if ((ready & span) != span) {
                     if (++spins > SSpinLimit) {
-                        s_fail = 1;
-                        atomicOr(&a.ctrl->status, kStatusLookbackTimeout);
+                        fail = true;
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(32);
                     continue;
                 }
-                excl += (uint32_t)d;
-                if (st == 2ull) break;
-                --j;
+                unsigned long long v = ((span >> lane) & 1u) ? (unsigned long long)(uint32_t)d : 0ull;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+                excl += v;
+                if (incl_lanes) break;
+                top -= 32;
             }
-            if (!s_fail) atomicExch(&a.desc[chunk], s_make_desc(a.epoch, 2ull, (uint32_t)(excl + total)));
+            if (lane == 0 && !fail)
+                atomicExch(&a.desc[chunk], s_make_desc(a.epoch, 2ull, (uint32_t)(excl + total)));
         }
-        s_excl = excl;
-        s_base = a.ctrl->pos[a.pos_in];
-        if (chunk == a.n_chunks - 1 && !s_fail) a.ctrl->pos[a.pos_in ^ 1] = s_base + excl + (unsigned long long)total;
-        if (!s_fail) s_chunk_state = jump(a.jump, a.base, s_base + excl);
+        unsigned long long pass_pos = 0;
+        if (lane == 0) {
+            s_fail = fail ? 1 : 0;
+            if (fail) atomicOr(&a.ctrl->status, kStatusLookbackTimeout);
+            pass_pos = a.ctrl->pos[a.pos_in];
+            if (chunk == a.n_chunks - 1 && !fail) a.ctrl->pos[a.pos_in ^ 1] = pass_pos + excl + (unsigned long long)total;
+        }
+        // the chunk's stream state: lanes 0..7 fetch one radix-256 digit's map each and the maps
+        // (powers of the same LCG step, so they commute) are composed in a tree
+        const unsigned long long n_pos = __shfl_sync(0xffffffffu, pass_pos, 0) + excl;
+        Affine f;
+        const unsigned dv = lane < kJumpDigits ? (unsigned)((n_pos >> (8 * lane)) & 255u) : 0u;
+        if (dv) {
+            f = a.jump[lane * kJumpRadix + dv];
+        } else {
+            f.m.lo = 1; f.m.hi = 0; f.p.lo = 0; f.p.hi = 0;
+        }
+#pragma unroll
+        for (int off = 1; off < kJumpDigits; off <<= 1) {
+            Affine g;
+            g.m.lo = __shfl_down_sync(0xffffffffu, f.m.lo, off);
+            g.m.hi = __shfl_down_sync(0xffffffffu, f.m.hi, off);
+            g.p.lo = __shfl_down_sync(0xffffffffu, f.p.lo, off);
+            g.p.hi = __shfl_down_sync(0xffffffffu, f.p.hi, off);
+            f = compose(f, g);
+        }
+        if (lane == 0) s_chunk_state = apply(f, a.base);
     }
     __syncthreads();
     if (s_fail || !active) return;
