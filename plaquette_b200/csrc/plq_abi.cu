@@ -375,9 +375,11 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
         }
         if (c->lookback) {
             c->n_chunks = local_chunks(n);
-            e = cudaMalloc((void **)&c->d_desc, sizeof(unsigned long long) * (size_t)c->n_chunks);
+            // descriptors for the larger chunk count of the two look-back pass kernels
+            const int64_t n_desc = std::max<int64_t>(c->n_chunks, scan_chunks(n));
+            e = cudaMalloc((void **)&c->d_desc, sizeof(unsigned long long) * (size_t)n_desc);
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(lookback)"));
-            cudaMemsetAsync(c->d_desc, 0, sizeof(unsigned long long) * (size_t)c->n_chunks, c->stream);
+            cudaMemsetAsync(c->d_desc, 0, sizeof(unsigned long long) * (size_t)n_desc, c->stream);
         }
     } else {
         int r2 = cluster_create(c);
@@ -481,7 +483,7 @@ int local_sweep(plq_chain *c) {
         a.color = pass & 1;
         if (c->lookback) {
             a.epoch = (uint32_t)(c->lookback_passes + 1);
-            a.ticket_base = c->lookback_passes * (uint64_t)c->n_chunks;
+            a.ticket_base = c->tickets_issued;
             a.pos_in = (int)(c->lookback_passes & 1);
             c->lookback_passes++;
         } else if (c->desc.rng == PLQ_RNG_STREAM) {
@@ -506,13 +508,15 @@ int local_sweep(plq_chain *c) {
             s.inc = c->inc;
             s.ctrl = c->d_ctrl;
             s.desc = c->d_desc;
-            s.n_chunks = c->n_chunks;
+            s.n_chunks = scan_chunks(c->n_sites);
             s.ticket_base = a.ticket_base;
             s.epoch = a.epoch;
             s.pos_in = a.pos_in;
             e = launch_scan_metro(s, c->d, c->stream);
+            c->tickets_issued += (uint64_t)s.n_chunks;
         } else {
             e = launch_local_pass(a, c->link, c->lookback, c->stream);
+            if (c->lookback) c->tickets_issued += (uint64_t)c->n_chunks;
         }
         c->launches++;
         if (e != cudaSuccess) return cuda_fail(e, "local pass launch");

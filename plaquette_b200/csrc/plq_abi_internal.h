@@ -53,6 +53,7 @@ struct plq_chain {
     uint64_t sweeps_done = 0;
     uint64_t host_pos = 0;          // deterministic stream passes: draws consumed
     uint64_t lookback_passes = 0;   // data-dependent passes launched
+    uint64_t tickets_issued = 0;    // look-back chunk tickets taken by those passes
     uint64_t launches = 0;
 
     // cluster state (plq_cluster.cu)

@@ -24,7 +24,7 @@ struct ScanArgs {
 };
 
 bool scan_metro_eligible(int d, const int32_t *L);
-// Chunks of one pass (equal to local_chunks(n_sites): 2048 ranks of a colour each).
+// Chunks (thread blocks, look-back descriptors) of one pass.
 int64_t scan_chunks(int64_t n_sites);
 cudaError_t launch_scan_metro(const ScanArgs &a, int d, cudaStream_t stream);
 
