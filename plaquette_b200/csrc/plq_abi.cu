@@ -509,11 +509,9 @@ int local_sweep(plq_chain *c) {
             s.ctrl = c->d_ctrl;
             s.desc = c->d_desc;
             s.n_chunks = scan_chunks(c->n_sites);
-            s.ticket_base = a.ticket_base;
             s.epoch = a.epoch;
             s.pos_in = a.pos_in;
-            e = launch_scan_metro(s, c->d, c->stream);
-            c->tickets_issued += (uint64_t)s.n_chunks;
+            e = launch_scan_metro(s, c->d, c->stream);  // takes no tickets
         } else {
             e = launch_local_pass(a, c->link, c->lookback, c->stream);
             if (c->lookback) c->tickets_issued += (uint64_t)c->n_chunks;

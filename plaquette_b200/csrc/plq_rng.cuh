@@ -61,12 +61,7 @@ struct Affine {
 PLQ_HD u128 apply(const Affine &f, u128 s);
 
 // g after f: s -> g(f(s)).
-PLQ_HD Affine compose(const Affine &f, const Affine &g) {
-    Affine r;
-    r.m = mul128(g.m, f.m);
-    r.p = add128(mul128(g.m, f.p), g.p);
-    return r;
-}
+PLQ_HD Affine compose(const Affine &f, const Affine &g);
 
 PLQ_HD uint64_t rotr64(uint64_t x, unsigned r) {
     r &= 63u;
@@ -135,6 +130,19 @@ PLQ_HD u128 apply(const Affine &f, u128 s) {
 #else
     return add128(mul128(f.m, s), f.p);
 #endif
+}
+
+PLQ_HD Affine compose(const Affine &f, const Affine &g) {
+    Affine r;
+#if defined(__CUDA_ARCH__)
+    const u128 zero{0, 0};
+    r.m = muladd128_limbs(g.m, f.m, zero);
+    r.p = muladd128_limbs(g.m, f.p, g.p);
+#else
+    r.m = mul128(g.m, f.m);
+    r.p = add128(mul128(g.m, f.p), g.p);
+#endif
+    return r;
 }
 
 // XSL-RR output of a 128-bit state.

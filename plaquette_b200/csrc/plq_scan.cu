@@ -5,7 +5,7 @@
 // variable draws only when its move is uphill (src/updater.rs:90), so its draw
 // position is the count of uphill variables of the colour before it in index
 // order -- a device-wide exclusive scan, done in one pass with decoupled
-// look-back over chunks taken in ticket order.  What this kernel changes is
+// look-back over chunks in block order.  What this kernel changes is
 // the cost per site:
 //   * a thread owns 16 consecutive sites (one 16-byte vector, 8 of the pass's
 //     colour); neighbour words come as vectors (+-y, +-z) and 4-byte words
@@ -46,17 +46,18 @@ __device__ __forceinline__ u128 jump_small(const Affine *table, u128 s, uint32_t
 }
 
 template <int D>
-__global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
-    __shared__ unsigned long long s_ticket;
+__global__ void __launch_bounds__(SThreads, 8) scan_metro_kernel(ScanArgs a) {
     __shared__ uint64_t s_tab[64];
     __shared__ int warp_tot[SThreads / 32];
     __shared__ u128 s_chunk_state;
     __shared__ int s_fail;
 
     if (threadIdx.x < a.table_entries) s_tab[threadIdx.x] = a.metro53[threadIdx.x];
-    if (threadIdx.x == 0) s_ticket = atomicAdd(&a.ctrl->ticket, 1ull) - a.ticket_base;
     __syncthreads();
-    const int64_t chunk = (int64_t)s_ticket;
+    // Chunk = block index: blocks are dispatched in index order, so a chunk's
+    // predecessors are running or done when it looks back (the waits are
+    // bounded all the same).
+    const int64_t chunk = (int64_t)blockIdx.x;
     if (chunk >= a.n_chunks) {
         if (threadIdx.x == 0) atomicOr(&a.ctrl->status, kStatusBounds);
         return;
@@ -68,7 +69,6 @@ __global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
     // ---- keys of the 16 sites
     uint32_t C[4] = {0, 0, 0, 0}, K[4] = {0, 0, 0, 0};
     uint32_t need_mask = 0;  // bit i: colour site i (0..7) draws
-    uint64_t entry[8];
     int b = 0;
     if (active) {
         // coordinates of the vector's first site (x multiple of 16)
@@ -113,8 +113,7 @@ __global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
         for (int i = 0; i < 8; ++i) {
             const int j = b + 2 * i;
             const uint32_t key = (K[j >> 2] >> (8 * (j & 3))) & 0xFFu;
-            entry[i] = s_tab[key];
-            if (entry[i] != ~0ull) need_mask |= 1u << i;
+            if (s_tab[key] != ~0ull) need_mask |= 1u << i;
         }
     }
     const int need = __popc(need_mask);
@@ -212,9 +211,9 @@ __global__ void __launch_bounds__(SThreads) scan_metro_kernel(ScanArgs a) {
         const int j = b + 2 * i;
         bool accept;
         if ((need_mask >> i) & 1u) {
-            uint64_t k = draw53(st);
+            const uint64_t k = draw53(st);
             st = pcg_step(st, a.inc);
-            accept = k < entry[i];
+            accept = k < s_tab[(K[j >> 2] >> (8 * (j & 3))) & 0xFFu];
         } else {
             accept = true;  // downhill: accept without a draw
         }

@@ -18,7 +18,6 @@ struct ScanArgs {
     Control *ctrl;
     unsigned long long *desc;
     int64_t n_chunks;
-    uint64_t ticket_base;
     uint32_t epoch;
     int pos_in;
 };
