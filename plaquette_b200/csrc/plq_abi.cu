@@ -500,6 +500,10 @@ int local_sweep(plq_chain *c) {
             s.L0 = c->g.L[0];
             s.L1 = c->g.L[1];
             s.L2 = c->g.L[2];
+            s.dm0 = c->g.dm[0];
+            s.dl0 = c->g.dl[0];
+            s.dm1 = c->g.dm[1];
+            s.dl1 = c->g.dl[1];
             s.color = a.color;
             s.metro53 = c->d_metro53;
             s.table_entries = (int)env_key_count(model_params(&c->desc));
@@ -511,7 +515,7 @@ int local_sweep(plq_chain *c) {
             s.n_chunks = scan_chunks(c->n_sites);
             s.epoch = a.epoch;
             s.pos_in = a.pos_in;
-            e = launch_scan_metro(s, c->d, c->stream);  // takes no tickets
+            e = launch_scan_metro(s, c->d, c->stream);
         } else {
             e = launch_local_pass(a, c->link, c->lookback, c->stream);
             if (c->lookback) c->tickets_issued += (uint64_t)c->n_chunks;

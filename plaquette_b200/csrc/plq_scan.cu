@@ -71,12 +71,13 @@ __global__ void __launch_bounds__(SThreads, 8) scan_metro_kernel(ScanArgs a) {
     uint32_t need_mask = 0;  // bit i: colour site i (0..7) draws
     int b = 0;
     if (active) {
-        // coordinates of the vector's first site (x multiple of 16)
-        const uint32_t row = (uint32_t)(s0 / a.L0);
-        const uint32_t x0 = (uint32_t)(s0 - (int64_t)row * a.L0);
+        // coordinates of the vector's first site (x multiple of 16; site
+        // indices are below 2^32 on this path, see scan_metro_eligible)
+        const uint32_t row = fdiv((uint32_t)s0, a.dm0, a.dl0);
+        const uint32_t x0 = (uint32_t)s0 - row * (uint32_t)a.L0;
         uint32_t y = row, z = 0;
         if (D == 3) {
-            z = row / (uint32_t)a.L1;
+            z = fdiv(row, a.dm1, a.dl1);
             y = row - z * (uint32_t)a.L1;
         }
         const uint4 c4 = *reinterpret_cast<const uint4 *>(a.state + s0);
@@ -109,12 +110,13 @@ __global__ void __launch_bounds__(SThreads, 8) scan_metro_kernel(ScanArgs a) {
         }
         // the pass's colour sits at byte offsets b, b+2, ... (x0 even)
         b = (int)((a.color + y + z) & 1u);
+        // shift each word by b bytes: colour site i is byte 2*(i&1) of word i>>1
+        const uint32_t sh = 8u * (uint32_t)b;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int j = b + 2 * i;
-            const uint32_t key = (K[j >> 2] >> (8 * (j & 3))) & 0xFFu;
-            if (s_tab[key] != ~0ull) need_mask |= 1u << i;
-        }
+        for (int w = 0; w < 4; ++w) K[w] >>= sh;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (s_tab[(K[i >> 1] >> (16 * (i & 1))) & 0xFFu] != ~0ull) need_mask |= 1u << i;
     }
     const int need = __popc(need_mask);
 
@@ -205,26 +207,26 @@ __global__ void __launch_bounds__(SThreads, 8) scan_metro_kernel(ScanArgs a) {
 
     // ---- draws and decisions
     u128 st = jump_small(a.jump, s_chunk_state, (uint32_t)thread_excl);
-    uint32_t flip[4] = {0, 0, 0, 0};
+    uint32_t flip[4] = {0, 0, 0, 0};  // in the shifted frame
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const int j = b + 2 * i;
-        bool accept;
+        bool accept = true;  // downhill: accept without a draw
         if ((need_mask >> i) & 1u) {
             const uint64_t k = draw53(st);
             st = pcg_step(st, a.inc);
-            accept = k < s_tab[(K[j >> 2] >> (8 * (j & 3))) & 0xFFu];
-        } else {
-            accept = true;  // downhill: accept without a draw
+            accept = k < s_tab[(K[i >> 1] >> (16 * (i & 1))) & 0xFFu];
         }
-        flip[j >> 2] |= (accept ? 1u : 0u) << (8 * (j & 3));
+        flip[i >> 1] |= (accept ? 1u : 0u) << (16 * (i & 1));
     }
-    uint4 out = make_uint4(C[0] ^ flip[0], C[1] ^ flip[1], C[2] ^ flip[2], C[3] ^ flip[3]);
-    *reinterpret_cast<uint4 *>(a.state + s0) = out;
+    const uint32_t fsh = 8u * (uint32_t)b;
+    *reinterpret_cast<uint4 *>(a.state + s0) = make_uint4(C[0] ^ (flip[0] << fsh), C[1] ^ (flip[1] << fsh),
+                                                          C[2] ^ (flip[2] << fsh), C[3] ^ (flip[3] << fsh));
 }
 
 bool scan_metro_eligible(int d, const int32_t *L) {
-    return (d == 2 || d == 3) && L[0] % 16 == 0 && L[0] >= 16;
+    int64_t n = 1;
+    for (int mu = 0; mu < d; ++mu) n *= L[mu];
+    return (d == 2 || d == 3) && L[0] % 16 == 0 && L[0] >= 16 && n < (int64_t(1) << 32);
 }
 
 int64_t scan_chunks(int64_t n_sites) { return (n_sites + SChunkSites - 1) / SChunkSites; }

@@ -10,6 +10,8 @@ struct ScanArgs {
     uint8_t *state;
     int64_t n_sites;
     int L0, L1, L2;
+    uint32_t dm0, dm1;  // division by L0 and by L1 (Granlund-Montgomery, as Geom)
+    int32_t dl0, dl1;
     int color;
     const uint64_t *metro53;  // decision table (q = 2 environment keys)
     int table_entries;
