@@ -113,3 +113,45 @@ class Ensemble:
     @property
     def launches(self) -> int:
         return int(lib().plq_ensemble_launches(self._h))
+
+
+def batched_workload_spec(seed: int = 20260718):
+    """The batched-ensemble workload: 64 4D Z2 gauge lattices, L in {8, 12, 16,
+    24} with 16 each, beta uniformly spaced over [0.40, 0.48], checkerboard heat
+    bath on links; beside them 256 3D Ising replicas in five parallel-tempering
+    ladders (L in {16, 24, 32, 48, 64}, 52 + 4 x 51 replicas), beta
+    geometrically spaced over [0.20, 0.24] in each ladder, checkerboard
+    Metropolis.  Keyed stream (the reference GPU kernels' randomness), hot
+    starts from per-member seeds.  Returns (descs, starts, ladders) with
+    ladders as (member ids, betas) pairs."""
+    from . import GAUGE, HEATBATH, ISING, METROPOLIS, RNG_KEYED, hot_start, make_desc
+
+    descs, starts, ladders = [], [], []
+    s = seed
+    for L in (8, 12, 16, 24):
+        for beta in np.linspace(0.40, 0.48, 16):
+            start, _ = hot_start(s, 2, 4 * L ** 4)
+            descs.append(make_desc(GAUGE, 2, (L, L, L, L), HEATBATH, beta=float(beta), seed=s, rng=RNG_KEYED,
+                                   sweeps_between=1, batch=1))
+            starts.append(start)
+            s += 1
+    for L, k in ((16, 52), (24, 51), (32, 51), (48, 51), (64, 51)):
+        betas = [float(b) for b in np.geomspace(0.20, 0.24, k)]
+        ids = []
+        for b in betas:
+            start, _ = hot_start(s, 2, L ** 3)
+            ids.append(len(descs))
+            descs.append(make_desc(ISING, 2, (L, L, L), METROPOLIS, beta=b, seed=s, rng=RNG_KEYED,
+                                   sweeps_between=1, batch=1))
+            starts.append(start)
+            s += 1
+        ladders.append((ids, betas))
+    return descs, starts, ladders
+
+
+def build_ensemble(gpu, descs, starts, ladders, seed: int = 20260718, pt_every: int = 10) -> Ensemble:
+    """An ensemble of `descs` from host `starts`, with its tempering ladders."""
+    ens = Ensemble(gpu, descs, starts)
+    for i, (ids, betas) in enumerate(ladders):
+        ens.add_ladder(ids, betas, pt_every, seed=seed + 1000 + i)
+    return ens
