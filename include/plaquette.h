@@ -64,6 +64,10 @@ enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
  * without any device fault.  No reference counterpart (the reference has no
  * staged tiles). */
 #define PLQ_FLAG_TEST_COPY_STALL 4
+/* Run every colour pass one variable per rank (the generic pass body) even
+ * where the four-sites-at-a-time body applies (both give identical results;
+ * used to check one against the other). */
+#define PLQ_FLAG_GENERIC_PASS 8
 
 typedef struct plq_ctx plq_ctx;
 typedef struct plq_chain plq_chain;

@@ -21,6 +21,7 @@
 #include "plq_local.h"
 #include "plq_scan.h"
 #include "plq_tables.h"
+#include "plq_words.cuh"
 
 using namespace plq;
 
@@ -357,6 +358,8 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
             w *= 2 * desc->d + 1;
         }
         c->lookback = desc->rng == PLQ_RNG_STREAM && desc->updater == PLQ_METROPOLIS;
+        c->words = !c->lookback && !(desc->flags & PLQ_FLAG_GENERIC_PASS) &&
+                   words_eligible(desc->model, c->q, c->d, c->g.L, desc->updater, desc->rng);
         // the fused two-colour sweep where a variable's draw is a closed form
         size_t table_bytes = desc->updater == PLQ_HEATBATH
                                  ? (desc->rng == PLQ_RNG_STREAM ? t.hb53.size() * 8 : t.hb24.size() * 4)
@@ -411,6 +414,7 @@ static LocalArgs local_args(plq_chain *c) {
     a.ctrl = c->d_ctrl;
     a.desc = c->d_desc;
     a.n_chunks = c->n_chunks;
+    a.words = c->words ? 1 : 0;
     return a;
 }
 
@@ -710,6 +714,6 @@ extern "C" const char *plq_chain_path(plq_chain *c) {
     if (!c) return "";
     if (c->cluster) return "cluster";
     if (c->fused) return "fused3d";
-    return c->lookback ? "lookback" : "pass";
+    return c->lookback ? "lookback" : (c->words ? "words" : "pass");
 }
 extern "C" void plq_chain_destroy(plq_chain *c) { chain_free(c); }

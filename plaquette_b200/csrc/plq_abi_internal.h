@@ -23,6 +23,7 @@ struct plq_chain {
     plq_chain_desc desc;
     int q = 2, d = 1;
     bool link = false, cluster = false, lookback = false;
+    bool words = false;  // passes four sites at a time (plq_words.cuh)
     int64_t n_sites = 0, n_vars = 0;
     plq::Geom g;
     uint32_t seed32 = 0;

@@ -102,6 +102,7 @@ struct LocalArgs {
     uint32_t epoch;
     int pos_in;               // which ctrl->pos[] to read; the other is written
     int64_t n_chunks;
+    int words;                // run the pass four sites at a time (plq_words.cuh)
 };
 
 }  // namespace plq

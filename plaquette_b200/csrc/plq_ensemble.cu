@@ -41,6 +41,7 @@
 #include "plq_local.h"
 #include "plq_local_impl.cuh"
 #include "plq_tables.h"
+#include "plq_words.cuh"
 
 using namespace plq;
 
@@ -139,8 +140,35 @@ __device__ void grid_barrier(const EnsArgs &e) {
     __syncthreads();
 }
 
+template <int D, int R>
+__device__ void run_words(const LocalArgs &a, int link, int64_t chunk) {
+    const bool st = a.jump != nullptr;
+    if (link) {
+        if (D >= 2) {
+            if (st) link_words_chunk<D, true, R>(a, chunk);
+            else link_words_chunk<D, false, R>(a, chunk);
+        }
+    } else if (a.q == 3) {
+        if (st) site_words_chunk<D, 3, true, R>(a, chunk);
+        else site_words_chunk<D, 3, false, R>(a, chunk);
+    } else {
+        if (st) site_words_chunk<D, 2, true, R>(a, chunk);
+        else site_words_chunk<D, 2, false, R>(a, chunk);
+    }
+}
+
 template <int R>
 __device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk) {
+    if (a.words) {
+        switch (d) {
+            case 1: run_words<1, R>(a, link, chunk); break;
+            case 2: run_words<2, R>(a, link, chunk); break;
+            case 3: run_words<3, R>(a, link, chunk); break;
+            case 4: run_words<4, R>(a, link, chunk); break;
+            default: break;
+        }
+        return;
+    }
     if (link) {
         switch (d) {
             case 2: local_chunk<2, true, false, R>(a, chunk); break;
@@ -399,8 +427,10 @@ int build_items(plq_ensemble *E) {
         spb.push_back((int64_t)im.size());
         for (size_t m = 0; m < E->members.size(); ++m) {
             if (sp >= E->members[m].passes) continue;
-            int64_t half = E->members[m].a.g.n_sites / 2;
-            int64_t nc = (half + chunk - 1) / chunk;
+            const LocalArgs &ma = E->members[m].a;
+            // work per item: 256 * ranks colour ranks, or 256 * ranks four-site words
+            const int64_t units = ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2;
+            int64_t nc = (units + chunk - 1) / chunk;
             for (int64_t c = 0; c < nc; ++c) {
                 im.push_back((int32_t)m);
                 ic.push_back((int32_t)c);
@@ -544,6 +574,8 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
             w *= 2 * d.d + 1;
         }
         a.seed32 = plq_fold_seed(d.seed);
+        a.words = !(d.flags & PLQ_FLAG_GENERIC_PASS) &&
+                  words_eligible(d.model, q, d.d, a.g.L, d.updater, d.rng) ? 1 : 0;
         // state (links: direction planes)
         uint8_t *st = nullptr;
         ce = cudaMalloc((void **)&st, (size_t)mem.n_vars);
@@ -1105,6 +1137,8 @@ int job_admit(plq_server *S, ServerJob *j, cudaStream_t stream) {
         w *= 2 * d.d + 1;
     }
     a.seed32 = plq_fold_seed(d.seed);
+    a.words = !(d.flags & PLQ_FLAG_GENERIC_PASS) &&
+              words_eligible(d.model, q, d.d, a.g.L, d.updater, d.rng) ? 1 : 0;
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void **p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
@@ -1226,7 +1260,9 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         spb.push_back((int64_t)im.size());
         for (size_t m = 0; m < n; ++m) {
             if (sp >= mems[m].passes) continue;
-            int64_t nc = (mems[m].a.g.n_sites / 2 + chunk - 1) / chunk;
+            const LocalArgs &ma = mems[m].a;
+            const int64_t units = ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2;
+            int64_t nc = (units + chunk - 1) / chunk;
             for (int64_t c = 0; c < nc; ++c) {
                 im.push_back((int32_t)m);
                 ic.push_back((int32_t)c);

@@ -24,8 +24,49 @@
 #include "plq_device.cuh"
 #include "plq_local.h"
 #include "plq_local_impl.cuh"
+#include "plq_words.cuh"
 
 namespace plq {
+
+template <int D, bool LINK, int Q, bool STREAM>
+__global__ void __launch_bounds__(kWordThreads) word_pass_kernel(LocalArgs a) {
+    if (LINK)
+        link_words_chunk<D, STREAM, kWordsPerThread>(a, blockIdx.x);
+    else
+        site_words_chunk<D, Q, STREAM, kWordsPerThread>(a, blockIdx.x);
+}
+
+int64_t word_chunks(int64_t n_sites) {
+    const int64_t per = (int64_t)kWordThreads * kWordsPerThread;
+    return (n_sites / 4 + per - 1) / per;
+}
+
+template <int D>
+static cudaError_t launch_words_d(const LocalArgs &a, bool link, cudaStream_t stream) {
+    const unsigned blocks = (unsigned)word_chunks(a.g.n_sites);
+    const bool st = a.jump != nullptr;
+    if (link) {
+        if (st) word_pass_kernel<D, true, 2, true><<<blocks, kWordThreads, 0, stream>>>(a);
+        else word_pass_kernel<D, true, 2, false><<<blocks, kWordThreads, 0, stream>>>(a);
+    } else if (a.q == 3) {
+        if (st) word_pass_kernel<D, false, 3, true><<<blocks, kWordThreads, 0, stream>>>(a);
+        else word_pass_kernel<D, false, 3, false><<<blocks, kWordThreads, 0, stream>>>(a);
+    } else {
+        if (st) word_pass_kernel<D, false, 2, true><<<blocks, kWordThreads, 0, stream>>>(a);
+        else word_pass_kernel<D, false, 2, false><<<blocks, kWordThreads, 0, stream>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_words(const LocalArgs &a, bool link, cudaStream_t stream) {
+    switch (a.g.d) {
+        case 1: return launch_words_d<1>(a, link, stream);
+        case 2: return launch_words_d<2>(a, link, stream);
+        case 3: return launch_words_d<3>(a, link, stream);
+        case 4: return launch_words_d<4>(a, link, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
 
 template <int D, bool LINK, bool LOOKBACK>
 __global__ void __launch_bounds__(kThreads) local_pass_kernel(LocalArgs a) {
@@ -57,6 +98,7 @@ static void launch_d(const LocalArgs &a, bool lookback, cudaStream_t stream, int
 int64_t local_chunks(int64_t n_sites) { return (n_sites / 2 + kChunk - 1) / kChunk; }
 
 cudaError_t launch_local_pass(const LocalArgs &a, bool link, bool lookback, cudaStream_t stream) {
+    if (a.words && !lookback) return launch_words(a, link, stream);
     int64_t blocks = local_chunks(a.g.n_sites);
     if (blocks <= 0) return cudaSuccess;
 #define PLQ_CASE(DD)                                              \

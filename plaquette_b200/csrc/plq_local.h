@@ -8,6 +8,8 @@ namespace plq {
 
 // Chunks (CTAs) one colour pass launches; also the look-back descriptor count.
 int64_t local_chunks(int64_t n_sites);
+// CTAs of one four-sites-at-a-time pass (a.words set).
+int64_t word_chunks(int64_t n_sites);
 // One colour pass: sites (link=false) or the links of direction a.dir.
 cudaError_t launch_local_pass(const LocalArgs &a, bool link, bool lookback, cudaStream_t stream);
 

@@ -29,31 +29,12 @@ __device__ __forceinline__ unsigned long long make_desc(uint32_t epoch, unsigned
     return ((unsigned long long)(epoch & 0x3FFFFFFFu) << 34) | (st << 32) | value;
 }
 
-template <int D>
-__device__ __forceinline__ void coords_of(const Geom &g, int64_t s, int32_t *x) {
-    uint32_t t = (uint32_t)s;
-#pragma unroll
-    for (int mu = 0; mu < D; ++mu) {
-        uint32_t q = fdiv(t, g.dm[mu], g.dl[mu]);
-        x[mu] = (int32_t)(t - q * (uint32_t)g.L[mu]);
-        t = q;
-    }
-}
-
-template <int D>
-__device__ __forceinline__ int64_t step_plus(const Geom &g, int64_t s, const int32_t *x, int mu) {
-    return x[mu] + 1 < g.L[mu] ? s + g.stride[mu] : s - (int64_t)(g.L[mu] - 1) * g.stride[mu];
-}
-template <int D>
-__device__ __forceinline__ int64_t step_minus(const Geom &g, int64_t s, const int32_t *x, int mu) {
-    return x[mu] > 0 ? s - g.stride[mu] : s + (int64_t)(g.L[mu] - 1) * g.stride[mu];
-}
-
 // Site of colour `color` with rank r among that colour in index order
-// (extent 0 even): s = 2r + b, b fixed by the parity of the row.
+// (extent 0 even): s = 2r + b, b fixed by the parity of the row.  Site
+// indices are below 2^31 (chain validation), so all index math is 32-bit.
 template <int D>
-__device__ __forceinline__ int64_t site_of_rank(const Geom &g, int64_t r, int color, int32_t *x) {
-    const uint32_t even = 2u * (uint32_t)r;  // < 2^31: a site index
+__device__ __forceinline__ uint32_t site_of_rank(const Geom &g, uint32_t r, int color, int32_t *x) {
+    const uint32_t even = 2u * r;
     const uint32_t row = fdiv(even, g.dm[0], g.dl[0]);
     int par = 0;
     uint32_t rr = row;
@@ -65,56 +46,44 @@ __device__ __forceinline__ int64_t site_of_rank(const Geom &g, int64_t r, int co
         x[mu] = c;
         par += c;
     }
-    int b = (color ^ par) & 1;
-    uint32_t s = even + (uint32_t)b;
+    const int b = (color ^ par) & 1;
+    const uint32_t s = even + (uint32_t)b;
     x[0] = (int32_t)(s - row * (uint32_t)g.L[0]);
-    return (int64_t)s;
+    return s;
 }
 
-// Environment of a variable: key into the decision tables, plus the two
-// neighbour counts a Potts Metropolis proposal needs (filled later).
-struct Env {
-    int64_t key;
-    int cur;
-    int prop;
-    int cp, cc;
-};
-
+// Index offsets to the +mu and -mu neighbours of the site at x (periodic).
 template <int D>
-__device__ __forceinline__ void site_env(const LocalArgs &a, int64_t s, const int32_t *x, int cur,
-                                         uint8_t *nb) {
+__device__ __forceinline__ void wrap_offsets(const Geom &g, const int32_t *x, int32_t *op, int32_t *om) {
 #pragma unroll
     for (int mu = 0; mu < D; ++mu) {
-        nb[2 * mu] = a.state[step_plus<D>(a.g, s, x, mu)];
-        nb[2 * mu + 1] = a.state[step_minus<D>(a.g, s, x, mu)];
+        const int32_t st = (int32_t)g.stride[mu];
+        const int32_t span = (g.L[mu] - 1) * st;
+        op[mu] = x[mu] + 1 < g.L[mu] ? st : -span;
+        om[mu] = x[mu] > 0 ? -st : span;
     }
-    (void)cur;
 }
 
+// Staple sum of link (s, mu): over nu != mu, the forward plaquette
+// U_nu(s+mu) U_mu(s+nu) U_nu(s) and the backward one U_nu(s+mu-nu) U_mu(s-nu)
+// U_nu(s-nu), each +1 or -1 (Z2 states 0/1 multiply as XOR).  Links are
+// stored as direction planes of n sites.
 template <int D>
-__device__ __forceinline__ int link_staple_sum(const LocalArgs &a, int64_t s, const int32_t *x,
-                                               int mu) {
-    const int64_t n = a.g.n_sites;
-    const uint8_t *U = a.state;
-    int64_t s_mu = step_plus<D>(a.g, s, x, mu);
-    int32_t xm[D];
-#pragma unroll
-    for (int k = 0; k < D; ++k) xm[k] = x[k];
-    xm[mu] = x[mu] + 1 < a.g.L[mu] ? x[mu] + 1 : 0;
-    int sum = 0;
+__device__ __forceinline__ int link_staple_sum(const uint8_t *U, uint32_t n, uint32_t s, const int32_t *op,
+                                               const int32_t *om, int mu) {
+    const uint8_t *Umu = U + (size_t)mu * n;
+    const uint32_t s_mu = s + (uint32_t)op[mu];
+    int unsat = 0;
 #pragma unroll
     for (int nu = 0; nu < D; ++nu) {
         if (nu == mu) continue;
-        int64_t s_nu = step_plus<D>(a.g, s, x, nu);
-        int64_t s_mnu = step_minus<D>(a.g, s, x, nu);
-        int64_t s_mu_mnu = step_minus<D>(a.g, s_mu, xm, nu);
-        // forward plaquette: U_nu(x+mu) U_mu(x+nu) U_nu(x)
-        int f = U[nu * n + s_mu] ^ U[mu * n + s_nu] ^ U[nu * n + s];
-        // backward plaquette: U_nu(x+mu-nu) U_mu(x-nu) U_nu(x-nu)
-        int bk = U[nu * n + s_mu_mnu] ^ U[mu * n + s_mnu] ^ U[nu * n + s_mnu];
-        sum += (1 - 2 * f) + (1 - 2 * bk);
+        const uint8_t *Unu = U + (size_t)nu * n;
+        const uint32_t s_mnu = s + (uint32_t)om[nu];
+        const int f = Unu[s_mu] ^ Umu[s + (uint32_t)op[nu]] ^ Unu[s];
+        const int bk = Unu[s_mu + (uint32_t)om[nu]] ^ Umu[s_mnu] ^ Unu[s_mnu];
+        unsat += f + bk;
     }
-    return sum;
+    return 2 * (D - 1) - 2 * unsat;  // sum of the 2(D-1) staple products, each +1 or -1
 }
 
 // Heat-bath choice from cut points: number of cut points <= k.
@@ -131,13 +100,15 @@ __device__ __forceinline__ int hb_choose(const T *cut, int qm1, uint64_t k) {
 // of the batched ensemble kernel (plq_ensemble.cu).
 template <int D, bool LINK, bool LOOKBACK, int R>
 __device__ __forceinline__ void local_chunk(const LocalArgs &a, int64_t chunk) {
-    const int64_t half = a.g.n_sites / 2;
+    const uint32_t n = (uint32_t)a.g.n_sites;
+    const uint32_t half = n / 2;
     const bool stream = a.jump != nullptr;
     const int q = a.q;
-    const int64_t r0 = chunk * (int64_t)blockDim.x * R + (int64_t)threadIdx.x * R;
+    const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
     constexpr int kRanksPerThread = R;
+    uint8_t *plane = a.state + (LINK ? (size_t)a.dir * n : (size_t)0);  // the pass's variables
 
-    int64_t vars[kRanksPerThread];
+    int32_t vars[kRanksPerThread];
     uint8_t curs[kRanksPerThread];
     uint8_t props[kRanksPerThread];
     unsigned long long entry[kRanksPerThread];  // decision entry (metro) or key (hb)
@@ -145,38 +116,42 @@ __device__ __forceinline__ void local_chunk(const LocalArgs &a, int64_t chunk) {
 
 #pragma unroll
     for (int i = 0; i < kRanksPerThread; ++i) {
-        int64_t r = r0 + i;
+        const uint32_t r = r0 + i;
         vars[i] = -1;
         entry[i] = 0;
         if (r >= half) continue;
-        int32_t x[D];
-        int64_t s = site_of_rank<D>(a.g, r, a.color, x);
+        int32_t x[D], op[D], om[D];
+        const uint32_t s = site_of_rank<D>(a.g, r, a.color, x);
+        wrap_offsets<D>(a.g, x, op, om);
         int64_t key;
         int cur;
         int prop = 0;
         int cp = 0, cc = 0;
         if (LINK) {
-            int64_t v = (int64_t)a.dir * a.g.n_sites + s;
-            cur = a.state[v];
-            int S = link_staple_sum<D>(a, s, x, a.dir);
+            cur = plane[s];
+            const int S = link_staple_sum<D>(a.state, n, s, op, om, a.dir);
             key = cur + 2 * ((S + 2 * (D - 1)) / 2);
-            vars[i] = s;  // site; the link is (s, dir)
+            vars[i] = (int32_t)s;  // site; the link is (s, dir)
             prop = 1 - cur;
         } else {
             cur = a.state[s];
             uint8_t nb[2 * D];
-            site_env<D>(a, s, x, cur, nb);
+#pragma unroll
+            for (int mu = 0; mu < D; ++mu) {
+                nb[2 * mu] = a.state[s + (uint32_t)op[mu]];
+                nb[2 * mu + 1] = a.state[s + (uint32_t)om[mu]];
+            }
             int64_t packed = 0;
 #pragma unroll
             for (int k = 0; k < 2 * D; ++k) packed += a.pw[nb[k]];
             key = cur + (int64_t)q * packed;
-            vars[i] = s;
+            vars[i] = (int32_t)s;
             if (a.kernel == PLQ_METROPOLIS) {
                 if (q == 2) {
                     prop = 1 - cur;
                 } else {
                     // keyed proposal (metropolis.wgsl:45-55)
-                    uint32_t k24 = keyed24(a.seed32 ^ kProposalKey, (uint32_t)s, a.sweep32);
+                    uint32_t k24 = keyed24(a.seed32 ^ kProposalKey, s, a.sweep32);
                     float u = __fmul_rn((float)k24, 5.9604644775390625e-8f);
                     float scaled = __fmul_rn(u, (float)(q - 1));
                     uint32_t draw = __float2uint_rz(scaled);
@@ -284,9 +259,8 @@ __device__ __forceinline__ void local_chunk(const LocalArgs &a, int64_t chunk) {
 #pragma unroll
     for (int i = 0; i < kRanksPerThread; ++i) {
         if (vars[i] < 0) continue;
-        int64_t s = vars[i];
-        int64_t v = LINK ? (int64_t)a.dir * a.g.n_sites + s : s;
-        uint32_t key_var = LINK ? (uint32_t)(s * D + a.dir) : (uint32_t)s;
+        const uint32_t s = (uint32_t)vars[i];
+        const uint32_t key_var = LINK ? s * (uint32_t)D + (uint32_t)a.dir : s;
         int out;
         if (a.kernel == PLQ_METROPOLIS) {
             bool accept;
@@ -314,7 +288,7 @@ __device__ __forceinline__ void local_chunk(const LocalArgs &a, int64_t chunk) {
                 out = hb_choose(a.hb24 + key * (q - 1), q - 1, (uint64_t)k);
             }
         }
-        a.state[v] = (uint8_t)out;
+        plane[s] = (uint8_t)out;
     }
 }
 

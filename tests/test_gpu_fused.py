@@ -51,7 +51,7 @@ def test_fused_equals_pass_kernels(gpu, mode):
         d = plq.make_desc(kind, q, shape, kernel, beta=0.4, seed=99, rng=rng, stream_offset=off,
                           sweeps_between=6, batch=1, flags=flags)
         c = plq.GpuChain(gpu, d, start)
-        assert c.path == ("fused3d" if flags == 0 else ("lookback" if kernel == plq.METROPOLIS and rng == plq.RNG_STREAM else "pass"))
+        assert c.path == ("fused3d" if flags == 0 else ("lookback" if kernel == plq.METROPOLIS and rng == plq.RNG_STREAM else "words"))
         outs.append(next(c))
         if rng == plq.RNG_STREAM:
             outs.append(c.stream_position())

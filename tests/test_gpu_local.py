@@ -206,3 +206,40 @@ def test_batch_samples_equal_sequential(oracle, gpu):
     for s in samples:
         oracle.local_sweeps(model, lat, want, plq.HEATBATH, 1.0, r, 2)
         assert np.array_equal(s, want)
+
+
+WORD_CASES = [
+    (plq.ISING, 2, (256, 128), plq.METROPOLIS, plq.RNG_KEYED, 0.4406868),
+    (plq.ISING, 2, (32, 24, 16), plq.HEATBATH, plq.RNG_STREAM, 0.2216544),
+    (plq.ISING, 2, (12, 8, 6, 4), plq.HEATBATH, plq.RNG_KEYED, 0.15),
+    (plq.ISING, 2, (4, 6, 8), plq.METROPOLIS, plq.RNG_KEYED, 0.3),
+    (plq.POTTS, 3, (40, 36), plq.HEATBATH, plq.RNG_STREAM, 1.0050),
+    (plq.POTTS, 3, (24, 16, 10), plq.HEATBATH, plq.RNG_KEYED, 0.5505),
+    (plq.POTTS, 3, (8, 6, 4, 4), plq.HEATBATH, plq.RNG_STREAM, 0.4),
+    (plq.POTTS, 2, (128,), plq.HEATBATH, plq.RNG_STREAM, 0.9),
+    (plq.GAUGE, 2, (16, 12), plq.HEATBATH, plq.RNG_STREAM, 0.7),
+    (plq.GAUGE, 2, (12, 8, 6), plq.METROPOLIS, plq.RNG_KEYED, 0.6),
+    (plq.GAUGE, 2, (16, 16, 16, 16), plq.HEATBATH, plq.RNG_STREAM, 0.4407),
+    (plq.GAUGE, 2, (12, 4, 6, 8), plq.HEATBATH, plq.RNG_KEYED, 0.5),
+    (plq.GAUGE, 2, (4, 4, 4, 4), plq.METROPOLIS, plq.RNG_KEYED, 0.44),
+]
+
+
+@pytest.mark.parametrize("case", WORD_CASES, ids=lambda c: f"{['ising','potts','gauge'][c[0]]}{c[1]}-"
+                         f"{'x'.join(map(str, c[2]))}-{'metro' if c[3] == plq.METROPOLIS else 'hb'}-"
+                         f"{'stream' if c[4] == plq.RNG_STREAM else 'keyed'}")
+def test_word_passes_equal_generic(gpu, case):
+    # four sites at a time (extent 0 a multiple of 4) == one variable per rank, bit for bit
+    kind, q, shape, kernel, rng_mode, beta = case
+    n_vars = int(np.prod(shape)) * (len(shape) if kind == plq.GAUGE else 1)
+    start, off = plq.hot_start(77, q, n_vars)
+    outs = []
+    for flags in (0, plq.FLAG_GENERIC_PASS):
+        d = plq.make_desc(kind, q, shape, kernel, beta=beta, seed=77, rng=rng_mode, stream_offset=off,
+                          sweeps_between=5, batch=1, flags=flags)
+        c = plq.GpuChain(gpu, d, start)
+        assert c.path == ("words" if flags == 0 else "pass")
+        outs.append((next(c), c.stream_position() if rng_mode == plq.RNG_STREAM else 0, list(c.primaries())))
+        c.close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1:] == outs[1][1:]
