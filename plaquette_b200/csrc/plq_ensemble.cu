@@ -157,9 +157,11 @@ __device__ void run_words(const LocalArgs &a, int link, int64_t chunk) {
     }
 }
 
-template <int R>
+// WORDS_ONLY: every member runs four sites at a time, so the generic body is
+// compiled out (far fewer registers, more CTAs per SM).
+template <int R, bool WORDS_ONLY>
 __device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk) {
-    if (a.words) {
+    if (WORDS_ONLY || a.words) {
         switch (d) {
             case 1: run_words<1, R>(a, link, chunk); break;
             case 2: run_words<2, R>(a, link, chunk); break;
@@ -169,6 +171,7 @@ __device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk) {
         }
         return;
     }
+    if (WORDS_ONLY) return;
     if (link) {
         switch (d) {
             case 2: local_chunk<2, true, false, R>(a, chunk); break;
@@ -306,7 +309,7 @@ __device__ void swap_phase(const EnsArgs &e, unsigned long long att) {
     }
 }
 
-template <int R>
+template <int R, bool WORDS_ONLY>
 __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
     for (unsigned long long t = 0; t < e.sweeps; ++t) {
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
                 int m = e.item_member[i];
                 if (threadIdx.x == 0) item_args(e, m, sp, t, sa);
                 __syncthreads();
-                run_item<R>(sa, sa.g.d, e.members[m].link, e.item_chunk[i]);
+                run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i]);
                 __syncthreads();
             }
             grid_barrier(e);
@@ -379,8 +382,9 @@ struct plq_ensemble {
     LaunchState *d_ls = nullptr;
     Control *d_ctrl = nullptr;
     // work items for the current configuration
-    int ranks = 8;
+    int ranks = 4;
     int ctas_per_sm = 2;
+    bool words_only = false;  // every member runs four sites at a time
     int32_t *d_item_member = nullptr, *d_item_chunk = nullptr;
     int64_t *d_sp_begin = nullptr;
     int n_sp = 0;
@@ -493,21 +497,21 @@ EnsArgs ens_args(plq_ensemble *E, uint64_t sweeps) {
 }
 
 template <int R>
-const void *kernel_for() {
-    return (const void *)ensemble_kernel<R>;
+const void *kernel_for(bool words_only) {
+    return words_only ? (const void *)ensemble_kernel<R, true> : (const void *)ensemble_kernel<R, false>;
 }
 
-const void *kernel_ptr(int ranks) {
+const void *kernel_ptr(int ranks, bool words_only) {
     switch (ranks) {
-        case 2: return kernel_for<2>();
-        case 4: return kernel_for<4>();
-        default: return kernel_for<8>();
+        case 2: return kernel_for<2>(words_only);
+        case 4: return kernel_for<4>(words_only);
+        default: return kernel_for<8>(words_only);
     }
 }
 
-int max_ctas_per_sm(int ranks) {
+int max_ctas_per_sm(int ranks, bool words_only) {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_ptr(ranks), kEnsThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_ptr(ranks, words_only), kEnsThreads, 0);
     return n;
 }
 
@@ -515,7 +519,8 @@ cudaError_t launch_persistent(plq_ensemble *E, uint64_t sweeps) {
     EnsArgs a = ens_args(E, sweeps);
     void *params[] = {&a};
     dim3 grid((unsigned)(E->ctx->sm_count * E->ctas_per_sm));
-    return cudaLaunchCooperativeKernel(kernel_ptr(E->ranks), grid, dim3(kEnsThreads), params, 0, E->stream);
+    return cudaLaunchCooperativeKernel(kernel_ptr(E->ranks, E->words_only), grid, dim3(kEnsThreads), params, 0,
+                                       E->stream);
 }
 
 }  // namespace
@@ -664,7 +669,9 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
     if (ce == cudaSuccess) ce = dev_upload(E, &ctrl, 1, &E->d_ctrl);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
     if (ce != cudaSuccess) return fail(ens_fail(ce, "ensemble set-up"));
-    E->ctas_per_sm = std::max(1, std::min(2, max_ctas_per_sm(E->ranks)));
+    E->words_only = true;
+    for (auto &m : E->members) E->words_only = E->words_only && m.a.words;
+    E->ctas_per_sm = std::max(1, std::min(4, max_ctas_per_sm(E->ranks, E->words_only)));
     int rc = build_items(E);
     if (rc != PLQ_OK) return fail(rc);
     *out = E;
@@ -859,7 +866,7 @@ extern "C" int plq_ensemble_set_config(plq_ensemble *E, int32_t ranks_per_thread
     if (!E) return plq_fail(PLQ_EINVAL, "NULL ensemble");
     if (ranks_per_thread != 2 && ranks_per_thread != 4 && ranks_per_thread != 8)
         return plq_fail(PLQ_EINVAL, "ranks per thread must be 2, 4 or 8");
-    int maxc = max_ctas_per_sm(ranks_per_thread);
+    int maxc = max_ctas_per_sm(ranks_per_thread, E->words_only);
     if (ctas_per_sm < 1 || ctas_per_sm > maxc)
         return plq_fail(PLQ_EINVAL, "CTAs per SM must be in 1.." + std::to_string(maxc));
     E->ranks = ranks_per_thread;
@@ -920,7 +927,7 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     for (int r : {2, 4, 8}) {
-        int maxc = max_ctas_per_sm(r);
+        int maxc = max_ctas_per_sm(r, E->words_only);
         for (int c = 1; c <= std::min(maxc, 4); c *= 2) {
             if (plq_ensemble_set_config(E, r, c) != PLQ_OK) continue;
             snapshot(false);
@@ -1252,7 +1259,7 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         msw[m] = S->active[m]->msweep;
         max_passes = std::max(max_passes, mems[m].passes);
     }
-    const int ranks = 8;
+    const int ranks = 4;
     const int64_t chunk = (int64_t)kEnsThreads * ranks;
     std::vector<int32_t> im, ic;
     std::vector<int64_t> spb;
@@ -1327,9 +1334,11 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
     a.sweeps = sweeps;
     a.ranks = ranks;
     void *params[] = {&a};
-    int ctas = std::max(1, std::min(2, max_ctas_per_sm(ranks)));
+    bool words_only = true;
+    for (size_t m = 0; m < n; ++m) words_only = words_only && mems[m].a.words;
+    int ctas = std::max(1, std::min(4, max_ctas_per_sm(ranks, words_only)));
     dim3 grid((unsigned)(S->ctx->sm_count * ctas));
-    e = cudaLaunchCooperativeKernel(kernel_ptr(ranks), grid, dim3(kEnsThreads), params, 0, stream);
+    e = cudaLaunchCooperativeKernel(kernel_ptr(ranks, words_only), grid, dim3(kEnsThreads), params, 0, stream);
     S->launches++;
     unsigned int status = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &B.ctrl->status, sizeof status, cudaMemcpyDeviceToHost, stream);

@@ -103,3 +103,39 @@ def test_tune_keeps_state(gpu):
     for m, ch in enumerate(chains):
         ch.advance(6)
         assert np.array_equal(ens.read(m), ch.read()), m
+
+
+def test_four_site_members_match_their_own_chains(gpu):
+    # every member eligible for the four-sites-at-a-time body: the ensemble runs its
+    # words-only kernel, and each member still equals its own chain
+    specs = [
+        (plq.ISING, 2, (16, 16, 16), plq.METROPOLIS, plq.RNG_KEYED, 0.2216544, 11),
+        (plq.ISING, 2, (24, 12, 8), plq.HEATBATH, plq.RNG_STREAM, 0.21, 12),
+        (plq.POTTS, 3, (12, 8, 8), plq.HEATBATH, plq.RNG_KEYED, 0.5505, 13),
+        (plq.GAUGE, 2, (8, 8, 8, 8), plq.HEATBATH, plq.RNG_KEYED, 0.44, 14),
+        (plq.GAUGE, 2, (12, 4, 4, 8), plq.HEATBATH, plq.RNG_STREAM, 0.40, 15),
+        (plq.GAUGE, 2, (4, 6, 6), plq.METROPOLIS, plq.RNG_KEYED, 0.7, 16),
+    ]
+    descs, starts = [], []
+    for kind, q, shape, upd, rng, beta, seed in specs:
+        n = int(np.prod(shape)) * (len(shape) if kind == plq.GAUGE else 1)
+        start, off = plq.hot_start(seed, q, n)
+        descs.append(plq.make_desc(kind, q, shape, upd, beta=beta, seed=seed, rng=rng, stream_offset=off,
+                                   sweeps_between=1, batch=1))
+        starts.append(start)
+    ens = Ensemble(gpu, descs, starts)
+    chains = [plq.GpuChain(gpu, d, s) for d, s in zip(descs, starts)]
+    for c in chains:
+        assert c.path == "words"
+    ens.advance(6)
+    for c in chains:
+        c.advance(6)
+    for m, c in enumerate(chains):
+        assert np.array_equal(ens.read(m), c.read()), m
+    for r, k in ((2, 1), (4, 2), (8, 1)):
+        ens.set_config(r, k)
+        ens.advance(2)
+    for c in chains:
+        c.advance(6)
+    for m, c in enumerate(chains):
+        assert np.array_equal(ens.read(m), c.read()), m
