@@ -190,10 +190,10 @@ __device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk) {
     }
 }
 
-// The member's pass arguments for super-phase sp of sweep index `sweep`.
-__device__ void item_args(const EnsArgs &e, int m, int sp, unsigned long long sweep_in_launch, LocalArgs &sa) {
+// The pass-specific fields of member m's arguments (already copied into sa)
+// for super-phase sp of sweep index `sweep`.
+__device__ void item_pass_fields(const EnsArgs &e, int m, int sp, unsigned long long sweep_in_launch, LocalArgs &sa) {
     const EnsMember &mem = e.members[m];
-    sa = mem.a;
     const TableSet &ts = e.tsets[e.ts_of_member[m]];
     sa.hb53 = ts.hb53;
     sa.hb24 = ts.hb24;
@@ -309,6 +309,8 @@ __device__ void swap_phase(const EnsArgs &e, unsigned long long att) {
     }
 }
 
+static_assert(sizeof(LocalArgs) % 4 == 0, "work items copy LocalArgs as 32-bit words");
+
 template <int R, bool WORDS_ONLY>
 __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
@@ -316,7 +318,15 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
         for (int sp = 0; sp < e.n_sp; ++sp) {
             for (int64_t i = e.sp_begin[sp] + blockIdx.x; i < e.sp_begin[sp + 1]; i += gridDim.x) {
                 int m = e.item_member[i];
-                if (threadIdx.x == 0) item_args(e, m, sp, t, sa);
+                // the member's arguments into shared memory, one 32-bit word per thread, then the
+                // pass-specific fields
+                {
+                    const uint32_t *src = reinterpret_cast<const uint32_t *>(&e.members[m].a);
+                    uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
+                    for (int k = threadIdx.x; k < (int)(sizeof(LocalArgs) / 4); k += blockDim.x) dst[k] = src[k];
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) item_pass_fields(e, m, sp, t, sa);
                 __syncthreads();
                 run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i]);
                 __syncthreads();
