@@ -316,20 +316,22 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
     for (unsigned long long t = 0; t < e.sweeps; ++t) {
         for (int sp = 0; sp < e.n_sp; ++sp) {
+            int last_m = -1;  // the arguments in shared memory (same member, same pass: reuse them)
             for (int64_t i = e.sp_begin[sp] + blockIdx.x; i < e.sp_begin[sp + 1]; i += gridDim.x) {
                 int m = e.item_member[i];
-                // the member's arguments into shared memory, one 32-bit word per thread, then the
-                // pass-specific fields
-                {
+                if (m != last_m) {
+                    // the member's arguments into shared memory, one 32-bit word per thread, then
+                    // the pass-specific fields
+                    __syncthreads();  // every thread is done with the previous member's arguments
                     const uint32_t *src = reinterpret_cast<const uint32_t *>(&e.members[m].a);
                     uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
                     for (int k = threadIdx.x; k < (int)(sizeof(LocalArgs) / 4); k += blockDim.x) dst[k] = src[k];
+                    __syncthreads();
+                    if (threadIdx.x == 0) item_pass_fields(e, m, sp, t, sa);
+                    __syncthreads();
+                    last_m = m;
                 }
-                __syncthreads();
-                if (threadIdx.x == 0) item_pass_fields(e, m, sp, t, sa);
-                __syncthreads();
                 run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i]);
-                __syncthreads();
             }
             grid_barrier(e);
         }
