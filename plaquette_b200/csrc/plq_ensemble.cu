@@ -1258,37 +1258,55 @@ struct TickBuffers {
 
 int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps) {
     const size_t n = S->active.size();
+    // members that run four sites at a time first: they go to the words-only kernel
+    // (few registers, several CTAs per SM), the rest to a second launch of the full kernel
+    std::vector<size_t> order;
+    for (size_t m = 0; m < n; ++m)
+        if (S->active[m]->mem.a.words) order.push_back(m);
+    const size_t nw = order.size();
+    for (size_t m = 0; m < n; ++m)
+        if (!S->active[m]->mem.a.words) order.push_back(m);
     std::vector<EnsMember> mems(n);
     std::vector<TableSet> tss(n);
     std::vector<int32_t> ts(n);
     std::vector<unsigned long long> pos(n), msw(n);
-    int max_passes = 0;
-    for (size_t m = 0; m < n; ++m) {
-        mems[m] = S->active[m]->mem;
-        tss[m] = S->active[m]->ts;
-        ts[m] = (int32_t)m;
-        pos[m] = S->active[m]->pos;
-        msw[m] = S->active[m]->msweep;
-        max_passes = std::max(max_passes, mems[m].passes);
+    for (size_t k = 0; k < n; ++k) {
+        const ServerJob *j = S->active[order[k]];
+        mems[k] = j->mem;
+        tss[k] = j->ts;
+        ts[k] = (int32_t)k;
+        pos[k] = j->pos;
+        msw[k] = j->msweep;
     }
-    const int ranks = 4;
-    const int64_t chunk = (int64_t)kEnsThreads * ranks;
+    // ranks per thread: 4 for the words-only kernel; 2 for the full kernel, whose generic
+    // body needs the registers (2 CTAs per SM instead of 1)
+    const int ranks_w = 4, ranks_g = 2;
     std::vector<int32_t> im, ic;
     std::vector<int64_t> spb;
-    for (int sp = 0; sp < max_passes; ++sp) {
-        spb.push_back((int64_t)im.size());
-        for (size_t m = 0; m < n; ++m) {
-            if (sp >= mems[m].passes) continue;
-            const LocalArgs &ma = mems[m].a;
-            const int64_t units = ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2;
-            int64_t nc = (units + chunk - 1) / chunk;
-            for (int64_t c = 0; c < nc; ++c) {
-                im.push_back((int32_t)m);
-                ic.push_back((int32_t)c);
+    // work items of members [lo, hi), member indices relative to lo; returns the super-phase count
+    auto build = [&](size_t lo, size_t hi, int ranks) {
+        const int64_t chunk = (int64_t)kEnsThreads * ranks;
+        int max_passes = 0;
+        for (size_t k = lo; k < hi; ++k) max_passes = std::max(max_passes, mems[k].passes);
+        for (int sp = 0; sp < max_passes; ++sp) {
+            spb.push_back((int64_t)im.size());
+            for (size_t k = lo; k < hi; ++k) {
+                if (sp >= mems[k].passes) continue;
+                const LocalArgs &ma = mems[k].a;
+                const int64_t units = ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2;
+                const int64_t nc = (units + chunk - 1) / chunk;
+                for (int64_t c = 0; c < nc; ++c) {
+                    im.push_back((int32_t)(k - lo));
+                    ic.push_back((int32_t)c);
+                }
             }
         }
-    }
-    spb.push_back((int64_t)im.size());
+        spb.push_back((int64_t)im.size());
+        return max_passes;
+    };
+    const int sp_w = build(0, nw, ranks_w);
+    const size_t spb_g = spb.size();
+    const int sp_g = build(nw, n, ranks_g);
     cudaError_t e = cudaSuccess;
     if (!B.ls) {
         e = cudaMalloc((void **)&B.ls, sizeof(LaunchState));
@@ -1321,37 +1339,45 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         B.cap_items = c;
     }
     if (e != cudaSuccess) return plq_fail(PLQ_ENOMEM, std::string("tick buffers: ") + cudaGetErrorString(e));
+    if (spb.size() > 64) return plq_fail(PLQ_EINVAL, "too many passes per sweep for a serving tick");
     cudaMemcpyAsync(B.members, mems.data(), n * sizeof(EnsMember), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.tsets, tss.data(), n * sizeof(TableSet), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.ts, ts.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.pos, pos.data(), n * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.msweep, msw.data(), n * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(B.im, im.data(), im.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(B.ic, ic.data(), ic.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
+    if (!im.empty()) {
+        cudaMemcpyAsync(B.im, im.data(), im.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
+        cudaMemcpyAsync(B.ic, ic.data(), ic.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
+    }
     cudaMemcpyAsync(B.spb, spb.data(), spb.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream);
-    EnsArgs a;
-    std::memset(&a, 0, sizeof a);
-    a.members = B.members;
-    a.n_members = (int)n;
-    a.tsets = B.tsets;
-    a.ts_of_member = B.ts;
-    a.pos = B.pos;
-    a.msweep = B.msweep;
-    a.item_member = B.im;
-    a.item_chunk = B.ic;
-    a.sp_begin = B.spb;
-    a.n_sp = max_passes;
-    a.ls = B.ls;
-    a.ctrl = B.ctrl;
-    a.sweeps = sweeps;
-    a.ranks = ranks;
-    void *params[] = {&a};
-    bool words_only = true;
-    for (size_t m = 0; m < n; ++m) words_only = words_only && mems[m].a.words;
-    int ctas = std::max(1, std::min(4, max_ctas_per_sm(ranks, words_only)));
-    dim3 grid((unsigned)(S->ctx->sm_count * ctas));
-    e = cudaLaunchCooperativeKernel(kernel_ptr(ranks, words_only), grid, dim3(kEnsThreads), params, 0, stream);
-    S->launches++;
+    // one cooperative launch per member group; item indices in the second group's
+    // super-phase bounds continue the first group's, member indices restart at its offset
+    auto launch = [&](size_t lo, size_t hi, int n_sp, size_t spb_off, bool words_only, int ranks) -> cudaError_t {
+        if (hi == lo || n_sp == 0) return cudaSuccess;
+        EnsArgs a;
+        std::memset(&a, 0, sizeof a);
+        a.members = B.members + lo;
+        a.n_members = (int)(hi - lo);
+        a.tsets = B.tsets;
+        a.ts_of_member = B.ts + lo;
+        a.pos = B.pos + lo;
+        a.msweep = B.msweep + lo;
+        a.item_member = B.im;
+        a.item_chunk = B.ic;
+        a.sp_begin = B.spb + spb_off;
+        a.n_sp = n_sp;
+        a.ls = B.ls;
+        a.ctrl = B.ctrl;
+        a.sweeps = sweeps;
+        a.ranks = ranks;
+        void *params[] = {&a};
+        const int ctas = std::max(1, std::min(4, max_ctas_per_sm(ranks, words_only)));
+        dim3 grid((unsigned)(S->ctx->sm_count * ctas));
+        S->launches++;
+        return cudaLaunchCooperativeKernel(kernel_ptr(ranks, words_only), grid, dim3(kEnsThreads), params, 0, stream);
+    };
+    e = launch(0, nw, sp_w, 0, true, ranks_w);
+    if (e == cudaSuccess) e = launch(nw, n, sp_g, spb_g, false, ranks_g);
     unsigned int status = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &B.ctrl->status, sizeof status, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
