@@ -491,19 +491,140 @@ def run_ensemble(args):
         pg.destroy_process_group()
 
 
+CLUSTER_WORKLOADS = {
+    # name: (extent, rng, shape, beta, what)
+    "sw-4096-keyed": ("all", "keyed", (4096, 4096), 0.4406868,
+                      "2D Ising 4096^2 periodic Swendsen-Wang, beta=0.4406868, p=1-exp(-2 beta), keyed reference "
+                      "GPU stream, uniform random start"),
+    "sw-4096-stream": ("all", "stream", (4096, 4096), 0.4406868,
+                       "2D Ising 4096^2 periodic Swendsen-Wang, beta=0.4406868, PCG64 reference stream (bit-exact "
+                       "with the reference CPU ClusterUpdate), uniform random start"),
+    "wolff-128-keyed": ("seeded", "keyed", (128, 128, 128), 0.2216544,
+                        "3D Ising 128^3 periodic Wolff (keyed seed site, frontier BFS), beta=0.2216544, uniform "
+                        "random start"),
+}
+
+
+def run_cluster(args):
+    """Cluster moves: Swendsen-Wang sweeps/s (labels, size histogram each
+    sweep available) or Wolff single-cluster updates/s."""
+    import numpy as np
+    import torch
+
+    import plaquette_b200 as plq
+
+    extent, rng_name, shape, beta, what = CLUSTER_WORKLOADS[args.workload]
+    world, rank, local, pg = dist_setup()
+    torch.cuda.set_device(local)
+    gpu = plq.Gpu.new(local)
+    if gpu is None:
+        raise RuntimeError("no CUDA device")
+    seed = SEED + rank
+    n = int(np.prod(shape))
+    start, offset = plq.hot_start(seed, 2, n)
+    rng = plq.RNG_STREAM if rng_name == "stream" else plq.RNG_KEYED
+    ext = plq.EXTENT_ALL if extent == "all" else plq.EXTENT_SEEDED
+    relabel = plq.RELABEL_REDRAW if extent == "all" else plq.RELABEL_FORCED
+    wolff = extent == "seeded"
+    per_step = 1000 if wolff else 1  # Wolff: one step = 1000 single-cluster updates
+
+    def make():
+        d = plq.make_desc(plq.ISING, 2, shape, plq.CLUSTER, beta=beta, seed=seed, rng=rng, stream_offset=offset,
+                          sweeps_between=per_step, batch=1, extent=ext, relabel=relabel)
+        return plq.GpuClusterChain(gpu, d, start)
+
+    chain = make()
+    stream = torch.cuda.ExternalStream(chain.cuda_stream, device=f"cuda:{local}")
+    chain.advance(args.warmup * per_step)
+    chain.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg, local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = chain.launches
+    t_wall0 = time.time()
+    ev0.record(stream)
+    chain.advance(args.steps * per_step)
+    ev1.record(stream)
+    ev1.synchronize()
+    t_wall1 = time.time()
+    chain.sync()
+    launches = chain.launches - launches0
+    clock_info = clocks.stop(t_wall0, t_wall1)
+    dev_ms = max_over_ranks(pg, ev0.elapsed_time(ev1), local)
+    units = args.steps * per_step * world
+    value = units / (dev_ms * 1e-3)
+    hist = chain.size_histogram(32)
+    chain.close()
+
+    # end to end: chain from a pinned host start, K steps, size histogram and final configuration back
+    pinned = torch.empty(n, dtype=torch.uint8).pin_memory()
+    pinned.numpy()[:] = start
+    out_pinned = torch.empty(n, dtype=torch.uint8).pin_memory()
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    d = plq.make_desc(plq.ISING, 2, shape, plq.CLUSTER, beta=beta, seed=seed, rng=rng, stream_offset=offset,
+                      sweeps_between=per_step, batch=1, extent=ext, relabel=relabel)
+    ec = plq.GpuClusterChain(gpu, d, pinned.numpy())
+    ec.advance(args.steps * per_step)
+    h2 = ec.size_histogram(32)
+    plq.check(plq.lib().plq_chain_read(ec._h, out_pinned.data_ptr()))
+    t1 = time.perf_counter()
+    ec.close()
+    e2e_s = max_over_ranks(pg, t1 - t0, local)
+    unit = "cluster updates/s" if wolff else "SW sweeps/s"
+    alg = 10.5 * n if not wolff else None  # SW: spins r+w, bond bits r+w, labels w+r (bytes per sweep)
+    line = {
+        "metric": unit, "value": round(value, 2), "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": what, "name": args.workload, "sites": n,
+                   "step": "1000 single-cluster updates" if wolff else "one Swendsen-Wang sweep",
+                   "l2": "state, bonds and labels (16.8 M sites: 101 MB) stream through L2 every sweep" if not wolff
+                   else "cluster work only; the 2.1 MB lattice stays in L2",
+                   "parallelism": f"independent lattice per GPU x{world}"},
+        "roofline": ({"bound": "hbm", "achieved": round(alg * args.steps / (dev_ms * 1e-3) / 1e9, 1),
+                      "peak": measured_peak_hbm()[0], "unit": "GB/s",
+                      "frac": round(alg * args.steps / (dev_ms * 1e-3) / 1e9 / measured_peak_hbm()[0], 4),
+                      "traffic": None, "peak_source": measured_peak_hbm()[1],
+                      "algorithmic_bytes_per_launch": alg, "kernel": "bonds + union-find + flatten + relabel",
+                      "note": "10.5 B/site per sweep algorithmic minimum"} if not wolff else
+                     {"bound": "latency", "achieved": None, "peak": None, "unit": None, "frac": None,
+                      "traffic": None, "note": "frontier BFS: work proportional to the cluster, not the lattice"}),
+        "size_histogram_log2": [int(x) for x in hist[:24]],
+        "e2e": {"value": round(units / e2e_s, 2), "unit": unit, "h2d_bytes_per_step": n / args.steps,
+                "d2h_bytes_per_step": (n + 8 * 32) / args.steps,
+                "what": "chain create from a pinned host start, K steps, cluster-size histogram and final "
+                        "configuration read back"},
+        "gpu_launches": launches,
+        "clocks": clock_info,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
-    ap.add_argument("--workload", default="potts3-512-hb-stream", choices=sorted(WORKLOADS) + [ENSEMBLE_WORKLOAD])
+    ap.add_argument("--workload", default="potts3-512-hb-stream",
+                    choices=sorted(WORKLOADS) + [ENSEMBLE_WORKLOAD] + sorted(CLUSTER_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "product":
         args.warmup = 3
-    if args.impl == "reference" and args.workload == ENSEMBLE_WORKLOAD:
+    if args.impl == "reference" and args.workload in CLUSTER_WORKLOADS:
+        if _env_int("RANK", 0) == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the single-lattice "
+                                                                  "local sweep; cluster moves are measured on the "
+                                                                  "product arm only"}), flush=True)
+    elif args.impl == "reference" and args.workload == ENSEMBLE_WORKLOAD:
         if _env_int("RANK", 0) == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble (one chain "
                                                                   "at a time on the CPU); time a single-lattice "
@@ -512,6 +633,8 @@ def main():
         run_reference(args)
     elif args.workload == ENSEMBLE_WORKLOAD:
         run_ensemble(args)
+    elif args.workload in CLUSTER_WORKLOADS:
+        run_cluster(args)
     else:
         run_product(args)
 

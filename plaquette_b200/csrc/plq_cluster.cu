@@ -268,17 +268,139 @@ __device__ __forceinline__ void unite(int32_t *parent, int32_t a, int32_t b, int
     }
 }
 
+// ---- tile-local labelling: a CTA owns a T0 x T1 tile of (dims 0, 1), T0 and T1
+// the largest power-of-two divisors of L0, L1 capped at 64.  It unites the
+// open bonds inside the tile on a shared-memory parent array (same rule:
+// larger root under smaller, so each local root is the tile component's
+// minimum site; local and global index orders agree), then points every site
+// at its local root.  Only bonds that leave the tile go through the global
+// union-find (boundary_hook_kernel): ~2 / 64 of the bonds of a 2D lattice.
+constexpr int kTileMax = 64;
+constexpr int kTileSites = kTileMax * kTileMax;
+
+__device__ __forceinline__ int tile_extent(int L) {
+    const int p2 = L & -L;  // largest power-of-two divisor
+    return p2 < kTileMax ? p2 : kTileMax;
+}
+
+__device__ __forceinline__ int lfind(int32_t *p, int32_t x, int cap, Control *ctrl) {
+    int32_t px = p[x];
+    int it = 0;
+    while (px != x) {
+        const int32_t gp = p[px];
+        if (gp != px) p[x] = gp;  // path halving: gp is an ancestor
+        x = px;
+        px = gp;
+        if (++it > cap) {
+            atomicOr(&ctrl->status, kStatusPassCap);
+            break;
+        }
+    }
+    return x;
+}
+
+__device__ __forceinline__ void lunite(int32_t *p, int32_t a, int32_t b, int cap, Control *ctrl) {
+    for (int it = 0;; ++it) {
+        a = lfind(p, a, cap, ctrl);
+        b = lfind(p, b, cap, ctrl);
+        if (a == b) return;
+        if (a > b) {
+            const int32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(&p[b], b, a) == b) return;
+        if (it > cap) {
+            atomicOr(&ctrl->status, kStatusPassCap);
+            return;
+        }
+    }
+}
+
 template <int D>
-__global__ void __launch_bounds__(kThreads) hook_kernel(ClusterArgs a) {
+__global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
+    __shared__ int32_t p[kTileSites];
+    const int L0 = a.g.L[0], L1 = D >= 2 ? a.g.L[1] : 1;
+    const int T0 = tile_extent(L0), T1 = D >= 2 ? tile_extent(L1) : 1;
+    const int T = T0 * T1;
+    const int tiles0 = L0 / T0, tiles1 = L1 / T1;
+    // tile origin: (tx * T0, ty * T1, slab) with slab the index over dims >= 2
+    const int64_t bid = blockIdx.x;
+    const int tx = (int)(bid % tiles0);
+    const int64_t r1 = bid / tiles0;
+    const int ty = (int)(r1 % tiles1);
+    const int64_t slab = r1 / tiles1;
+    const int64_t base = slab * (int64_t)L0 * L1 + (int64_t)ty * T1 * L0 + (int64_t)tx * T0;
+    const int cap = a.cap < kTileSites + 64 ? a.cap : kTileSites + 64;
+    for (int li = threadIdx.x; li < T; li += blockDim.x) p[li] = li;
+    __syncthreads();
+    for (int li = threadIdx.x; li < T; li += blockDim.x) {
+        const int xl = li % T0, yl = li / T0;
+        const int64_t s = base + xl + (int64_t)yl * L0;
+        const uint8_t b = a.bonds[s];
+        if (b & 1u) {  // +x inside the tile (wrapping when the tile spans the row)
+            if (xl + 1 < T0) lunite(p, li, li + 1, cap, a.ctrl);
+            else if (T0 == L0) lunite(p, li, li - (T0 - 1), cap, a.ctrl);
+        }
+        if (D >= 2 && (b & 2u)) {  // +y inside the tile
+            if (yl + 1 < T1) lunite(p, li, li + T0, cap, a.ctrl);
+            else if (T1 == L1) lunite(p, li, li - T0 * (T1 - 1), cap, a.ctrl);
+        }
+    }
+    __syncthreads();
+    for (int li = threadIdx.x; li < T; li += blockDim.x) {
+        int32_t r = li, pr = p[r];
+        int it = 0;
+        while (pr != r && ++it <= kTileSites) {  // read-only walk to the local root
+            r = pr;
+            pr = p[r];
+        }
+        const int64_t s = base + li % T0 + (int64_t)(li / T0) * L0;
+        a.parent[s] = (int32_t)(base + r % T0 + (int64_t)(r / T0) * L0);
+    }
+}
+
+// Global unions for the open bonds that leave their tile: +x bonds of the
+// tile's last column (when tiles split the rows), +y bonds of its last row
+// (when tiles split dim 1), and every bond along dims >= 2.  Thread t of the
+// grid takes candidate site t of each family in turn.
+template <int D>
+__global__ void __launch_bounds__(kThreads) boundary_hook_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
-        uint8_t b = a.bonds[s];
-        if (!b) continue;
-        int32_t x[D];
-        site_coords<D>(a.g, s, x);
+    const int L0 = a.g.L[0], L1 = D >= 2 ? a.g.L[1] : 1;
+    const int T0 = tile_extent(L0), T1 = D >= 2 ? tile_extent(L1) : 1;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (T0 < L0) {  // sites with x = k*T0 + T0-1: n / T0 of them
+        for (int64_t c = t0; c < n / T0; c += stride) {
+            const int64_t s = c * T0 + (T0 - 1);
+            if (!(a.bonds[s] & 1u)) continue;
+            int32_t x[D];
+            site_coords<D>(a.g, s, x);
+            unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, 0), a.cap, a.ctrl);
+        }
+    }
+    if (D >= 2 && T1 < L1) {  // rows with y = k*T1 + T1-1: n / T1 sites
+        const int64_t per_row = L0;
+        for (int64_t c = t0; c < n / T1; c += stride) {
+            const int64_t row = c / per_row;  // index among the selected rows
+            const int64_t s = (row * T1 + (T1 - 1)) * per_row + (c - row * per_row);
+            if (!(a.bonds[s] & 2u)) continue;
+            int32_t x[D];
+            site_coords<D>(a.g, s, x);
+            unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, 1), a.cap, a.ctrl);
+        }
+    }
+    if (D >= 3) {
+        for (int64_t s = t0; s < n; s += stride) {
+            const uint8_t b = (uint8_t)(a.bonds[s] >> 2);
+            if (!b) continue;
+            int32_t x[D];
+            site_coords<D>(a.g, s, x);
 #pragma unroll
-        for (int mu = 0; mu < D; ++mu)
-            if ((b >> mu) & 1u) unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, mu), a.cap, a.ctrl);
+            for (int mu = 2; mu < D; ++mu)
+                if ((b >> (mu - 2)) & 1u) unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, mu), a.cap, a.ctrl);
+        }
     }
 }
 
@@ -488,12 +610,21 @@ __global__ void sizes_kernel(const int32_t *parent, int32_t *size, int64_t n) {
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
         atomicAdd(&size[parent[s]], 1);
 }
+// Clusters per size bin [2^k, 2^(k+1)): counted per CTA in shared memory (bins
+// 0..31 cover every int32 size), one global atomic per bin per CTA.
 __global__ void size_hist_kernel(const int32_t *parent, const int32_t *size, int64_t n, long long *hist, int nbins) {
+    __shared__ unsigned int bins[32];
+    if (threadIdx.x < 32) bins[threadIdx.x] = 0;
+    __syncthreads();
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
         if (parent[s] != (int32_t)s) continue;
-        int bin = 31 - __clz(size[s]);
+        atomicAdd(&bins[31 - __clz(size[s])], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32 && bins[threadIdx.x]) {
+        int bin = (int)threadIdx.x;
         if (bin >= nbins) bin = nbins - 1;
-        atomicAdd((unsigned long long *)&hist[bin], 1ull);
+        atomicAdd((unsigned long long *)&hist[bin], (unsigned long long)bins[threadIdx.x]);
     }
 }
 
@@ -507,6 +638,7 @@ struct ClusterDev {
     int32_t *queue = nullptr;
     unsigned long long *desc = nullptr;
     int64_t n_chunks = 0;
+    int64_t n_tiles = 0;  // CTAs of tile_hook_kernel
     int32_t *events = nullptr;
     int *first_new = nullptr;
     int32_t *sizes = nullptr;
@@ -584,9 +716,10 @@ int sweep_d(plq_chain *c, uint64_t sweeps) {
         } else {
             bonds_kernel<D, false><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
         }
-        hook_kernel<D><<<gs, kThreads, 0, c->stream>>>(a);
+        tile_hook_kernel<D><<<(unsigned)cd->n_tiles, kThreads, 0, c->stream>>>(a);
+        boundary_hook_kernel<D><<<gs, kThreads, 0, c->stream>>>(a);
         flatten_kernel<<<gs, kThreads, 0, c->stream>>>(a);
-        c->launches += 3;
+        c->launches += 4;
         if (!stream) {
             relabel_keyed_kernel<<<gs, kThreads, 0, c->stream>>>(a);
             c->launches++;
@@ -658,6 +791,11 @@ int cluster_create(plq_chain *c) {
     cd->kp53 = lo53;
     c->pass_cap = (c->desc.flags & PLQ_FLAG_TINY_PASS_CAP) ? 1 : std::min<int64_t>(n + 64, 1 << 30);
     cd->n_chunks = (n + kChunk - 1) / kChunk;
+    {
+        auto tile = [](int64_t L) { const int64_t p2 = L & -L; return p2 < kTileMax ? p2 : (int64_t)kTileMax; };
+        const int64_t t0 = tile(c->g.L[0]), t1 = c->d >= 2 ? tile(c->g.L[1]) : 1;
+        cd->n_tiles = n / (t0 * t1);
+    }
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void **p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
