@@ -195,7 +195,6 @@ __global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
             if (a.state[nbr_plus(a.g, s, x, mu)] == cur) m |= (uint8_t)(1u << mu);
         agree[i] = m;
         count += __popc(m);
-        a.parent[s] = (int32_t)s;  // label init (cluster_prelude.wgsl:83-93)
     }
     u128 st{0, 0};
     if (STREAM) {
@@ -273,7 +272,8 @@ __device__ __forceinline__ void unite(int32_t *parent, int32_t a, int32_t b, int
 // open bonds inside the tile on a shared-memory parent array (same rule:
 // larger root under smaller, so each local root is the tile component's
 // minimum site; local and global index orders agree), then points every site
-// at its local root.  Only bonds that leave the tile go through the global
+// at its local root -- this is also the label init (cluster_prelude.wgsl:83-93)
+// of every site.  Only bonds that leave the tile go through the global
 // union-find (boundary_hook_kernel): ~2 / 64 of the bonds of a 2D lattice.
 constexpr int kTileMax = 64;
 constexpr int kTileSites = kTileMax * kTileMax;
@@ -332,15 +332,33 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     const int64_t slab = r1 / tiles1;
     const int64_t base = slab * (int64_t)L0 * L1 + (int64_t)ty * T1 * L0 + (int64_t)tx * T0;
     const int cap = a.cap < kTileSites + 64 ? a.cap : kTileSites + 64;
-    for (int li = threadIdx.x; li < T; li += blockDim.x) p[li] = li;
+    // x runs first: a warp holds 32 consecutive sites; each site points straight at
+    // the start of its run of open +x bonds (the run's minimum), found with one ballot
+    const int lane = threadIdx.x & 31;
+    const int rounds = (T + (int)blockDim.x - 1) / (int)blockDim.x;
+    for (int k = 0; k < rounds; ++k) {
+        const int li = k * (int)blockDim.x + (int)threadIdx.x;
+        const bool valid = li < T;
+        const int xl = li % T0;
+        // the bond into this site from its -x neighbour, inside this warp's segment
+        bool joined = false;
+        if (valid && lane > 0 && xl > 0) joined = (a.bonds[base + (xl - 1) + (int64_t)(li / T0) * L0] & 1u) != 0;
+        const unsigned starts = __ballot_sync(0xffffffffu, !joined);
+        const int start = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
+        if (valid) p[li] = li - lane + start;
+    }
     __syncthreads();
+    // the remaining bonds inside the tile: +x across a warp segment or around the row, and +y
     for (int li = threadIdx.x; li < T; li += blockDim.x) {
         const int xl = li % T0, yl = li / T0;
         const int64_t s = base + xl + (int64_t)yl * L0;
         const uint8_t b = a.bonds[s];
-        if (b & 1u) {  // +x inside the tile (wrapping when the tile spans the row)
-            if (xl + 1 < T0) lunite(p, li, li + 1, cap, a.ctrl);
-            else if (T0 == L0) lunite(p, li, li - (T0 - 1), cap, a.ctrl);
+        if (b & 1u) {
+            if (xl + 1 < T0) {
+                if ((li & 31) == 31) lunite(p, li, li + 1, cap, a.ctrl);
+            } else if (T0 == L0) {
+                lunite(p, li, li - (T0 - 1), cap, a.ctrl);
+            }
         }
         if (D >= 2 && (b & 2u)) {  // +y inside the tile
             if (yl + 1 < T1) lunite(p, li, li + T0, cap, a.ctrl);
@@ -348,13 +366,21 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
         }
     }
     __syncthreads();
-    for (int li = threadIdx.x; li < T; li += blockDim.x) {
-        int32_t r = li, pr = p[r];
-        int it = 0;
-        while (pr != r && ++it <= kTileSites) {  // read-only walk to the local root
-            r = pr;
-            pr = p[r];
+    // pointer jumping to the local roots: a pointer only ever moves to an ancestor,
+    // so concurrent jumps are safe; log2(depth) + 1 rounds (bounded)
+    for (int round = 0; round < 32; ++round) {
+        int changed = 0;
+        for (int li = threadIdx.x; li < T; li += blockDim.x) {
+            const int32_t pl = p[li], pp = p[pl];
+            if (pp != pl) {
+                p[li] = pp;
+                changed = 1;
+            }
         }
+        if (!__syncthreads_or(changed)) break;
+    }
+    for (int li = threadIdx.x; li < T; li += blockDim.x) {
+        const int32_t r = p[li];
         const int64_t s = base + li % T0 + (int64_t)(li / T0) * L0;
         a.parent[s] = (int32_t)(base + r % T0 + (int64_t)(r / T0) * L0);
     }
