@@ -39,7 +39,16 @@ constexpr int FTHREADS = 256;
 constexpr int FRUN = 16;                      // bytes per run
 constexpr int FRUNS_PER_THREAD = 2;
 constexpr int FPLANE_SITES = FTHREADS * FRUNS_PER_THREAD * FRUN;  // 8192 interior sites per plane
-constexpr int FPREF = 3, FNS = FPREF + 5;     // ring of 8 planes
+// Ring depth and CTAs per SM by kernel variant: planes are prefetched FPREF
+// steps ahead into a ring of FPREF + 5 slots (planes z-1..z+2 in use, z+3..
+// z+FPREF+3 in flight).  Three CTAs per SM (FPREF 2, 75 KB of shared memory
+// each) measured faster for all but the keyed q = 3 heat bath (two CTAs, FPREF 3).
+template <int Q, bool STREAM>
+struct FusedCfg {
+    static constexpr int ctas = (Q == 3 && !STREAM) ? 2 : 3;
+    static constexpr int pref = ctas == 3 ? 2 : 3;
+    static constexpr int slots = pref + 5;
+};
 constexpr int FTABLE_BYTES = 4096;
 constexpr int FMAX_L0 = 512;  // 2 ring rows of L0/4 words: one word per thread
 
@@ -181,9 +190,10 @@ __device__ __forceinline__ uint4 update_run(const FusedArgs &a, const uint8_t *t
 }
 
 template <int Q, bool STREAM, bool HB>
-__global__ void __launch_bounds__(FTHREADS, 2)
+__global__ void __launch_bounds__(FTHREADS, FusedCfg<Q, STREAM>::ctas)
     fused3d_kernel(const FusedArgs a, const __grid_constant__ CUtensorMap tm_rows,
                    const __grid_constant__ CUtensorMap tm_halo) {
+    constexpr int FPREF = FusedCfg<Q, STREAM>::pref, FNS = FusedCfg<Q, STREAM>::slots;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // TMA destinations start on 128-byte boundaries: align the base here
     // (the launch reserves 128 bytes for it) rather than trust the window's.
@@ -355,8 +365,8 @@ int fused3d_default_tz(int L2) {
     return 0;
 }
 
-size_t fused3d_smem_bytes(int L0) {
-    return 128 + (size_t)FNS * (size_t)L0 * (size_t)(fused_ty(L0) + 4) + FTABLE_BYTES + FNS * sizeof(uint64_t);
+size_t fused3d_smem_bytes(int L0, int slots) {
+    return 128 + (size_t)slots * (size_t)L0 * (size_t)(fused_ty(L0) + 4) + FTABLE_BYTES + slots * sizeof(uint64_t);
 }
 int fused3d_table_limit_bytes() { return FTABLE_BYTES; }
 
@@ -392,7 +402,7 @@ cudaError_t fused3d_make_maps(const uint8_t *buf, int L0, int L1, int L2, FusedM
 template <int Q, bool STREAM, bool HB>
 static cudaError_t launch_t(FusedArgs a, const FusedMaps &m, cudaStream_t s) {
     auto kern = fused3d_kernel<Q, STREAM, HB>;
-    size_t smem = fused3d_smem_bytes(a.L0);
+    size_t smem = fused3d_smem_bytes(a.L0, FusedCfg<Q, STREAM>::slots);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     a.ty = fused_ty(a.L0);

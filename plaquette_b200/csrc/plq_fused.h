@@ -33,7 +33,7 @@ struct FusedMaps {
 
 bool fused3d_eligible(int model, int q, int d, const int32_t *L, int updater, int rng);
 int fused3d_default_tz(int L2);
-size_t fused3d_smem_bytes(int L0);
+size_t fused3d_smem_bytes(int L0, int slots);
 int fused3d_table_limit_bytes();
 cudaError_t fused3d_make_maps(const uint8_t *buf, int L0, int L1, int L2, FusedMaps *out);
 cudaError_t launch_fused3d(const FusedArgs &a, const FusedMaps &maps, int q, bool stream, bool hb, cudaStream_t s);
