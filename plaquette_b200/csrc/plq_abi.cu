@@ -236,14 +236,40 @@ void chain_free(plq_chain *c) {
     if (!c) return;
     if (c->ctx) cudaSetDevice(c->ctx->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->obs_stream) cudaStreamSynchronize(c->obs_stream);
     cluster_free(c);
     void *ptrs[] = {c->d_state, c->d_state_alt, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
                     c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->obs_stream) cudaStreamDestroy(c->obs_stream);
+    if (c->swept) cudaEventDestroy(c->swept);
+    for (cudaEvent_t ev : c->measured)
+        if (ev) cudaEventDestroy(ev);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
+}
+
+// Index of the first byte >= q (q <= 64) in a[0, n), or -1.  Sixty-four bytes per
+// step: a byte b is flagged when b >= 128 or b + (128 - q) reaches 128; a carry
+// out of a byte happens only when that byte is flagged already, so a clean
+// block is clean byte for byte.  The flagged block is then scanned bytewise.
+int64_t first_state_at_least(const uint8_t *a, int64_t n, int q) {
+    const uint64_t H = 0x8080808080808080ull, add = 0x0101010101010101ull * (uint64_t)(128 - q);
+    int64_t i = 0;
+    for (; i + 64 <= n; i += 64) {
+        uint64_t bad = 0;
+        for (int k = 0; k < 8; ++k) {
+            uint64_t w;
+            std::memcpy(&w, a + i + 8 * k, 8);
+            bad |= (w | (w + add)) & H;
+        }
+        if (bad) break;
+    }
+    for (; i < n; ++i)
+        if (a[i] >= q) return i;
+    return -1;
 }
 
 extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const uint8_t *start,
@@ -259,12 +285,12 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
         int64_t n = 1;
         for (int i = 0; i < desc->d; ++i) n *= desc->shape[i];
         int64_t n_vars = desc->model == PLQ_GAUGE ? n * desc->d : n;
-        if (start)
-            for (int64_t i = 0; i < n_vars; ++i)
-                if (start[i] >= q)
-                    return plq_fail(PLQ_EINVAL, "start variable " + std::to_string(i) + " holds state " +
-                                                    std::to_string(start[i]) + ", not below q = " +
-                                                    std::to_string(q));
+        if (start) {
+            const int64_t i = first_state_at_least(start, n_vars, q);
+            if (i >= 0)
+                return plq_fail(PLQ_EINVAL, "start variable " + std::to_string(i) + " holds state " +
+                                                std::to_string(start[i]) + ", not below q = " + std::to_string(q));
+        }
     }
     PLQ_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
 
@@ -375,6 +401,11 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
                 e = fused3d_make_maps(c->fused_map_buf[k], c->g.L[0], c->g.L[1], c->g.L[2], &c->fused_maps[k]);
                 if (e != cudaSuccess) return fail(cuda_fail(e, "tensor map of the state buffer"));
             }
+            e = cudaStreamCreateWithFlags(&c->obs_stream, cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->swept, cudaEventDisableTiming);
+            for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+                e = cudaEventCreateWithFlags(&c->measured[k], cudaEventDisableTiming);
+            if (e != cudaSuccess) return fail(cuda_fail(e, "measurement stream"));
         }
         if (c->lookback) {
             c->n_chunks = local_chunks(n);
@@ -462,6 +493,11 @@ static int fused_sweep(plq_chain *c) {
         f.plane = to_affine(affine_steps(c->h_jump, (uint64_t)f.L0 * (uint64_t)f.L1 / 2));
     }
     f.status = &c->d_ctrl->status;
+    const int dst_k = f.dst == c->fused_map_buf[0] ? 0 : 1;
+    if (c->measuring[dst_k]) {  // a sample of this buffer is still being measured
+        PLQ_CUDA(cudaStreamWaitEvent(c->stream, c->measured[dst_k], 0), "wait for measurement");
+        c->measuring[dst_k] = false;
+    }
     f.stall = (c->desc.flags & PLQ_FLAG_TEST_COPY_STALL) ? 1 : 0;
     f.wait_limit = f.stall ? 1024 : (1 << 21);
     const FusedMaps &maps = c->fused_maps[f.src == c->fused_map_buf[0] ? 0 : 1];
@@ -645,12 +681,29 @@ extern "C" int plq_chain_next_batch(plq_chain *c, int64_t count, uint8_t *out_st
                 if (rc != PLQ_OK) return rc;
             }
             if (out_primaries) {
-                cudaError_t e = launch_primaries(c->d_state, c->g, c->desc.model, c->q,
-                                                 c->d_snap_obs + k * np, c->stream);
+                cudaError_t e;
+                if (c->fused && !out_states) {
+                    // measure this sample beside the next sweep, which writes the other buffer
+                    const int k_buf = c->d_state == c->fused_map_buf[0] ? 0 : 1;
+                    PLQ_CUDA(cudaEventRecord(c->swept, c->stream), "sample event");
+                    PLQ_CUDA(cudaStreamWaitEvent(c->obs_stream, c->swept, 0), "sample wait");
+                    e = launch_primaries(c->d_state, c->g, c->desc.model, c->q, c->d_snap_obs + k * np,
+                                         c->obs_stream);
+                    if (e == cudaSuccess) e = cudaEventRecord(c->measured[k_buf], c->obs_stream);
+                    c->measuring[k_buf] = true;
+                } else {
+                    e = launch_primaries(c->d_state, c->g, c->desc.model, c->q, c->d_snap_obs + k * np,
+                                         c->stream);
+                }
                 c->launches++;
                 if (e != cudaSuccess) return cuda_fail(e, "primaries");
             }
         }
+        for (int k = 0; k < 2; ++k)  // every measurement of this batch lands before the read-back
+            if (c->measuring[k]) {
+                PLQ_CUDA(cudaStreamWaitEvent(c->stream, c->measured[k], 0), "measurement wait");
+                c->measuring[k] = false;
+            }
         if (out_states)
             PLQ_CUDA(cudaMemcpyAsync(out_states + done * c->n_vars, c->d_snap, (size_t)(m * c->n_vars),
                                      cudaMemcpyDeviceToHost, c->stream),

@@ -35,6 +35,12 @@ struct plq_chain {
     int fused_tz = 0;
     plq::FusedMaps fused_maps[2];          // TMA descriptors of the two state buffers
     const uint8_t *fused_map_buf[2] = {nullptr, nullptr};
+    // Fused chains measure a sample on a second stream while the next sweep (which
+    // writes the other buffer) runs; a sweep about to overwrite a buffer waits for
+    // the measurement still reading it.
+    cudaStream_t obs_stream = nullptr;
+    cudaEvent_t swept = nullptr, measured[2] = {nullptr, nullptr};
+    bool measuring[2] = {false, false};
     std::vector<plq::AffineHost> h_jump;  // host copy of the jump table
     uint8_t *d_io = nullptr;     // host-order staging on the device
     uint64_t *d_hb53 = nullptr, *d_metro53 = nullptr;
@@ -64,6 +70,8 @@ struct plq_chain {
 };
 
 int plq_fail(int code, const std::string &msg);
+// Index of the first byte >= q (q <= 64) in a[0, n), or -1 (64 bytes per step).
+int64_t first_state_at_least(const uint8_t *a, int64_t n, int q);
 std::string shape_string(const plq_chain_desc *d);
 void chain_free(plq_chain *c);
 int local_sweep(plq_chain *c);

@@ -600,8 +600,8 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         E->allocs.push_back(st);
         a.state = st;
         if (starts && starts[m]) {
-            for (int64_t i = 0; i < mem.n_vars; ++i)
-                if (starts[m][i] >= q) return fail(plq_fail(PLQ_EINVAL, "start state out of range"));
+            if (first_state_at_least(starts[m], mem.n_vars, q) >= 0)
+                return fail(plq_fail(PLQ_EINVAL, "start state out of range"));
             if (mem.link) {
                 uint8_t *tmp = nullptr;
                 ce = cudaMalloc((void **)&tmp, (size_t)mem.n_vars);
@@ -1582,11 +1582,10 @@ extern "C" int plq_server_submit(plq_server *S, const plq_chain_desc *desc, cons
     int64_t n_vars = desc->model == PLQ_GAUGE ? n * desc->d : n;
     const int q = desc->model == PLQ_POTTS ? desc->q : 2;
     if (start) {
-        for (int64_t i = 0; i < n_vars; ++i)
-            if (start[i] >= q) {
-                delete j;
-                return plq_fail(PLQ_EINVAL, "start state out of range");
-            }
+        if (first_state_at_least(start, n_vars, q) >= 0) {
+            delete j;
+            return plq_fail(PLQ_EINVAL, "start state out of range");
+        }
         j->start.assign(start, start + n_vars);
         j->has_start = true;
     }

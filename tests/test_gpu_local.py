@@ -243,3 +243,18 @@ def test_word_passes_equal_generic(gpu, case):
         c.close()
     assert np.array_equal(outs[0][0], outs[1][0])
     assert outs[0][1:] == outs[1][1:]
+
+
+@pytest.mark.parametrize("pos", [0, 7, 63, 64, 65, 1000, 4095])
+@pytest.mark.parametrize("bad", [2, 3, 127, 128, 255])
+def test_out_of_range_start_state_refused(gpu, pos, bad):
+    # State::new refuses an index >= q: the first offending variable is named
+    start = np.ones(64 * 64, dtype=np.uint8)
+    start[pos] = bad
+    if pos + 3 < start.size:
+        start[pos + 3] = 200  # a later offender does not mask the first
+    d = plq.make_desc(plq.ISING, 2, (64, 64), plq.METROPOLIS, beta=0.4, seed=1, rng=plq.RNG_KEYED)
+    with pytest.raises(plq.PlaquetteError, match=f"start variable {pos} holds state {bad}, not below q = 2"):
+        plq.GpuChain(gpu, d, start)
+    ok = np.ones(64 * 64, dtype=np.uint8)
+    plq.GpuChain(gpu, d, ok).close()
