@@ -143,6 +143,22 @@ int plq_chain_read(plq_chain *chain, uint8_t *out_states);
  * {agree, count[0..q)} (potts/mod.rs:125-271); gauge {plaquette_sum}
  * (gauge/mod.rs:99-124).  Returns the count written via *n_out (may be NULL). */
 int plq_chain_primaries(plq_chain *chain, int64_t *out, int32_t *n_out);
+/* Ising / Potts chains: axis_pair_sums (src/models/mod.rs:44-61) of the current
+ * configuration -- for each axis mu (row by row) and displacement r = 0..L_mu/2,
+ * the sum over sites of s_i * s_{i+r mu} (Ising, ising/mod.rs:84-95) or of
+ * [s_i == s_{i+r mu}] (Potts, potts/mod.rs:218-234).  `capacity` entries of
+ * `out` must hold sum over mu of (L_mu/2 + 1); the correlators divide by N. */
+int plq_chain_axis_pair_sums(plq_chain *chain, int64_t *out, int64_t capacity);
+/* Gauge chains: Z2Gauge::polyakov_loop (gauge/mod.rs:179-212) of the current
+ * configuration along `dir` as *sum (of the +1/-1 line products) / *lines. */
+int plq_chain_polyakov(plq_chain *chain, int32_t dir, int64_t *sum, int64_t *lines);
+/* Gauge chains: Z2Gauge::wilson_rectangles (gauge/mod.rs:226-274) of the
+ * current configuration as totals[r * (m + 1) + t] / *placements for r, t in
+ * 0..m, m = min(max_side, shortest extent / 2) returned via *m_out (row and
+ * column 0 hold *placements: the 1.0 anchor).  m above 32 is refused
+ * (PLQ_EUNSUPPORTED); `capacity` entries of totals must hold (m + 1)^2. */
+int plq_chain_wilson(plq_chain *chain, int32_t max_side, int64_t *totals, int64_t capacity, int64_t *placements,
+                     int32_t *m_out);
 int plq_chain_sync(plq_chain *chain);
 /* Device status word: PLQ_OK, or PLQ_ECAP / PLQ_EDEVICE after a fault. */
 int plq_chain_status(plq_chain *chain);

@@ -132,6 +132,12 @@ def lib():
                                             C.c_uint32, C.c_uint32]
         L.orc_keyed_cluster_sweep.argtypes = [P(_Model), P(_Lattice), u8p, C.c_int32, C.c_int32, C.c_double,
                                               C.c_uint32, C.c_uint32, i64p]
+        L.orc_axis_pair_sums.argtypes = [P(_Model), P(_Lattice), u8p, i64p]
+        L.orc_axis_pair_sums.restype = C.c_int64
+        L.orc_polyakov_sum.argtypes = [P(_Lattice), u8p, C.c_int32, i64p]
+        L.orc_polyakov_sum.restype = C.c_int64
+        L.orc_wilson_totals.argtypes = [P(_Lattice), u8p, C.c_int32, i64p, i64p]
+        L.orc_wilson_totals.restype = C.c_int32
     return _lib
 
 
@@ -340,3 +346,35 @@ def hot_start(n_vars: int, q: int, rng: PcgStream) -> np.ndarray:
     out = np.empty(n_vars, dtype=np.uint8)
     lib().orc_hot_start(rng.ref, q, n_vars, _u8(out))
     return out
+
+
+def axis_pair_sums(model: Model, lat: Lattice, cfg: np.ndarray) -> list[np.ndarray]:
+    """``axis_pair_sums`` (src/models/mod.rs:44-61) with the model's pair:
+    one int64 row per axis, displacements r = 0..L_mu/2."""
+    shape = [int(lat.lat.shape[i]) for i in range(lat.lat.d)]
+    out = np.zeros(sum(L // 2 + 1 for L in shape), dtype=np.int64)
+    lib().orc_axis_pair_sums(model.ref, C.byref(lat.lat), _u8(cfg), _i64(out))
+    rows, off = [], 0
+    for L in shape:
+        rows.append(out[off:off + L // 2 + 1].copy())
+        off += L // 2 + 1
+    return rows
+
+
+def polyakov_sum(lat: Lattice, cfg: np.ndarray, direction: int) -> tuple[int, int]:
+    """``Z2Gauge::polyakov_loop`` (gauge/mod.rs:179-212) as (sum, lines)."""
+    lines = np.zeros(1, dtype=np.int64)
+    total = lib().orc_polyakov_sum(C.byref(lat.lat), _u8(cfg), direction, _i64(lines))
+    return int(total), int(lines[0])
+
+
+def wilson_totals(lat: Lattice, cfg: np.ndarray, max_side: int) -> tuple[np.ndarray, int]:
+    """``Z2Gauge::wilson_rectangles`` (gauge/mod.rs:226-274) as the integer
+    totals table and the common divisor (placements)."""
+    shortest = min(int(lat.lat.shape[i]) for i in range(lat.lat.d))
+    mx = min(max_side, shortest // 2)
+    totals = np.zeros((mx + 1) * (mx + 1), dtype=np.int64)
+    placements = np.zeros(1, dtype=np.int64)
+    got = lib().orc_wilson_totals(C.byref(lat.lat), _u8(cfg), max_side, _i64(totals), _i64(placements))
+    assert got == mx
+    return totals.reshape(mx + 1, mx + 1), int(placements[0])

@@ -818,3 +818,108 @@ void orc_keyed_cluster_sweep(const orc_model *m, const orc_lattice *lat, uint8_t
     free(minsite);
     free(parent);
 }
+
+/* ===================================================== measurements */
+
+/* Lattice::site_shift (src/lattice.rs:353-361) */
+static int64_t site_shift(const orc_lattice *lat, int64_t site, int dir, int64_t delta) {
+    int64_t st = lat->stride[dir], l = lat->shape[dir];
+    int64_t coord = (site / st) % l;
+    int64_t base = site - coord * st;
+    return base + ((coord + delta % l) % l) * st;
+}
+
+int64_t orc_axis_pair_sums(const orc_model *m, const orc_lattice *lat, const uint8_t *cfg, int64_t *out) {
+    int d = lat->d;
+    int64_t off = 0;
+    for (int mu = 0; mu < d; ++mu) {
+        int64_t half = lat->shape[mu] / 2;
+        for (int64_t r = 0; r <= half; ++r) {
+            int64_t sum = 0;
+            for (int64_t site = 0; site < lat->n_sites; ++site) {
+                int a = cfg[site], b = cfg[site_shift(lat, site, mu, r)];
+                if (m->model == ORC_ISING)
+                    sum += (int64_t)(decode(a) * decode(b));
+                else
+                    sum += a == b;
+            }
+            out[off + r] = sum;
+        }
+        off += half + 1;
+    }
+    return off;
+}
+
+/* Lattice::loop_links (src/lattice.rs:467-486) over the steps (dir, +1 / -1),
+ * as a product of the link signs; links are cfg[site * d + dir]. */
+static int loop_product(const orc_lattice *lat, const uint8_t *cfg, int64_t base, const int *dirs,
+                        const int *signs, int n_steps) {
+    int d = lat->d;
+    int64_t site = base;
+    int prod = 1;
+    for (int k = 0; k < n_steps; ++k) {
+        int dir = dirs[k];
+        int64_t link;
+        if (signs[k] > 0) {
+            link = site * d + dir;
+            site = site_shift(lat, site, dir, 1);
+        } else {
+            site = site_shift(lat, site, dir, lat->shape[dir] - 1);
+            link = site * d + dir;
+        }
+        prod *= decode(cfg[link]);
+    }
+    return prod;
+}
+
+int64_t orc_polyakov_sum(const orc_lattice *lat, const uint8_t *cfg, int32_t dir, int64_t *lines) {
+    int l = (int)lat->shape[dir];
+    int *dirs = (int *)malloc(sizeof(int) * (size_t)l), *signs = (int *)malloc(sizeof(int) * (size_t)l);
+    for (int k = 0; k < l; ++k) {
+        dirs[k] = dir;
+        signs[k] = 1;
+    }
+    int64_t total = 0, count = 0;
+    for (int64_t site = 0; site < lat->n_sites; ++site) {
+        if ((site / lat->stride[dir]) % lat->shape[dir] != 0) continue;
+        total += loop_product(lat, cfg, site, dirs, signs, l);
+        ++count;
+    }
+    free(dirs);
+    free(signs);
+    *lines = count;
+    return total;
+}
+
+int32_t orc_wilson_totals(const orc_lattice *lat, const uint8_t *cfg, int32_t max_side, int64_t *totals,
+                          int64_t *placements) {
+    int d = lat->d;
+    int64_t shortest = lat->shape[0];
+    for (int mu = 1; mu < d; ++mu)
+        if (lat->shape[mu] < shortest) shortest = lat->shape[mu];
+    int32_t mx = max_side < shortest / 2 ? max_side : (int32_t)(shortest / 2);
+    int *dirs = (int *)malloc(sizeof(int) * (size_t)(4 * mx + 4));
+    int *signs = (int *)malloc(sizeof(int) * (size_t)(4 * mx + 4));
+    for (int64_t i = 0; i < (int64_t)(mx + 1) * (mx + 1); ++i) totals[i] = 0;
+    for (int r = 1; r <= mx; ++r)
+        for (int t = 1; t <= mx; ++t) {
+            int64_t total = 0;
+            for (int mu = 0; mu < d; ++mu)
+                for (int nu = 0; nu < d; ++nu) {
+                    if (mu == nu) continue;
+                    /* Loop::rectangle (src/lattice.rs:532-555): r x (mu,+), t x (nu,+), r x (mu,-), t x (nu,-) */
+                    int n = 0;
+                    for (int k = 0; k < r; ++k) dirs[n] = mu, signs[n++] = 1;
+                    for (int k = 0; k < t; ++k) dirs[n] = nu, signs[n++] = 1;
+                    for (int k = 0; k < r; ++k) dirs[n] = mu, signs[n++] = -1;
+                    for (int k = 0; k < t; ++k) dirs[n] = nu, signs[n++] = -1;
+                    for (int64_t site = 0; site < lat->n_sites; ++site)
+                        total += loop_product(lat, cfg, site, dirs, signs, n);
+                }
+            totals[r * (mx + 1) + t] = total;
+        }
+    free(dirs);
+    free(signs);
+    *placements = (int64_t)d * (d - 1) * lat->n_sites;
+    return mx;
+}

@@ -144,6 +144,21 @@ void orc_keyed_cluster_sweep(const orc_model *m, const orc_lattice *lat, uint8_t
                              int32_t extent, int32_t relabel, double beta,
                              uint32_t seed32, uint32_t sweep, int64_t *root_out);
 
+/* ------------------------------------------------------ measurements */
+/* axis_pair_sums (src/models/mod.rs:44-61) with Ising's product of signs
+ * (ising/mod.rs:84-95) or Potts's equality (potts/mod.rs:218-234): entry
+ * off_mu + r for r = 0..L_mu/2, off_mu = sum over nu < mu of (L_nu/2 + 1).
+ * Returns the number of entries written. */
+int64_t orc_axis_pair_sums(const orc_model *m, const orc_lattice *lat, const uint8_t *cfg, int64_t *out);
+/* Z2Gauge::polyakov_loop (gauge/mod.rs:179-212) before the final division:
+ * the sum of the line products along `dir`; *lines gets the divisor. */
+int64_t orc_polyakov_sum(const orc_lattice *lat, const uint8_t *cfg, int32_t dir, int64_t *lines);
+/* Z2Gauge::wilson_rectangles (gauge/mod.rs:226-274) before the divisions:
+ * totals[r * (max + 1) + t] = sum of the rectangle products over every
+ * ordered plane and site (r, t >= 1), *placements the divisor.  Returns max. */
+int32_t orc_wilson_totals(const orc_lattice *lat, const uint8_t *cfg, int32_t max_side, int64_t *totals,
+                          int64_t *placements);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,6 +108,10 @@ _SIGNATURES = {
     "plq_chain_cuda_stream": ([C.c_void_p], C.c_void_p),
     "plq_chain_launches": ([C.c_void_p], C.c_uint64),
     "plq_chain_path": ([C.c_void_p], C.c_char_p),
+    "plq_chain_axis_pair_sums": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "plq_chain_polyakov": ([C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
+    "plq_chain_wilson": ([C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64),
+                          C.POINTER(C.c_int32)], C.c_int),
     "plq_chain_cluster_labels": ([C.c_void_p, C.c_void_p], C.c_int),
     "plq_chain_cluster_histogram": ([C.c_void_p, C.c_void_p, C.c_int32], C.c_int),
     "plq_chain_destroy": ([C.c_void_p], None),
@@ -305,6 +309,33 @@ class GpuChain:
         n = C.c_int32(0)
         check(lib().plq_chain_primaries(self._h, out.ctypes.data, C.byref(n)))
         return out[: n.value]
+
+    def axis_pair_sums(self) -> list[np.ndarray]:
+        """``axis_pair_sums`` (src/models/mod.rs:44-61) of the current
+        configuration: one int64 row per axis, displacements 0..L_mu/2."""
+        shape = [int(self.desc.shape[i]) for i in range(self.desc.d)]
+        out = np.zeros(sum(L // 2 + 1 for L in shape), dtype=np.int64)
+        check(lib().plq_chain_axis_pair_sums(self._h, out.ctypes.data, out.size))
+        rows, off = [], 0
+        for L in shape:
+            rows.append(out[off:off + L // 2 + 1].copy())
+            off += L // 2 + 1
+        return rows
+
+    def polyakov(self, direction: int) -> tuple[int, int]:
+        """Polyakov loop along `direction` as (sum of line products, lines)."""
+        s, n = C.c_int64(0), C.c_int64(0)
+        check(lib().plq_chain_polyakov(self._h, direction, C.byref(s), C.byref(n)))
+        return s.value, n.value
+
+    def wilson(self, max_side: int) -> tuple[np.ndarray, int]:
+        """Wilson rectangle totals table (r, t = 0..m) and the placements divisor."""
+        shortest = min(int(self.desc.shape[i]) for i in range(self.desc.d))
+        m = min(max_side, shortest // 2)
+        out = np.zeros((m + 1) * (m + 1), dtype=np.int64)
+        pl, mo = C.c_int64(0), C.c_int32(0)
+        check(lib().plq_chain_wilson(self._h, max_side, out.ctypes.data, out.size, C.byref(pl), C.byref(mo)))
+        return out.reshape(mo.value + 1, mo.value + 1), pl.value
 
     def sync(self) -> None:
         check(lib().plq_chain_sync(self._h))

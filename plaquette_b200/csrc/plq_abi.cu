@@ -19,6 +19,7 @@
 #include "plq_device.cuh"
 #include "plq_fused.h"
 #include "plq_local.h"
+#include "plq_measure.h"
 #include "plq_scan.h"
 #include "plq_tables.h"
 #include "plq_words.cuh"
@@ -239,7 +240,8 @@ void chain_free(plq_chain *c) {
     if (c->obs_stream) cudaStreamSynchronize(c->obs_stream);
     cluster_free(c);
     void *ptrs[] = {c->d_state, c->d_state_alt, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
-                    c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs};
+                    c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs, c->d_loop_bits,
+                    c->d_meas, c->d_pairs};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -630,6 +632,128 @@ extern "C" int plq_chain_read(plq_chain *c, uint8_t *out) {
         PLQ_CUDA(cudaMemcpyAsync(out, c->d_state, (size_t)c->n_vars, cudaMemcpyDeviceToHost, c->stream), "read");
     }
     return check_status(c);
+}
+
+// Measurement scratch of at least `entries` int64 (and the pair lists).
+static int ensure_meas(plq_chain *c, int64_t entries) {
+    if (c->meas_cap >= entries) return PLQ_OK;
+    if (c->d_meas) cudaFree(c->d_meas);
+    if (c->d_pairs) cudaFree(c->d_pairs);
+    c->d_meas = nullptr;
+    c->d_pairs = nullptr;
+    c->meas_cap = 0;
+    PLQ_CUDA(cudaMalloc((void **)&c->d_meas, sizeof(long long) * (size_t)entries), "cudaMalloc(measurements)");
+    PLQ_CUDA(cudaMalloc((void **)&c->d_pairs, sizeof(int32_t) * 2 * (size_t)entries), "cudaMalloc(pairs)");
+    c->meas_cap = entries;
+    return PLQ_OK;
+}
+
+extern "C" int plq_chain_axis_pair_sums(plq_chain *c, int64_t *out, int64_t capacity) {
+    if (!c || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
+    if (c->link) return plq_fail(PLQ_EINVAL, "axis pair sums are a site-model measurement");
+    const int64_t entries = pair_sum_entries(c->g);
+    if (capacity < entries)
+        return plq_fail(PLQ_EINVAL, "output holds " + std::to_string(capacity) + " entries, " +
+                                        std::to_string(entries) + " needed");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    int rc = ensure_meas(c, entries);
+    if (rc != PLQ_OK) return rc;
+    // the (mu, r >= 1) pairs: all mu values, then all r values
+    std::vector<int32_t> pairs, rs;
+    for (int mu = 0; mu < c->d; ++mu)
+        for (int r = 1; r <= c->g.L[mu] / 2; ++r) {
+            pairs.push_back(mu);
+            rs.push_back(r);
+        }
+    const int n_pairs = (int)rs.size();
+    pairs.insert(pairs.end(), rs.begin(), rs.end());
+    std::vector<long long> differ(n_pairs, 0);
+    if (n_pairs) {
+        PLQ_CUDA(cudaMemcpyAsync(c->d_pairs, pairs.data(), sizeof(int32_t) * 2 * (size_t)n_pairs,
+                                 cudaMemcpyHostToDevice, c->stream),
+                 "pair lists");
+        cudaError_t e = launch_pair_differ(c->d_state, c->g, c->d_pairs, c->d_pairs + n_pairs, n_pairs, c->d_meas,
+                                           c->stream);
+        c->launches++;
+        if (e != cudaSuccess) return cuda_fail(e, "pair sums");
+        PLQ_CUDA(cudaMemcpyAsync(differ.data(), c->d_meas, sizeof(long long) * (size_t)n_pairs,
+                                 cudaMemcpyDeviceToHost, c->stream),
+                 "pair sums read");
+    }
+    rc = check_status(c);
+    if (rc != PLQ_OK) return rc;
+    // Ising: sum of s_i s_j = pairs - 2 * differing; Potts: agreeing = pairs - differing
+    const int64_t n = c->n_sites;
+    int64_t off = 0;
+    int k = 0;
+    for (int mu = 0; mu < c->d; ++mu) {
+        out[off] = n;  // r = 0: every site with itself
+        for (int r = 1; r <= c->g.L[mu] / 2; ++r, ++k)
+            out[off + r] = c->desc.model == PLQ_ISING ? n - 2 * (int64_t)differ[k] : n - (int64_t)differ[k];
+        off += c->g.L[mu] / 2 + 1;
+    }
+    return PLQ_OK;
+}
+
+extern "C" int plq_chain_polyakov(plq_chain *c, int32_t dir, int64_t *sum, int64_t *lines) {
+    if (!c || !sum || !lines) return plq_fail(PLQ_EINVAL, "NULL argument");
+    if (!c->link) return plq_fail(PLQ_EINVAL, "the Polyakov loop is a gauge measurement");
+    if (dir < 0 || dir >= c->d) return plq_fail(PLQ_EINVAL, "direction out of range");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    int rc = ensure_meas(c, 1);
+    if (rc != PLQ_OK) return rc;
+    cudaError_t e = launch_polyakov(c->d_state, c->g, dir, c->d_meas, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(e, "polyakov");
+    long long s = 0;
+    PLQ_CUDA(cudaMemcpyAsync(&s, c->d_meas, sizeof s, cudaMemcpyDeviceToHost, c->stream), "polyakov read");
+    rc = check_status(c);
+    if (rc != PLQ_OK) return rc;
+    *sum = s;
+    *lines = c->n_sites / c->g.L[dir];
+    return PLQ_OK;
+}
+
+extern "C" int plq_chain_wilson(plq_chain *c, int32_t max_side, int64_t *totals, int64_t capacity,
+                                int64_t *placements, int32_t *m_out) {
+    if (!c || !totals || !placements) return plq_fail(PLQ_EINVAL, "NULL argument");
+    if (!c->link) return plq_fail(PLQ_EINVAL, "Wilson loops are a gauge measurement");
+    if (c->d < 2) return plq_fail(PLQ_EINVAL, "Wilson loops need at least two dimensions");
+    if (max_side < 0) return plq_fail(PLQ_EINVAL, "max_side is negative");
+    int32_t shortest = c->g.L[0];
+    for (int mu = 1; mu < c->d; ++mu) shortest = std::min(shortest, c->g.L[mu]);
+    const int32_t m = std::min(max_side, shortest / 2);
+    if (m > wilson_max_supported())
+        return plq_fail(PLQ_EUNSUPPORTED, "Wilson rectangles wider than " + std::to_string(wilson_max_supported()) +
+                                              " are not supported on the device");
+    const int64_t entries = (int64_t)(m + 1) * (m + 1);
+    if (capacity < entries)
+        return plq_fail(PLQ_EINVAL, "totals hold " + std::to_string(capacity) + " entries, " +
+                                        std::to_string(entries) + " needed");
+    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    int rc = ensure_meas(c, entries);
+    if (rc != PLQ_OK) return rc;
+    if (!c->d_loop_bits)
+        PLQ_CUDA(cudaMalloc((void **)&c->d_loop_bits, sizeof(uint32_t) * (size_t)c->n_vars), "cudaMalloc(loop bits)");
+    const int64_t pl = (int64_t)c->d * (c->d - 1) * c->n_sites;
+    std::vector<unsigned long long> neg((size_t)entries, 0);
+    if (m > 0) {
+        cudaError_t e = launch_wilson(c->d_state, c->g, m, c->d_loop_bits,
+                                      reinterpret_cast<unsigned long long *>(c->d_meas), c->stream);
+        c->launches += 2;
+        if (e != cudaSuccess) return cuda_fail(e, "wilson");
+        PLQ_CUDA(cudaMemcpyAsync(neg.data(), c->d_meas, sizeof(unsigned long long) * (size_t)entries,
+                                 cudaMemcpyDeviceToHost, c->stream),
+                 "wilson read");
+    }
+    rc = check_status(c);
+    if (rc != PLQ_OK) return rc;
+    for (int r = 0; r <= m; ++r)
+        for (int t = 0; t <= m; ++t)
+            totals[r * (m + 1) + t] = (r == 0 || t == 0) ? pl : pl - 2 * (int64_t)neg[(size_t)(r * (m + 1) + t)];
+    *placements = pl;
+    if (m_out) *m_out = m;
+    return PLQ_OK;
 }
 
 extern "C" int plq_chain_primaries(plq_chain *c, int64_t *out, int32_t *n_out) {

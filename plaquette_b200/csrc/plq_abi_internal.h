@@ -53,6 +53,10 @@ struct plq_chain {
     int64_t n_chunks = 0;
     long long *d_obs = nullptr;
     uint8_t *d_snap = nullptr;
+    uint32_t *d_loop_bits = nullptr;   // Wilson line parities (n_sites * d words), on first use
+    long long *d_meas = nullptr;       // measurement results (meas_cap int64)
+    int32_t *d_pairs = nullptr;        // (mu, r) pair lists of the correlator (2 * meas_cap)
+    int64_t meas_cap = 0;
     long long *d_snap_obs = nullptr;
     int64_t snap_cap = 0, snap_obs_cap = 0;
     void *h_pinned = nullptr;

@@ -93,3 +93,28 @@ def histogram(values, bins: int = 1024, lo: float = -3.0, hi: float = 3.0) -> np
     idx = np.floor((v - lo) / (hi - lo) * bins).astype(np.int64)
     np.clip(idx, 0, bins - 1, out=idx)
     return np.bincount(idx, minlength=bins).astype(np.int64)
+
+
+def correlator(model: int, pair_sums, n_vars: int, q: int = 2) -> list[np.ndarray]:
+    """Per-config correlator rows from ``axis_pair_sums``: Ising C_r = sum / N
+    (ising/mod.rs:84-95); Potts C_r = agree / N - 1/Q (potts/mod.rs:218-234)."""
+    n = float(n_vars)
+    if model == ISING:
+        return [np.array([float(int(c)) / n for c in row]) for row in pair_sums]
+    floor = 1.0 / float(q)
+    return [np.array([float(int(c)) / n - floor for c in row]) for row in pair_sums]
+
+
+def polyakov_loop(total: int, lines: int) -> float:
+    """Z2Gauge::polyakov_loop (gauge/mod.rs:179-212): signed line average."""
+    return float(total) / float(lines)
+
+
+def wilson_table(totals, placements: int) -> np.ndarray:
+    """Z2Gauge::wilson_rectangles (gauge/mod.rs:226-274): totals / placements,
+    row and column 0 the 1.0 anchor."""
+    t = np.asarray(totals, dtype=np.int64)
+    out = t.astype(np.float64) / float(placements)
+    out[0, :] = 1.0
+    out[:, 0] = 1.0
+    return out

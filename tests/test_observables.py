@@ -67,3 +67,14 @@ def test_series_equals_per_sample_functions():
     s = obs.series(obs.ISING, ip, n, j=1.5, h=0.25)
     for k in range(50):
         assert s["e"][k] == obs.energy(obs.ISING, ip[k], j=1.5, h=0.25) / n
+
+
+def test_correlator_and_loop_formulas():
+    rows = [np.array([16, 8, -4]), np.array([16, 0, 16])]
+    c = obs.correlator(obs.ISING, rows, 16)
+    assert c[0].tolist() == [1.0, 0.5, -0.25] and c[1].tolist() == [1.0, 0.0, 1.0]
+    p = obs.correlator(obs.POTTS, [np.array([12, 6])], 12, q=3)
+    assert p[0].tolist() == [1.0 - 1.0 / 3.0, 0.5 - 1.0 / 3.0]
+    assert obs.polyakov_loop(-3, 12) == -0.25
+    t = obs.wilson_table(np.array([[48, 48], [48, 12]]), 48)
+    assert t.tolist() == [[1.0, 1.0], [1.0, 0.25]]
