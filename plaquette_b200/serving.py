@@ -67,6 +67,15 @@ class Server:
         self._jobs[jid.value] = (n * desc.d if desc.model == GAUGE else n, desc)
         return jid.value
 
+    def submit_run(self, spec, want_states: bool = False) -> int:
+        """Submit a parsed run configuration (runspec.parse): its start
+        configuration and all its sweeps, thermalisation included."""
+        from .runspec import start_configuration
+
+        start, offset = start_configuration(spec)
+        spec.desc.stream_offset = offset
+        return self.submit(spec.desc, start, spec.total_sweeps, want_states)
+
     def wait(self, job: int, timeout_s: float = -1.0) -> int:
         st = C.c_int32()
         check(lib().plq_server_wait(self._h, job, timeout_s, C.byref(st)))
