@@ -151,6 +151,9 @@ __device__ void run_words(const LocalArgs &a, int link, int64_t chunk) {
     } else if (a.q == 3) {
         if (st) site_words_chunk<D, 3, true, R>(a, chunk);
         else site_words_chunk<D, 3, false, R>(a, chunk);
+    } else if (a.q == 4) {
+        if (st) site_words_chunk<D, 4, true, R>(a, chunk);
+        else site_words_chunk<D, 4, false, R>(a, chunk);
     } else {
         if (st) site_words_chunk<D, 2, true, R>(a, chunk);
         else site_words_chunk<D, 2, false, R>(a, chunk);

@@ -51,6 +51,9 @@ static cudaError_t launch_words_d(const LocalArgs &a, bool link, cudaStream_t st
     } else if (a.q == 3) {
         if (st) word_pass_kernel<D, false, 3, true><<<blocks, kWordThreads, 0, stream>>>(a);
         else word_pass_kernel<D, false, 3, false><<<blocks, kWordThreads, 0, stream>>>(a);
+    } else if (a.q == 4) {
+        if (st) word_pass_kernel<D, false, 4, true><<<blocks, kWordThreads, 0, stream>>>(a);
+        else word_pass_kernel<D, false, 4, false><<<blocks, kWordThreads, 0, stream>>>(a);
     } else {
         if (st) word_pass_kernel<D, false, 2, true><<<blocks, kWordThreads, 0, stream>>>(a);
         else word_pass_kernel<D, false, 2, false><<<blocks, kWordThreads, 0, stream>>>(a);

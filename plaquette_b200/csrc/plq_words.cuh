@@ -12,7 +12,8 @@
 // b+2, b the row's parity) draw and decide as in the generic body:
 //
 //  * sites, q <= 3: key = cur + q * sum of g(neighbour), g(0)=0, g(1)=1,
-//    g(2)=2d+1 (the packing weights of the generic key);
+//    g(2)=2d+1 (the packing weights of the generic key); q = 4 (heat bath):
+//    the same key in 16-bit lanes holding just the two colour sites;
 //  * Z2 links: key = cur + 4(d-1) - 2 * (number of staples with product -1),
 //    the generic cur + 2 * ((S + 2(d-1)) / 2) for the staple sum S.
 //
@@ -128,7 +129,7 @@ __device__ __forceinline__ uint32_t word_update(const LocalArgs &a, uint32_t C, 
     return C ^ (delta << sh);
 }
 
-// Sites (Ising, Potts q <= 3): one chunk of a colour pass, R words per thread.
+// Sites (Ising, Potts q <= 3, Potts q = 4 heat bath): one chunk of a colour pass, R words per thread.
 template <int D, int Q, bool STREAM, int R>
 __device__ __forceinline__ void site_words_chunk(const LocalArgs &a, int64_t chunk) {
     const uint32_t n_words = (uint32_t)(a.g.n_sites / 4);
@@ -152,6 +153,38 @@ __device__ __forceinline__ void site_words_chunk(const LocalArgs &a, int64_t chu
         for (int mu = 1; mu < D; ++mu) {
             nb[2 * mu] = ld_word(S, P.s + (uint32_t)P.op[mu]);
             nb[2 * mu + 1] = ld_word(S, P.s + (uint32_t)P.om[mu]);
+        }
+        if (Q == 4) {
+            // keys reach 4 + 4 * 2d * (2d+1)^2: two colour sites per word in 16-bit lanes
+            // (bytes b and b+2 of each word); g(s) = pw[s] from the two state bits:
+            // g = b0 + P b1 + (P^2 - 1 - P) b0 b1 with P = 2d + 1.
+            const uint32_t sh = 8u * (uint32_t)P.b;
+            const uint32_t LM = 0x00FF00FFu, L1 = 0x00010001u;
+            uint32_t sum = 0;
+#pragma unroll
+            for (int k = 0; k < 2 * D; ++k) {
+                const uint32_t x = (nb[k] >> sh) & LM;
+                const uint32_t b0 = x & L1, b1 = (x >> 1) & L1;
+                sum += b0 + P2 * b1 + (P2 * P2 - 1u - P2) * (b0 & b1);
+            }
+            const uint32_t Cl = (C >> sh) & LM;
+            const uint32_t K16 = Cl + 4u * sum;
+            uint32_t delta = 0;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const uint32_t key = (K16 >> (16 * i)) & 0xFFFFu;
+                const uint32_t cur = (Cl >> (16 * i)) & 0xFFu;
+                uint64_t k;
+                if (STREAM) {
+                    k = draw53(st);
+                    st = pcg_step(st, a.inc);
+                } else {
+                    k = keyed24(a.seed32, P.s + (uint32_t)(P.b + 2 * i), a.sweep32);
+                }
+                delta |= (word_decide<4, STREAM>(a, key, cur, k) ^ cur) << (16 * i);
+            }
+            *reinterpret_cast<uint32_t *>(a.state + (size_t)P.s) = C ^ (delta << sh);
+            continue;
         }
         uint32_t raw = 0;
 #pragma unroll
@@ -221,7 +254,7 @@ __host__ __device__ inline bool words_eligible(int model, int q, int d, const in
     if (updater == PLQ_METROPOLIS && !(rng == PLQ_RNG_KEYED && q == 2)) return false;
     if (updater != PLQ_METROPOLIS && updater != PLQ_HEATBATH) return false;
     if (model == PLQ_GAUGE) return d >= 2;
-    return q == 2 || q == 3;
+    return q == 2 || q == 3 || (q == 4 && updater == PLQ_HEATBATH);
 }
 
 }  // namespace plq

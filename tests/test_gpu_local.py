@@ -69,6 +69,7 @@ CASES = [
     (plq.POTTS, 3, (8, 8, 6), 0.5505, {}),
     (plq.POTTS, 3, (6, 4), 0.8, {"offsets": [0.3, -0.2, 0.1]}),
     (plq.POTTS, 4, (6, 6, 4), 0.62, {}),
+    (plq.POTTS, 4, (8, 6, 4), 0.62, {"offsets": [0.1, 0.0, -0.2, 0.05]}),
     (plq.POTTS, 5, (8, 8), 1.1, {"j": 1.5}),
     (plq.GAUGE, 2, (8, 8), 0.7, {}),
     (plq.GAUGE, 2, (4, 4, 6), 0.6, {}),
@@ -217,6 +218,9 @@ WORD_CASES = [
     (plq.POTTS, 3, (24, 16, 10), plq.HEATBATH, plq.RNG_KEYED, 0.5505),
     (plq.POTTS, 3, (8, 6, 4, 4), plq.HEATBATH, plq.RNG_STREAM, 0.4),
     (plq.POTTS, 2, (128,), plq.HEATBATH, plq.RNG_STREAM, 0.9),
+    (plq.POTTS, 4, (16, 12), plq.HEATBATH, plq.RNG_STREAM, 1.1),
+    (plq.POTTS, 4, (8, 8, 8), plq.HEATBATH, plq.RNG_KEYED, 0.62),
+    (plq.POTTS, 4, (4, 4, 4, 4), plq.HEATBATH, plq.RNG_STREAM, 0.5),
     (plq.GAUGE, 2, (16, 12), plq.HEATBATH, plq.RNG_STREAM, 0.7),
     (plq.GAUGE, 2, (12, 8, 6), plq.METROPOLIS, plq.RNG_KEYED, 0.6),
     (plq.GAUGE, 2, (16, 16, 16, 16), plq.HEATBATH, plq.RNG_STREAM, 0.4407),
