@@ -2,7 +2,7 @@
  * plaquette.h -- C ABI of the B200 lattice Monte Carlo backend.
  *
  * This library replaces the reference's wgpu device path (src/device.rs,
- * src/gpu_cluster.rs, src/models/{ising,potts,gauge}/gpu.rs, src/wgsl/*)
+ * src/gpu_cluster.rs, src/models/{ising,potts,gauge}/gpu.rs, the src/wgsl/ shaders)
  * behind the same chain semantics: a chain owns all device state, `advance`
  * runs sweeps without waiting, `next` runs `sweeps_between` sweeps and hands
  * back an owned copy of the configuration.  Plain C types only; the library

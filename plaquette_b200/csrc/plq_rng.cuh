@@ -170,11 +170,13 @@ PLQ_HD uint64_t draw53(u128 state_after_step) { return xsl_rr(state_after_step) 
 constexpr int kJumpDigits = 8;
 constexpr int kJumpRadix = 256;
 
-// The state reached after `n` steps from `s0` (n steps: position n draws
-// next_u64 from state s_{n+1}; see stream_draw53 below).
+// The state reached after `n` steps from `s0` (the draw at stream position n
+// is the output of the state one step further).
 PLQ_HD u128 jump(const Affine *table, u128 s0, uint64_t n) {
     u128 s = s0;
+#if defined(__CUDA_ARCH__)
 #pragma unroll 1
+#endif
     for (int d = 0; d < kJumpDigits && n; ++d) {
         unsigned v = (unsigned)(n & 255u);
         if (v) s = apply(table[d * kJumpRadix + v], s);
