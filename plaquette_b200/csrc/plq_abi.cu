@@ -241,7 +241,7 @@ void chain_free(plq_chain *c) {
     cluster_free(c);
     void *ptrs[] = {c->d_state, c->d_state_alt, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
                     c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs, c->d_loop_bits,
-                    c->d_meas, c->d_pairs};
+                    c->d_meas, c->d_pairs, c->d_hb53_fused};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -392,9 +392,26 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
         size_t table_bytes = desc->updater == PLQ_HEATBATH
                                  ? (desc->rng == PLQ_RNG_STREAM ? t.hb53.size() * 8 : t.hb24.size() * 4)
                                  : t.metro24.size() * 4;
+        // The fused stream heat bath compares the full 64-bit XSL-RR output with cut points
+        // shifted left by 11 (k >= c  <=>  out >= c * 2^11 for c < 2^53), which needs every
+        // cut below 2^53; a "never" cut of 2^53 (a probability that rounds to 1) sends the
+        // chain to the per-colour passes instead.
+        bool shifted_ok = true;
+        std::vector<uint64_t> hb53_shifted;
+        if (desc->rng == PLQ_RNG_STREAM && desc->updater == PLQ_HEATBATH) {
+            hb53_shifted.reserve(t.hb53.size());
+            for (uint64_t cut : t.hb53) {
+                if (cut >= (uint64_t(1) << 53)) shifted_ok = false;
+                hb53_shifted.push_back(cut << 11);
+            }
+        }
         if (!(desc->flags & PLQ_FLAG_NO_FUSED) && fused3d_eligible(desc->model, c->q, c->d, c->g.L, desc->updater, desc->rng) &&
-            table_bytes <= (size_t)fused3d_table_limit_bytes()) {
+            table_bytes <= (size_t)fused3d_table_limit_bytes() && shifted_ok) {
             c->fused = true;
+            if (!hb53_shifted.empty()) {
+                int r3 = upload(hb53_shifted, &c->d_hb53_fused, c->stream);
+                if (r3 != PLQ_OK) return fail(r3);
+            }
             c->fused_tz = fused3d_default_tz(c->g.L[2]);
             e = cudaMalloc((void **)&c->d_state_alt, (size_t)c->n_vars);
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(state_alt)"));
@@ -474,7 +491,7 @@ static int fused_sweep(plq_chain *c) {
     const bool hb = c->desc.updater == PLQ_HEATBATH;
     if (hb) {
         if (stream) {
-            f.table = c->d_hb53;
+            f.table = c->d_hb53_fused;
             f.table_words = (int)(env_key_count(model_params(&c->desc)) * (c->q - 1) * 2);
         } else {
             f.table = c->d_hb24;

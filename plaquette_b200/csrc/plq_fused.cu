@@ -152,7 +152,7 @@ __device__ __forceinline__ uint32_t update_word(const FusedArgs &a, const uint8_
         const uint32_t cur = (Cs >> (16 * i)) & 0xFFu;
         uint64_t k;
         if (STREAM) {
-            k = draw53(st);
+            k = xsl_rr(st);  // all 64 bits: the table holds the 53-bit cut points << 11
             st = pcg_step(st, a.inc);
         } else {
             k = keyed24(a.seed32, var0 + (uint32_t)(b + 2 * i), a.sweep32);

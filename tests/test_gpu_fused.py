@@ -92,3 +92,16 @@ def test_tile_copy_wait_limit_reports_and_context_survives(oracle, gpu):
     chain.close()
     got, want, *_ = run_pair(oracle, gpu, plq.ISING, 2, shape, plq.METROPOLIS, plq.RNG_KEYED, 0.3, 2)
     assert np.array_equal(got, want)
+
+
+def test_never_cut_point_leaves_the_fused_sweep(oracle, gpu):
+    # at beta = 40 some heat-bath probabilities round to 1 in f64, so a cut point is
+    # 2^53 ("never"), which the fused sweep's shifted table cannot hold: the chain
+    # runs the per-colour passes and still equals the oracle
+    shape = (128, 64, 8)
+    got, want, chain, *_ = run_pair(oracle, gpu, plq.POTTS, 3, shape, plq.HEATBATH, plq.RNG_STREAM, 40.0, 2)
+    assert chain.path == "words"
+    assert np.array_equal(got, want)
+    got, want, chain, *_ = run_pair(oracle, gpu, plq.POTTS, 3, shape, plq.HEATBATH, plq.RNG_STREAM, 0.5505, 2)
+    assert chain.path == "fused3d"
+    assert np.array_equal(got, want)
