@@ -11,8 +11,10 @@
 //               axis-minor order (cluster.rs:44-62), placed by a device-wide
 //               exclusive scan (decoupled look-back) over agreeing bonds.
 //  2. labels -- lock-free union-find: every open bond unites its ends by
-//               hooking the larger root under the smaller with a CAS, then a
-//               flatten pass.  Roots only ever hook under smaller roots, so
+//               hooking the larger root under the smaller with a CAS, then the
+//               roots of the tile-local components are flattened and every
+//               site takes its root in two hops inside the relabel pass.
+//               Roots only ever hook under smaller roots, so
 //               each component ends rooted at its minimum site: the canonical
 //               min-site label of the reference GPU (the fixed point of
 //               cluster_prelude.wgsl:113-147), and, ranked, the reference
@@ -64,6 +66,7 @@ struct ClusterArgs {
     uint8_t *state;
     uint8_t *bonds;
     int32_t *parent;
+    uint32_t *rootbits;  // bit s set: site s was the root of its tile-local component
     uint8_t *fresh;
     int32_t *rank;
     uint32_t *stamp;
@@ -170,6 +173,12 @@ __device__ __forceinline__ int64_t take_chunk(const ClusterArgs &a, bool lookbac
 }
 
 // ------------------------------------------------------------- 1. bonds
+// High bit of each byte of the result set iff that byte of a equals that of b.
+__device__ __forceinline__ uint64_t bytes_equal(uint64_t a, uint64_t b) {
+    const uint64_t e = a ^ b, lo7 = 0x7F7F7F7F7F7F7F7Full;
+    return ~(((e & lo7) + lo7) | e) & ~lo7;
+}
+
 template <int D, bool STREAM>
 __global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
@@ -179,22 +188,51 @@ __global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
         return;
     }
     const int64_t s0 = chunk * kChunk + (int64_t)threadIdx.x * kSitesPerThread;
+    // With L0 % 8 == 0 a thread's 8 sites (s0 is a multiple of 8) lie in one row, and every
+    // +mu neighbour row is 8-byte aligned: one vector load per direction, one vector store.
+    const bool row8 = (a.g.L[0] & 7) == 0;
     uint8_t agree[kSitesPerThread];
     int count = 0;
+    if (row8) {
 #pragma unroll
-    for (int i = 0; i < kSitesPerThread; ++i) {
-        int64_t s = s0 + i;
-        agree[i] = 0;
-        if (s >= n) continue;
-        int32_t x[D];
-        site_coords<D>(a.g, s, x);
-        uint8_t cur = a.state[s];
-        uint8_t m = 0;
+        for (int i = 0; i < kSitesPerThread; ++i) agree[i] = 0;
+        if (s0 < n) {
+            int32_t x[D];
+            site_coords<D>(a.g, s0, x);
+            const uint64_t cv = *reinterpret_cast<const uint64_t *>(a.state + s0);
+            // +x: bytes s0+1 .. s0+8, the last one wrapping to the row start
+            const int64_t past = x[0] + kSitesPerThread < a.g.L[0] ? s0 + kSitesPerThread
+                                                                   : s0 + kSitesPerThread - a.g.L[0];
+            uint64_t eq[D];
+            eq[0] = bytes_equal(cv, (cv >> 8) | ((uint64_t)a.state[past] << 56));
 #pragma unroll
-        for (int mu = 0; mu < D; ++mu)
-            if (a.state[nbr_plus(a.g, s, x, mu)] == cur) m |= (uint8_t)(1u << mu);
-        agree[i] = m;
-        count += __popc(m);
+            for (int mu = 1; mu < D; ++mu)
+                eq[mu] = bytes_equal(cv, *reinterpret_cast<const uint64_t *>(a.state + nbr_plus(a.g, s0, x, mu)));
+#pragma unroll
+            for (int i = 0; i < kSitesPerThread; ++i) {
+                uint32_t m = 0;
+#pragma unroll
+                for (int mu = 0; mu < D; ++mu) m |= (uint32_t)((eq[mu] >> (8 * i + 7)) & 1u) << mu;
+                agree[i] = (uint8_t)m;
+                count += __popc(m);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kSitesPerThread; ++i) {
+            int64_t s = s0 + i;
+            agree[i] = 0;
+            if (s >= n) continue;
+            int32_t x[D];
+            site_coords<D>(a.g, s, x);
+            uint8_t cur = a.state[s];
+            uint8_t m = 0;
+#pragma unroll
+            for (int mu = 0; mu < D; ++mu)
+                if (a.state[nbr_plus(a.g, s, x, mu)] == cur) m |= (uint8_t)(1u << mu);
+            agree[i] = m;
+            count += __popc(m);
+        }
     }
     u128 st{0, 0};
     if (STREAM) {
@@ -210,6 +248,7 @@ __global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
         __syncthreads();
         if (count) st = jump(a.jump, a.base, s_base + excl);
     }
+    uint64_t opened = 0;
 #pragma unroll
     for (int i = 0; i < kSitesPerThread; ++i) {
         int64_t s = s0 + i;
@@ -228,8 +267,10 @@ __global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
             }
             if (drawn) open |= (uint8_t)(1u << mu);
         }
-        a.bonds[s] = open;
+        if (row8) opened |= (uint64_t)open << (8 * i);
+        else a.bonds[s] = open;
     }
+    if (row8 && s0 < n) *reinterpret_cast<uint64_t *>(a.bonds + s0) = opened;
 }
 
 // ------------------------------------------------------------ 2. labels
@@ -320,6 +361,7 @@ __device__ __forceinline__ void lunite(int32_t *p, int32_t a, int32_t b, int cap
 template <int D>
 __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     __shared__ int32_t p[kTileSites];
+    __shared__ uint8_t bs[kTileSites];  // the tile's bond bytes
     const int L0 = a.g.L[0], L1 = D >= 2 ? a.g.L[1] : 1;
     const int T0 = tile_extent(L0), T1 = D >= 2 ? tile_extent(L1) : 1;
     const int T = T0 * T1;
@@ -340,19 +382,22 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
         const int li = k * (int)blockDim.x + (int)threadIdx.x;
         const bool valid = li < T;
         const int xl = li % T0;
-        // the bond into this site from its -x neighbour, inside this warp's segment
-        bool joined = false;
-        if (valid && lane > 0 && xl > 0) joined = (a.bonds[base + (xl - 1) + (int64_t)(li / T0) * L0] & 1u) != 0;
+        const uint32_t own = valid ? a.bonds[base + xl + (int64_t)(li / T0) * L0] : 0u;
+        if (valid) bs[li] = (uint8_t)own;
+        // the bond into this site from its -x neighbour (lane - 1), inside this warp's segment
+        const uint32_t from_left = __shfl_up_sync(0xffffffffu, own, 1);
+        const bool joined = valid && lane > 0 && xl > 0 && (from_left & 1u) != 0;
         const unsigned starts = __ballot_sync(0xffffffffu, !joined);
         const int start = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
         if (valid) p[li] = li - lane + start;
     }
     __syncthreads();
-    // the remaining bonds inside the tile: +x across a warp segment or around the row, and +y
+    // the remaining bonds inside the tile: +x across a warp segment or around the row, and +y.
+    // (Skipping a +y bond that the x-1 bonds already imply saves 16 % of these unions at
+    // criticality but measured slower: the extra shared-memory reads cost more.)
     for (int li = threadIdx.x; li < T; li += blockDim.x) {
         const int xl = li % T0, yl = li / T0;
-        const int64_t s = base + xl + (int64_t)yl * L0;
-        const uint8_t b = a.bonds[s];
+        const uint32_t b = bs[li];
         if (b & 1u) {
             if (xl + 1 < T0) {
                 if ((li & 31) == 31) lunite(p, li, li + 1, cap, a.ctrl);
@@ -379,10 +424,20 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
         }
         if (!__syncthreads_or(changed)) break;
     }
+    // every site points at its local root; the local roots are marked in rootbits.  With
+    // T0 >= 32 a warp's 32 sites are one aligned word of the mask, written whole; narrower
+    // tiles set bits atomically in words that the roots pass cleared.
     for (int li = threadIdx.x; li < T; li += blockDim.x) {
         const int32_t r = p[li];
         const int64_t s = base + li % T0 + (int64_t)(li / T0) * L0;
         a.parent[s] = (int32_t)(base + r % T0 + (int64_t)(r / T0) * L0);
+        const uint32_t bit = r == li ? 1u << (s & 31) : 0u;
+        if (T0 >= 32) {
+            const uint32_t word = __reduce_or_sync(0xffffffffu, bit);
+            if (lane == 0) a.rootbits[s >> 5] = word;
+        } else if (bit) {
+            atomicOr(&a.rootbits[s >> 5], bit);
+        }
     }
 }
 
@@ -446,10 +501,40 @@ __device__ __forceinline__ int32_t find_root_ro(const int32_t *parent, int32_t x
     return x;
 }
 
-__global__ void flatten_kernel(ClusterArgs a) {
+// Points every tile-local root straight at its component's root and clears
+// the mask; one thread per site, a warp per mask word.  No union runs any
+// more, so the root a walk ends on is final: the walk writes it back along
+// its path, and since final roots are the only values stored, concurrent
+// walks only ever find shorter paths.  Afterwards every site is at most two
+// hops from its root: tile_hook left it pointing at its local root, and the
+// boundary unions only re-point roots, or halve paths onto local roots.
+__global__ void flatten_roots_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
-        a.parent[s] = find_root_ro(a.parent, (int32_t)s, a.cap, a.ctrl);
+    const int64_t n_pad = (n + 31) & ~(int64_t)31;  // whole warps, so the word clear below is warp-wide
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_pad; s += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t word = a.rootbits[s >> 5];
+        __syncwarp();
+        if (word && (threadIdx.x & 31) == 0) a.rootbits[s >> 5] = 0u;
+        if (!((word >> (s & 31)) & 1u)) continue;
+        const int32_t root = find_root_ro(a.parent, (int32_t)s, a.cap, a.ctrl);
+        int32_t x = (int32_t)s;
+        for (int it = 0; x != root && it <= a.cap; ++it) {
+            const int32_t nx = ld_relaxed32(&a.parent[x]);
+            a.parent[x] = root;
+            x = nx;
+        }
+    }
+}
+
+// The root of site s once flatten_roots_kernel ran; also stores it, which
+// leaves the parent array flat (every site holding its root) for the
+// readers after the sweep.  A site read here as another's parent is a
+// local root, already holding its root, so the store does not change it.
+__device__ __forceinline__ int32_t take_root(const ClusterArgs &a, int64_t s) {
+    const int32_t p = a.parent[s];
+    const int32_t r = a.parent[p];
+    if (r != p) a.parent[s] = r;
+    return r;
 }
 
 // ----------------------------------------------------------- 3. relabel
@@ -458,7 +543,7 @@ __global__ void relabel_keyed_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
     const uint32_t q = (uint32_t)a.q;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t root = (uint32_t)a.parent[s];
+        const uint32_t root = (uint32_t)take_root(a, s);
         float u = __fmul_rn((float)keyed24(a.seed32 ^ kRootSalt, root, a.sweep32), 5.9604644775390625e-8f);
         if (a.relabel == PLQ_RELABEL_FORCED) {
             uint32_t step = __float2uint_rz(__fmul_rn(u, (float)(q - 1u)));
@@ -552,7 +637,7 @@ __global__ void root_draw_kernel(ClusterArgs a) {
 __global__ void apply_fresh_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
-        a.state[s] = a.fresh[a.parent[s]];
+        a.state[s] = a.fresh[take_root(a, s)];
 }
 
 __global__ void finish_pos_kernel(Control *ctrl, int n_events) {
@@ -658,6 +743,7 @@ __global__ void size_hist_kernel(const int32_t *parent, const int32_t *size, int
 struct ClusterDev {
     uint8_t *bonds = nullptr;
     int32_t *parent = nullptr;
+    uint32_t *rootbits = nullptr;
     uint8_t *fresh = nullptr;
     int32_t *rank = nullptr;
     uint32_t *stamp = nullptr;
@@ -688,6 +774,7 @@ ClusterArgs cluster_args(plq_chain *c) {
     a.state = c->d_state;
     a.bonds = cd->bonds;
     a.parent = cd->parent;
+    a.rootbits = cd->rootbits;
     a.fresh = cd->fresh;
     a.rank = cd->rank;
     a.stamp = cd->stamp;
@@ -744,7 +831,7 @@ int sweep_d(plq_chain *c, uint64_t sweeps) {
         }
         tile_hook_kernel<D><<<(unsigned)cd->n_tiles, kThreads, 0, c->stream>>>(a);
         boundary_hook_kernel<D><<<gs, kThreads, 0, c->stream>>>(a);
-        flatten_kernel<<<gs, kThreads, 0, c->stream>>>(a);
+        flatten_roots_kernel<<<gs, kThreads, 0, c->stream>>>(a);
         c->launches += 4;
         if (!stream) {
             relabel_keyed_kernel<<<gs, kThreads, 0, c->stream>>>(a);
@@ -833,6 +920,9 @@ int cluster_create(plq_chain *c) {
     } else {
         alloc((void **)&cd->bonds, (size_t)n);
         alloc((void **)&cd->parent, sizeof(int32_t) * (size_t)n);
+        alloc((void **)&cd->rootbits, sizeof(uint32_t) * (size_t)((n + 31) / 32));
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(cd->rootbits, 0, sizeof(uint32_t) * (size_t)((n + 31) / 32), c->stream);
         alloc((void **)&cd->desc, sizeof(unsigned long long) * (size_t)cd->n_chunks);
         if (e == cudaSuccess)
             e = cudaMemsetAsync(cd->desc, 0, sizeof(unsigned long long) * (size_t)cd->n_chunks, c->stream);
@@ -868,7 +958,7 @@ int cluster_sweep(plq_chain *c) { return cluster_sweep_n(c, 1); }
 void cluster_free(plq_chain *c) {
     ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
     if (!cd) return;
-    void *ptrs[] = {cd->bonds, cd->parent, cd->fresh, cd->rank, cd->stamp, cd->queue,
+    void *ptrs[] = {cd->bonds, cd->parent, cd->rootbits, cd->fresh, cd->rank, cd->stamp, cd->queue,
                     cd->desc, cd->events, cd->first_new, cd->sizes};
     for (void *p : ptrs)
         if (p) cudaFree(p);

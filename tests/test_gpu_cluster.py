@@ -53,6 +53,10 @@ SW_STREAM = [
     (plq.POTTS, 3, (8, 6, 4), plq.RELABEL_FORCED, 0.7),
     (plq.POTTS, 5, (10, 10), plq.RELABEL_REDRAW, 1.2),
     (plq.ISING, 2, (2, 2, 2, 2), plq.RELABEL_REDRAW, 0.3),
+    # 64-site tiles spanning whole rows and columns (both wraps inside one tile)
+    (plq.ISING, 2, (64, 64), plq.RELABEL_REDRAW, 0.4406868),
+    # 32-site tile rows that split the rows, 8-row tiles
+    (plq.POTTS, 3, (96, 40), plq.RELABEL_REDRAW, 1.0050),
 ]
 
 
@@ -88,6 +92,12 @@ SW_KEYED = [
     (plq.ISING, 2, (6, 8, 4), plq.RELABEL_REDRAW, 0.2216544),
     (plq.POTTS, 3, (10, 12), plq.RELABEL_FORCED, 1.0),
     (plq.POTTS, 4, (8, 8, 6), plq.RELABEL_REDRAW, 0.6),
+    # tile extents 64 and 32 (whole warps per mask word), with and without wraps inside a tile
+    (plq.ISING, 2, (64, 48), plq.RELABEL_REDRAW, 0.4406868),
+    (plq.ISING, 2, (128, 64), plq.RELABEL_REDRAW, 0.4406868),
+    (plq.ISING, 2, (96, 32, 4), plq.RELABEL_REDRAW, 0.2216544),
+    (plq.ISING, 2, (128,), plq.RELABEL_REDRAW, 1.5),
+    (plq.POTTS, 3, (64, 96), plq.RELABEL_FORCED, 1.0),
 ]
 
 
