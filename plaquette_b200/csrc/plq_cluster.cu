@@ -411,24 +411,14 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
         }
     }
     __syncthreads();
-    // pointer jumping to the local roots: a pointer only ever moves to an ancestor,
-    // so concurrent jumps are safe; log2(depth) + 1 rounds (bounded)
-    for (int round = 0; round < 32; ++round) {
-        int changed = 0;
-        for (int li = threadIdx.x; li < T; li += blockDim.x) {
-            const int32_t pl = p[li], pp = p[pl];
-            if (pp != pl) {
-                p[li] = pp;
-                changed = 1;
-            }
-        }
-        if (!__syncthreads_or(changed)) break;
-    }
-    // every site points at its local root; the local roots are marked in rootbits.  With
-    // T0 >= 32 a warp's 32 sites are one aligned word of the mask, written whole; narrower
-    // tiles set bits atomically in words that the roots pass cleared.
+    // The forest is final: each site walks to its local root (read-only; trees at β_c are
+    // about 2.3 deep on average, at most ~10, so this beats block-wide pointer-jumping rounds)
+    // and points at it.  The local roots are marked in rootbits: with T0 >= 32 a warp's 32
+    // sites are one aligned word of the mask, written whole; narrower tiles set bits
+    // atomically in words that the roots pass cleared.
     for (int li = threadIdx.x; li < T; li += blockDim.x) {
-        const int32_t r = p[li];
+        int32_t r = li;
+        for (int it = 0; p[r] != r && it < kTileSites; ++it) r = p[r];
         const int64_t s = base + li % T0 + (int64_t)(li / T0) * L0;
         a.parent[s] = (int32_t)(base + r % T0 + (int64_t)(r / T0) * L0);
         const uint32_t bit = r == li ? 1u << (s & 31) : 0u;
