@@ -69,6 +69,10 @@ struct ClusterArgs {
     uint32_t *rootbits;  // bit s set: site s was the root of its tile-local component
     uint8_t *fresh;
     int32_t *rank;
+    struct ChunkBase {     // stream relabel: per root_rank chunk, the state at the label draw of
+        u128 st;           // the chunk's first root (no second draws before it) and that root's rank
+        int64_t rank0, pad;
+    } *chunk_base;
     uint32_t *stamp;
     int32_t *queue;
     Geom g;
@@ -240,13 +244,19 @@ __global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
         bool ok;
         uint64_t excl = chunk_scan(a, chunk, count, total, ok);
         if (!ok) return;
-        __shared__ unsigned long long s_base;
+        // One full jump per chunk, to its first draw (thread 0's prefix is the chunk's); each
+        // thread then applies the low digits of its offset inside the chunk (< kChunk * D draws).
+        // Jump maps are iterates of one affine map, so they compose in any order.
+        __shared__ unsigned long long s_base, s_excl0;
+        __shared__ u128 s_state;
         if (threadIdx.x == 0) {
             s_base = a.ctrl->pos[0];
             if (chunk == a.n_chunks - 1) a.ctrl->pos[1] = s_base + excl + (unsigned long long)total;
+            s_excl0 = excl;
+            s_state = jump(a.jump, a.base, s_base + excl);
         }
         __syncthreads();
-        if (count) st = jump(a.jump, a.base, s_base + excl);
+        if (count) st = jump(a.jump, s_state, excl - s_excl0);
     }
     uint64_t opened = 0;
 #pragma unroll
@@ -571,17 +581,21 @@ __global__ void __launch_bounds__(kThreads) root_rank_kernel(ClusterArgs a) {
     bool ok;
     uint64_t excl = chunk_scan(a, chunk, count, total, ok);
     if (!ok) return;
-    if (threadIdx.x == 0 && chunk == a.n_chunks - 1) a.ctrl->scratch[0] = excl + (unsigned long long)total;
+    if (threadIdx.x == 0) {
+        if (chunk == a.n_chunks - 1) a.ctrl->scratch[0] = excl + (unsigned long long)total;
+        // labels are drawn from the end of the bond draws, in root rank order
+        a.chunk_base[chunk].st = jump(a.jump, a.base, a.ctrl->pos[1] + excl);
+        a.chunk_base[chunk].rank0 = (int64_t)excl;
+    }
     int r = (int)excl;
 #pragma unroll
     for (int i = 0; i < kSitesPerThread; ++i)
         if ((mask >> i) & 1u) a.rank[s0 + i] = r++;
 }
 
-// rand 0.10 random_range(0..range) for range < 2^32 at stream position pos:
-// returns the value and whether a second draw was taken.
-__device__ __forceinline__ uint32_t next_below_at(const ClusterArgs &a, uint64_t pos, uint32_t range, bool &second) {
-    u128 st = jump(a.jump, a.base, pos);
+// rand 0.10 random_range(0..range) for range < 2^32 whose first draw is the
+// output of state st: returns the value and whether a second draw was taken.
+__device__ __forceinline__ uint32_t next_below_from(const ClusterArgs &a, u128 st, uint32_t range, bool &second) {
     uint32_t x = (uint32_t)xsl_rr(st);
     uint64_t m = (uint64_t)x * range;
     uint32_t result = (uint32_t)(m >> 32), lo = (uint32_t)m;
@@ -596,10 +610,10 @@ __device__ __forceinline__ uint32_t next_below_at(const ClusterArgs &a, uint64_t
 }
 
 // stream: each root draws its cluster's fresh label (ClusterUpdate::fresh_label,
-// updater.rs:507-521) at bond_end + rank + (known second draws before it).
+// updater.rs:507-521) at bond_end + rank + (known second draws before it),
+// jumping from its root_rank chunk's first label draw.
 __global__ void root_draw_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
-    const uint64_t bond_end = a.ctrl->pos[1];
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
         if (a.parent[s] != (int32_t)s) continue;
         int32_t r = a.rank[s];
@@ -609,14 +623,15 @@ __global__ void root_draw_kernel(ClusterArgs a) {
             before += a.events[e] < r;
             known |= a.events[e] == r;
         }
-        uint64_t pos = bond_end + (uint64_t)r + (uint64_t)before;
+        const ClusterArgs::ChunkBase &cb = a.chunk_base[s / kChunk];
+        const u128 st = jump(a.jump, cb.st, (uint64_t)((int64_t)r - cb.rank0) + (uint64_t)before);
         uint32_t cur = a.state[s];
         uint32_t label;
         bool second;
         if (a.relabel == PLQ_RELABEL_REDRAW) {
-            label = next_below_at(a, pos, (uint32_t)a.q, second);
+            label = next_below_from(a, st, (uint32_t)a.q, second);
         } else {  // propose (updater.rs:659-668); q >= 3 here
-            uint32_t d = next_below_at(a, pos, (uint32_t)(a.q - 1), second);
+            uint32_t d = next_below_from(a, st, (uint32_t)(a.q - 1), second);
             label = d + (d >= cur ? 1u : 0u);
         }
         a.fresh[s] = (uint8_t)label;
@@ -736,6 +751,7 @@ struct ClusterDev {
     uint32_t *rootbits = nullptr;
     uint8_t *fresh = nullptr;
     int32_t *rank = nullptr;
+    ClusterArgs::ChunkBase *chunk_base = nullptr;
     uint32_t *stamp = nullptr;
     int32_t *queue = nullptr;
     unsigned long long *desc = nullptr;
@@ -767,6 +783,7 @@ ClusterArgs cluster_args(plq_chain *c) {
     a.rootbits = cd->rootbits;
     a.fresh = cd->fresh;
     a.rank = cd->rank;
+    a.chunk_base = cd->chunk_base;
     a.stamp = cd->stamp;
     a.queue = cd->queue;
     a.g = c->g;
@@ -919,6 +936,7 @@ int cluster_create(plq_chain *c) {
         if (c->desc.rng == PLQ_RNG_STREAM) {
             alloc((void **)&cd->fresh, (size_t)n);
             alloc((void **)&cd->rank, sizeof(int32_t) * (size_t)n);
+            alloc((void **)&cd->chunk_base, sizeof(ClusterArgs::ChunkBase) * (size_t)cd->n_chunks);
             alloc((void **)&cd->events, sizeof(int32_t) * kMaxEvents);
             alloc((void **)&cd->first_new, sizeof(int));
         }
@@ -948,7 +966,7 @@ int cluster_sweep(plq_chain *c) { return cluster_sweep_n(c, 1); }
 void cluster_free(plq_chain *c) {
     ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
     if (!cd) return;
-    void *ptrs[] = {cd->bonds, cd->parent, cd->rootbits, cd->fresh, cd->rank, cd->stamp, cd->queue,
+    void *ptrs[] = {cd->bonds, cd->parent, cd->rootbits, cd->fresh, cd->rank, cd->chunk_base, cd->stamp, cd->queue,
                     cd->desc, cd->events, cd->first_new, cd->sizes};
     for (void *p : ptrs)
         if (p) cudaFree(p);
