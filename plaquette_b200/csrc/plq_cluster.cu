@@ -557,7 +557,36 @@ __global__ void relabel_keyed_kernel(ClusterArgs a) {
     }
 }
 
-// stream: rank of each root among roots (first-encounter order)
+// rand 0.10 random_range(0..range) for range < 2^32 whose first draw is the
+// output of state st: returns the value and whether a second draw was taken.
+__device__ __forceinline__ uint32_t next_below_from(const ClusterArgs &a, u128 st, uint32_t range, bool &second) {
+    uint32_t x = (uint32_t)xsl_rr(st);
+    uint64_t m = (uint64_t)x * range;
+    uint32_t result = (uint32_t)(m >> 32), lo = (uint32_t)m;
+    second = lo > (uint32_t)(0u - range);
+    if (second) {
+        st = pcg_step(st, a.inc);
+        uint32_t x2 = (uint32_t)xsl_rr(st);
+        uint32_t hi2 = (uint32_t)(((uint64_t)x2 * range) >> 32);
+        if ((uint64_t)lo + hi2 > 0xFFFFFFFFull) result += 1;
+    }
+    return result;
+}
+
+// The fresh label of a cluster (ClusterUpdate::fresh_label, updater.rs:507-521)
+// whose first draw is the output of st: next_below(q), or with forced change the
+// proposal of updater.rs:659-668 (q >= 3 there).
+__device__ __forceinline__ uint32_t fresh_label(const ClusterArgs &a, u128 st, uint32_t cur, bool &second) {
+    if (a.relabel == PLQ_RELABEL_REDRAW) return next_below_from(a, st, (uint32_t)a.q, second);
+    const uint32_t d = next_below_from(a, st, (uint32_t)(a.q - 1), second);
+    return d + (d >= cur ? 1u : 0u);
+}
+
+// stream: rank of each root among roots (first-encounter order), and each
+// root's fresh label drawn with no second draws known: rank r draws at
+// bond_end + r, so a thread steps the stream from one root to the next.  A root
+// whose label takes a second draw reports its rank in first_new; the host then
+// re-runs the draws (root_draw_kernel) with that event known.
 template <int D>
 __global__ void __launch_bounds__(kThreads) root_rank_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
@@ -581,32 +610,32 @@ __global__ void __launch_bounds__(kThreads) root_rank_kernel(ClusterArgs a) {
     bool ok;
     uint64_t excl = chunk_scan(a, chunk, count, total, ok);
     if (!ok) return;
+    __shared__ u128 s_state;
+    __shared__ unsigned long long s_excl0;
     if (threadIdx.x == 0) {
         if (chunk == a.n_chunks - 1) a.ctrl->scratch[0] = excl + (unsigned long long)total;
         // labels are drawn from the end of the bond draws, in root rank order
-        a.chunk_base[chunk].st = jump(a.jump, a.base, a.ctrl->pos[1] + excl);
+        const u128 st0 = jump(a.jump, a.base, a.ctrl->pos[1] + excl);
+        a.chunk_base[chunk].st = st0;
         a.chunk_base[chunk].rank0 = (int64_t)excl;
+        s_state = st0;
+        s_excl0 = excl;
     }
+    __syncthreads();
+    if (!count) return;
+    u128 st = jump(a.jump, s_state, excl - s_excl0);
     int r = (int)excl;
 #pragma unroll
-    for (int i = 0; i < kSitesPerThread; ++i)
-        if ((mask >> i) & 1u) a.rank[s0 + i] = r++;
-}
-
-// rand 0.10 random_range(0..range) for range < 2^32 whose first draw is the
-// output of state st: returns the value and whether a second draw was taken.
-__device__ __forceinline__ uint32_t next_below_from(const ClusterArgs &a, u128 st, uint32_t range, bool &second) {
-    uint32_t x = (uint32_t)xsl_rr(st);
-    uint64_t m = (uint64_t)x * range;
-    uint32_t result = (uint32_t)(m >> 32), lo = (uint32_t)m;
-    second = lo > (uint32_t)(0u - range);
-    if (second) {
+    for (int i = 0; i < kSitesPerThread; ++i) {
+        if (!((mask >> i) & 1u)) continue;
+        const int64_t s = s0 + i;
+        a.rank[s] = r;
+        bool second;
+        a.fresh[s] = (uint8_t)fresh_label(a, st, a.state[s], second);
+        if (second) atomicMin(a.first_new, r);
         st = pcg_step(st, a.inc);
-        uint32_t x2 = (uint32_t)xsl_rr(st);
-        uint32_t hi2 = (uint32_t)(((uint64_t)x2 * range) >> 32);
-        if ((uint64_t)lo + hi2 > 0xFFFFFFFFull) result += 1;
+        ++r;
     }
-    return result;
 }
 
 // stream: each root draws its cluster's fresh label (ClusterUpdate::fresh_label,
@@ -625,16 +654,8 @@ __global__ void root_draw_kernel(ClusterArgs a) {
         }
         const ClusterArgs::ChunkBase &cb = a.chunk_base[s / kChunk];
         const u128 st = jump(a.jump, cb.st, (uint64_t)((int64_t)r - cb.rank0) + (uint64_t)before);
-        uint32_t cur = a.state[s];
-        uint32_t label;
         bool second;
-        if (a.relabel == PLQ_RELABEL_REDRAW) {
-            label = next_below_from(a, st, (uint32_t)a.q, second);
-        } else {  // propose (updater.rs:659-668); q >= 3 here
-            uint32_t d = next_below_from(a, st, (uint32_t)(a.q - 1), second);
-            label = d + (d >= cur ? 1u : 0u);
-        }
-        a.fresh[s] = (uint8_t)label;
+        a.fresh[s] = (uint8_t)fresh_label(a, st, a.state[s], second);
         if (second && !known) atomicMin(a.first_new, r);
     }
 }
@@ -845,18 +866,21 @@ int sweep_d(plq_chain *c, uint64_t sweeps) {
             c->launches++;
         } else {
             lookback(a);
+            const int none = 0x7FFFFFFF;
+            cudaMemcpyAsync(cd->first_new, &none, sizeof none, cudaMemcpyHostToDevice, c->stream);
+            // ranks, and the labels with no second draws known
             root_rank_kernel<D><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
             c->launches++;
             cd->host_events.clear();
             for (int round = 0;; ++round) {
-                a.n_events = (int)cd->host_events.size();
-                int none = 0x7FFFFFFF;
-                cudaMemcpyAsync(cd->first_new, &none, sizeof none, cudaMemcpyHostToDevice, c->stream);
-                if (a.n_events)
+                if (round > 0) {  // again, with the second draws found so far known
+                    a.n_events = (int)cd->host_events.size();
+                    cudaMemcpyAsync(cd->first_new, &none, sizeof none, cudaMemcpyHostToDevice, c->stream);
                     cudaMemcpyAsync(cd->events, cd->host_events.data(), sizeof(int32_t) * a.n_events,
                                     cudaMemcpyHostToDevice, c->stream);
-                root_draw_kernel<<<gs, kThreads, 0, c->stream>>>(a);
-                c->launches++;
+                    root_draw_kernel<<<gs, kThreads, 0, c->stream>>>(a);
+                    c->launches++;
+                }
                 int first = none;
                 cudaMemcpyAsync(&first, cd->first_new, sizeof first, cudaMemcpyDeviceToHost, c->stream);
                 cudaError_t e = cudaStreamSynchronize(c->stream);

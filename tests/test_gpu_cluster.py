@@ -86,6 +86,35 @@ def test_sw_stream_bit_exact(oracle, gpu, case):
         assert np.array_equal(hist, want_hist)
 
 
+@pytest.mark.parametrize("relabel,seed", [(plq.RELABEL_REDRAW, 4), (plq.RELABEL_FORCED, 6)])
+def test_sw_stream_second_draw_events(oracle, gpu, relabel, seed):
+    """rand's range sampler takes a second draw when the low word of x * range
+    lands in its rejection zone: probability (range - 1) / 2^32 per draw, and never
+    for a power-of-two range.  At beta = 0 every site is its own cluster, so a
+    4096^2 lattice draws 2^24 labels per sweep.  With q = 63 these seeds make two
+    such draws in the first sweep, so the device re-runs the label draws twice with
+    the events known.  States and stream positions stay bit-exact with the CPU."""
+    q, shape = 63, (4096, 4096)
+    lat = oracle.Lattice(shape)
+    model = oracle.Model.potts(q, 1.0)
+    n = lat.n_sites
+    start, off = plq.hot_start(seed, q, n)
+    chain = _chain(gpu, plq.POTTS, q, shape, plq.EXTENT_ALL, relabel, 0.0, seed, start, plq.RNG_STREAM, off)
+    r = oracle.PcgStream(seed)
+    r.advance(off)
+    want = start.copy()
+    for sweep in range(2):
+        g = want.reshape(shape[1], shape[0]).astype(np.int16)
+        agreeing = int((g == np.roll(g, -1, 1)).sum() + (g == np.roll(g, -1, 0)).sum())
+        d0 = r.draws
+        oracle.cluster_sweep(model, lat, want, oracle.ALL, relabel, 0.0, r)
+        if sweep == 0:
+            assert r.draws - d0 - agreeing - n == 2  # the two second draws
+        got = next(chain)
+        assert np.array_equal(got, want), sweep
+        assert chain.stream_position() == r.draws
+
+
 SW_KEYED = [
     (plq.ISING, 2, (16, 16), plq.RELABEL_REDRAW, 0.4406868),
     (plq.ISING, 2, (5, 7), plq.RELABEL_REDRAW, 0.5),
