@@ -133,34 +133,51 @@ __device__ uint64_t chunk_scan(const ClusterArgs &a, int64_t chunk, int v, int &
         if (w < wid) warp_excl += t;
         total += t;
     }
-    if (threadIdx.x == 0) {
+    // Warp 0 looks back over 32 predecessors per round: the nearest one with an inclusive
+    // prefix ends the walk, and the aggregates up to it are summed with one warp reduction.
+    if (wid == 0) {
         unsigned long long excl = 0;
+        bool fail = false;
         if (chunk == 0) {
-            atomicExch(&a.desc[0], make_desc(a.epoch, kDescPrefix, (uint32_t)total));
+            if (lane == 0) atomicExch(&a.desc[0], make_desc(a.epoch, kDescPrefix, (uint32_t)total));
         } else {
-            atomicExch(&a.desc[chunk], make_desc(a.epoch, kDescAgg, (uint32_t)total));
-            int64_t j = chunk - 1;
+            if (lane == 0) atomicExch(&a.desc[chunk], make_desc(a.epoch, kDescAgg, (uint32_t)total));
+            const uint32_t ep = a.epoch & 0x3FFFFFFFu;
+            int64_t top = chunk - 1;
             int spins = 0;
-            while (j >= 0) {
-                unsigned long long d = ld_relaxed(&a.desc[j]);
-                uint32_t ep = (uint32_t)(d >> 34);
-                unsigned long long st = (d >> 32) & 3ull;
-                if (ep != (a.epoch & 0x3FFFFFFFu) || st == 0) {
+            while (true) {
+                const int64_t idx = top - lane;
+                // before chunk 0: an inclusive prefix of 0
+                const unsigned long long d = idx >= 0 ? ld_relaxed(&a.desc[idx]) : make_desc(a.epoch, kDescPrefix, 0u);
+                const unsigned long long st = (uint32_t)(d >> 34) == ep ? (d >> 32) & 3ull : 0ull;
+                const unsigned incl_lanes = __ballot_sync(0xffffffffu, st == kDescPrefix);
+                const unsigned ready = __ballot_sync(0xffffffffu, st != 0ull);
+                // lanes up to the nearest inclusive prefix (all 32 when none is in this window)
+                const unsigned span = incl_lanes ? (((incl_lanes & (0u - incl_lanes)) << 1) - 1u) : 0xffffffffu;
+                if ((ready & span) != span) {
                     if (++spins > kSpinLimit) {
-                        s_fail = 1;
-                        atomicOr(&a.ctrl->status, kStatusLookbackTimeout);
+                        fail = true;
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(32);
                     continue;
                 }
-                excl += (uint32_t)d;
-                if (st == kDescPrefix) break;
-                --j;
+                unsigned long long v = ((span >> lane) & 1u) ? (unsigned long long)(uint32_t)d : 0ull;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+                excl += v;
+                if (incl_lanes) break;
+                top -= 32;
             }
-            if (!s_fail) atomicExch(&a.desc[chunk], make_desc(a.epoch, kDescPrefix, (uint32_t)(excl + total)));
+            if (lane == 0 && !fail) atomicExch(&a.desc[chunk], make_desc(a.epoch, kDescPrefix, (uint32_t)(excl + total)));
         }
-        s_excl = excl;
+        if (lane == 0) {
+            if (fail) {
+                s_fail = 1;
+                atomicOr(&a.ctrl->status, kStatusLookbackTimeout);
+            }
+            s_excl = excl;
+        }
     }
     __syncthreads();
     ok = s_fail == 0;
@@ -384,6 +401,9 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     const int64_t slab = r1 / tiles1;
     const int64_t base = slab * (int64_t)L0 * L1 + (int64_t)ty * T1 * L0 + (int64_t)tx * T0;
     const int cap = a.cap < kTileSites + 64 ? a.cap : kTileSites + 64;
+    // T0 is a power of two: local index li = yl * T0 + xl splits by shift and mask (a runtime
+    // division would cost ~20 instructions, several times per site)
+    const int sh0 = __ffs(T0) - 1, m0 = T0 - 1;
     // x runs first: a warp holds 32 consecutive sites; each site points straight at
     // the start of its run of open +x bonds (the run's minimum), found with one ballot
     const int lane = threadIdx.x & 31;
@@ -391,8 +411,8 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     for (int k = 0; k < rounds; ++k) {
         const int li = k * (int)blockDim.x + (int)threadIdx.x;
         const bool valid = li < T;
-        const int xl = li % T0;
-        const uint32_t own = valid ? a.bonds[base + xl + (int64_t)(li / T0) * L0] : 0u;
+        const int xl = li & m0;
+        const uint32_t own = valid ? a.bonds[base + xl + (int64_t)(li >> sh0) * L0] : 0u;
         if (valid) bs[li] = (uint8_t)own;
         // the bond into this site from its -x neighbour (lane - 1), inside this warp's segment
         const uint32_t from_left = __shfl_up_sync(0xffffffffu, own, 1);
@@ -406,7 +426,7 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     // (Skipping a +y bond that the x-1 bonds already imply saves 16 % of these unions at
     // criticality but measured slower: the extra shared-memory reads cost more.)
     for (int li = threadIdx.x; li < T; li += blockDim.x) {
-        const int xl = li % T0, yl = li / T0;
+        const int xl = li & m0, yl = li >> sh0;
         const uint32_t b = bs[li];
         if (b & 1u) {
             if (xl + 1 < T0) {
@@ -429,8 +449,8 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     for (int li = threadIdx.x; li < T; li += blockDim.x) {
         int32_t r = li;
         for (int it = 0; p[r] != r && it < kTileSites; ++it) r = p[r];
-        const int64_t s = base + li % T0 + (int64_t)(li / T0) * L0;
-        a.parent[s] = (int32_t)(base + r % T0 + (int64_t)(r / T0) * L0);
+        const int64_t s = base + (li & m0) + (int64_t)(li >> sh0) * L0;
+        a.parent[s] = (int32_t)(base + (r & m0) + (int64_t)(r >> sh0) * L0);
         const uint32_t bit = r == li ? 1u << (s & 31) : 0u;
         if (T0 >= 32) {
             const uint32_t word = __reduce_or_sync(0xffffffffu, bit);
@@ -464,7 +484,7 @@ __global__ void __launch_bounds__(kThreads) boundary_hook_kernel(ClusterArgs a) 
     if (D >= 2 && T1 < L1) {  // rows with y = k*T1 + T1-1: n / T1 sites
         const int64_t per_row = L0;
         for (int64_t c = t0; c < n / T1; c += stride) {
-            const int64_t row = c / per_row;  // index among the selected rows
+            const int64_t row = fdiv((uint32_t)c, a.g.dm[0], a.g.dl[0]);  // index among the selected rows
             const int64_t s = (row * T1 + (T1 - 1)) * per_row + (c - row * per_row);
             if (!(a.bonds[s] & 2u)) continue;
             int32_t x[D];
