@@ -11,9 +11,9 @@
 //               axis-minor order (cluster.rs:44-62), placed by a device-wide
 //               exclusive scan (decoupled look-back) over agreeing bonds.
 //  2. labels -- lock-free union-find: every open bond unites its ends by
-//               hooking the larger root under the smaller with a CAS, then the
-//               roots of the tile-local components are flattened and every
-//               site takes its root in two hops inside the relabel pass.
+//               hooking the larger root under the smaller with a CAS; the
+//               relabel pass then walks each site to its root (a short walk:
+//               sites point at their tile-local roots) and stores it.
 //               Roots only ever hook under smaller roots, so
 //               each component ends rooted at its minimum site: the canonical
 //               min-site label of the reference GPU (the fixed point of
@@ -66,7 +66,6 @@ struct ClusterArgs {
     uint8_t *state;
     uint8_t *bonds;
     int32_t *parent;
-    uint32_t *rootbits;  // bit s set: site s was the root of its tile-local component
     uint8_t *fresh;
     int32_t *rank;
     struct ChunkBase {     // stream relabel: per root_rank chunk, the state at the label draw of
@@ -443,21 +442,12 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     __syncthreads();
     // The forest is final: each site walks to its local root (read-only; trees at β_c are
     // about 2.3 deep on average, at most ~10, so this beats block-wide pointer-jumping rounds)
-    // and points at it.  The local roots are marked in rootbits: with T0 >= 32 a warp's 32
-    // sites are one aligned word of the mask, written whole; narrower tiles set bits
-    // atomically in words that the roots pass cleared.
+    // and points at it.
     for (int li = threadIdx.x; li < T; li += blockDim.x) {
         int32_t r = li;
         for (int it = 0; p[r] != r && it < kTileSites; ++it) r = p[r];
         const int64_t s = base + (li & m0) + (int64_t)(li >> sh0) * L0;
         a.parent[s] = (int32_t)(base + (r & m0) + (int64_t)(r >> sh0) * L0);
-        const uint32_t bit = r == li ? 1u << (s & 31) : 0u;
-        if (T0 >= 32) {
-            const uint32_t word = __reduce_or_sync(0xffffffffu, bit);
-            if (lane == 0) a.rootbits[s >> 5] = word;
-        } else if (bit) {
-            atomicOr(&a.rootbits[s >> 5], bit);
-        }
     }
 }
 
@@ -505,8 +495,8 @@ __global__ void __launch_bounds__(kThreads) boundary_hook_kernel(ClusterArgs a) 
     }
 }
 
-// Read-only find for the flatten pass: a compressing find could overwrite a
-// site another thread has just flattened with a non-root ancestor.
+// Read-only find for the relabel pass: a compressing find could overwrite a
+// site another thread has just set to its root with a non-root ancestor.
 __device__ __forceinline__ int32_t find_root_ro(const int32_t *parent, int32_t x, int cap, Control *ctrl) {
     int32_t p = ld_relaxed32(&parent[x]);
     int it = 0;
@@ -521,38 +511,16 @@ __device__ __forceinline__ int32_t find_root_ro(const int32_t *parent, int32_t x
     return x;
 }
 
-// Points every tile-local root straight at its component's root and clears
-// the mask; one thread per site, a warp per mask word.  No union runs any
-// more, so the root a walk ends on is final: the walk writes it back along
-// its path, and since final roots are the only values stored, concurrent
-// walks only ever find shorter paths.  Afterwards every site is at most two
-// hops from its root: tile_hook left it pointing at its local root, and the
-// boundary unions only re-point roots, or halve paths onto local roots.
-__global__ void flatten_roots_kernel(ClusterArgs a) {
-    const int64_t n = a.g.n_sites;
-    const int64_t n_pad = (n + 31) & ~(int64_t)31;  // whole warps, so the word clear below is warp-wide
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_pad; s += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t word = a.rootbits[s >> 5];
-        __syncwarp();
-        if (word && (threadIdx.x & 31) == 0) a.rootbits[s >> 5] = 0u;
-        if (!((word >> (s & 31)) & 1u)) continue;
-        const int32_t root = find_root_ro(a.parent, (int32_t)s, a.cap, a.ctrl);
-        int32_t x = (int32_t)s;
-        for (int it = 0; x != root && it <= a.cap; ++it) {
-            const int32_t nx = ld_relaxed32(&a.parent[x]);
-            a.parent[x] = root;
-            x = nx;
-        }
-    }
-}
-
-// The root of site s once flatten_roots_kernel ran; also stores it, which
-// leaves the parent array flat (every site holding its root) for the
-// readers after the sweep.  A site read here as another's parent is a
-// local root, already holding its root, so the store does not change it.
+// The root of site s after the boundary unions; also stores it, which leaves
+// the parent array flat (every site holding its root) for the readers after
+// the sweep.  tile_hook left every site pointing at its local root, and the
+// boundary unions only re-point roots (or halve paths onto local roots), so
+// the walk from a site's parent is short: at beta_c about 7 % of the local
+// roots end up under another root, a few levels deep at most.  Every value
+// stored is a final root, so concurrent walks stay correct.
 __device__ __forceinline__ int32_t take_root(const ClusterArgs &a, int64_t s) {
     const int32_t p = a.parent[s];
-    const int32_t r = a.parent[p];
+    const int32_t r = find_root_ro(a.parent, p, a.cap, a.ctrl);
     if (r != p) a.parent[s] = r;
     return r;
 }
@@ -789,7 +757,6 @@ __global__ void size_hist_kernel(const int32_t *parent, const int32_t *size, int
 struct ClusterDev {
     uint8_t *bonds = nullptr;
     int32_t *parent = nullptr;
-    uint32_t *rootbits = nullptr;
     uint8_t *fresh = nullptr;
     int32_t *rank = nullptr;
     ClusterArgs::ChunkBase *chunk_base = nullptr;
@@ -821,7 +788,6 @@ ClusterArgs cluster_args(plq_chain *c) {
     a.state = c->d_state;
     a.bonds = cd->bonds;
     a.parent = cd->parent;
-    a.rootbits = cd->rootbits;
     a.fresh = cd->fresh;
     a.rank = cd->rank;
     a.chunk_base = cd->chunk_base;
@@ -879,8 +845,7 @@ int sweep_d(plq_chain *c, uint64_t sweeps) {
         }
         tile_hook_kernel<D><<<(unsigned)cd->n_tiles, kThreads, 0, c->stream>>>(a);
         boundary_hook_kernel<D><<<gs, kThreads, 0, c->stream>>>(a);
-        flatten_roots_kernel<<<gs, kThreads, 0, c->stream>>>(a);
-        c->launches += 4;
+        c->launches += 3;
         if (!stream) {
             relabel_keyed_kernel<<<gs, kThreads, 0, c->stream>>>(a);
             c->launches++;
@@ -971,9 +936,6 @@ int cluster_create(plq_chain *c) {
     } else {
         alloc((void **)&cd->bonds, (size_t)n);
         alloc((void **)&cd->parent, sizeof(int32_t) * (size_t)n);
-        alloc((void **)&cd->rootbits, sizeof(uint32_t) * (size_t)((n + 31) / 32));
-        if (e == cudaSuccess)
-            e = cudaMemsetAsync(cd->rootbits, 0, sizeof(uint32_t) * (size_t)((n + 31) / 32), c->stream);
         alloc((void **)&cd->desc, sizeof(unsigned long long) * (size_t)cd->n_chunks);
         if (e == cudaSuccess)
             e = cudaMemsetAsync(cd->desc, 0, sizeof(unsigned long long) * (size_t)cd->n_chunks, c->stream);
@@ -1010,7 +972,7 @@ int cluster_sweep(plq_chain *c) { return cluster_sweep_n(c, 1); }
 void cluster_free(plq_chain *c) {
     ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
     if (!cd) return;
-    void *ptrs[] = {cd->bonds, cd->parent, cd->rootbits, cd->fresh, cd->rank, cd->chunk_base, cd->stamp, cd->queue,
+    void *ptrs[] = {cd->bonds, cd->parent, cd->fresh, cd->rank, cd->chunk_base, cd->stamp, cd->queue,
                     cd->desc, cd->events, cd->first_new, cd->sizes};
     for (void *p : ptrs)
         if (p) cudaFree(p);
