@@ -512,18 +512,37 @@ __device__ __forceinline__ int32_t find_root_ro(const int32_t *parent, int32_t x
     return x;
 }
 
-// The root of site s after the boundary unions; also stores it, which leaves
-// the parent array flat (every site holding its root) for the readers after
-// the sweep.  tile_hook left every site pointing at its local root, and the
-// boundary unions only re-point roots (or halve paths onto local roots), so
-// the walk from a site's parent is short: at beta_c about 7 % of the local
-// roots end up under another root, a few levels deep at most.  Every value
-// stored is a final root, so concurrent walks stay correct.
-__device__ __forceinline__ int32_t take_root(const ClusterArgs &a, int64_t s) {
-    const int32_t p = a.parent[s];
-    const int32_t r = find_root_ro(a.parent, p, a.cap, a.ctrl);
-    if (r != p) a.parent[s] = r;
-    return r;
+// Sites a thread resolves at once (stride apart): the loads of all of them
+// are issued before any is used, so their latencies overlap.
+constexpr int kRootBatch = 4;
+
+// The roots of sites s0, s0 + stride, ... after the boundary unions; also
+// stores them, which leaves the parent array flat (every site holding its
+// root) for the readers after the sweep.  tile_hook left every site pointing
+// at its local root, and the boundary unions only re-point roots (or halve
+// paths onto local roots), so the walk from a site's parent is short: at
+// beta_c about 7 % of the local roots end up under another root, a few levels
+// deep at most.  Every value stored is a final root, so concurrent walks stay
+// correct.
+__device__ __forceinline__ void take_roots(const ClusterArgs &a, int64_t s0, int64_t stride, int64_t n,
+                                           int32_t *root) {
+    int32_t p[kRootBatch], q[kRootBatch];
+#pragma unroll
+    for (int k = 0; k < kRootBatch; ++k) {
+        const int64_t s = s0 + k * stride;
+        p[k] = s < n ? a.parent[s] : 0;  // only this thread writes parent[s] here
+    }
+#pragma unroll
+    for (int k = 0; k < kRootBatch; ++k) q[k] = s0 + k * stride < n ? ld_relaxed32(&a.parent[p[k]]) : 0;
+#pragma unroll
+    for (int k = 0; k < kRootBatch; ++k) {
+        const int64_t s = s0 + k * stride;
+        root[k] = 0;
+        if (s >= n) continue;
+        const int32_t r = q[k] == p[k] ? p[k] : find_root_ro(a.parent, q[k], a.cap, a.ctrl);
+        if (r != p[k]) a.parent[s] = r;
+        root[k] = r;
+    }
 }
 
 // ----------------------------------------------------------- 3. relabel
@@ -531,17 +550,25 @@ __device__ __forceinline__ int32_t take_root(const ClusterArgs &a, int64_t s) {
 __global__ void relabel_keyed_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
     const uint32_t q = (uint32_t)a.q;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t root = (uint32_t)take_root(a, s);
-        float u = __fmul_rn((float)keyed24(a.seed32 ^ kRootSalt, root, a.sweep32), 5.9604644775390625e-8f);
-        if (a.relabel == PLQ_RELABEL_FORCED) {
-            uint32_t step = __float2uint_rz(__fmul_rn(u, (float)(q - 1u)));
-            if (step >= q - 1u) step = q - 2u;
-            a.state[s] = (uint8_t)((a.state[s] + 1u + step) % q);
-        } else {
-            uint32_t draw = __float2uint_rz(__fmul_rn(u, (float)q));
-            if (draw >= q) draw = q - 1u;
-            a.state[s] = (uint8_t)draw;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s0 < n; s0 += stride * kRootBatch) {
+        int32_t roots[kRootBatch];
+        take_roots(a, s0, stride, n, roots);
+#pragma unroll
+        for (int k = 0; k < kRootBatch; ++k) {
+            const int64_t s = s0 + k * stride;
+            if (s >= n) continue;
+            const uint32_t root = (uint32_t)roots[k];
+            float u = __fmul_rn((float)keyed24(a.seed32 ^ kRootSalt, root, a.sweep32), 5.9604644775390625e-8f);
+            if (a.relabel == PLQ_RELABEL_FORCED) {
+                uint32_t step = __float2uint_rz(__fmul_rn(u, (float)(q - 1u)));
+                if (step >= q - 1u) step = q - 2u;
+                a.state[s] = (uint8_t)((a.state[s] + 1u + step) % q);
+            } else {
+                uint32_t draw = __float2uint_rz(__fmul_rn(u, (float)q));
+                if (draw >= q) draw = q - 1u;
+                a.state[s] = (uint8_t)draw;
+            }
         }
     }
 }
@@ -651,8 +678,17 @@ __global__ void root_draw_kernel(ClusterArgs a) {
 
 __global__ void apply_fresh_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
-        a.state[s] = a.fresh[take_root(a, s)];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s0 < n; s0 += stride * kRootBatch) {
+        int32_t roots[kRootBatch];
+        take_roots(a, s0, stride, n, roots);
+        uint8_t f[kRootBatch];
+#pragma unroll
+        for (int k = 0; k < kRootBatch; ++k) f[k] = s0 + k * stride < n ? a.fresh[roots[k]] : 0;
+#pragma unroll
+        for (int k = 0; k < kRootBatch; ++k)
+            if (s0 + k * stride < n) a.state[s0 + k * stride] = f[k];
+    }
 }
 
 __global__ void finish_pos_kernel(Control *ctrl, int n_events) {
