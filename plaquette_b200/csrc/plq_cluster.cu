@@ -726,19 +726,30 @@ __global__ void __launch_bounds__(kBfsThreads) wolff_bfs_kernel(ClusterArgs a) {
                 int64_t u = a.queue[i];
                 int32_t x[D];
                 site_coords<D>(a.g, u, x);
+                // the 2D neighbours' loads, then their stamp exchanges, each issued together so
+                // their latencies overlap; the cluster (a set) does not depend on the order
+                int64_t v[2 * D];
+                uint8_t sv[2 * D];
 #pragma unroll
-                for (int mu = 0; mu < D; ++mu) {
+                for (int k = 0; k < 2 * D; ++k) {
+                    v[k] = (k & 1) == 0 ? nbr_plus(a.g, u, x, k >> 1) : nbr_minus(a.g, u, x, k >> 1);
+                    sv[k] = a.state[v[k]];
+                }
+                bool join[2 * D];
 #pragma unroll
-                    for (int sgn = 0; sgn < 2; ++sgn) {
-                        int64_t v = sgn == 0 ? nbr_plus(a.g, u, x, mu) : nbr_minus(a.g, u, x, mu);
-                        if (a.state[v] != cur) continue;
-                        uint32_t bond = (uint32_t)((sgn == 0 ? u : v) * D + mu);
-                        if (keyed24(a.seed32 ^ kBondKey, bond, sweep) >= a.kp24) continue;
-                        if (atomicExch(&a.stamp[v], epoch) == epoch) continue;  // already a member
-                        int slot = atomicAdd(&s_tail, 1);
-                        a.queue[slot] = (int32_t)v;
-                        atomicMin(&s_min, (int32_t)v);
-                    }
+                for (int k = 0; k < 2 * D; ++k) {
+                    const uint32_t bond = (uint32_t)(((k & 1) == 0 ? u : v[k]) * D + (k >> 1));
+                    join[k] = sv[k] == cur && keyed24(a.seed32 ^ kBondKey, bond, sweep) < a.kp24;
+                }
+#pragma unroll
+                for (int k = 0; k < 2 * D; ++k)
+                    if (join[k]) join[k] = atomicExch(&a.stamp[v[k]], epoch) != epoch;  // not yet a member
+#pragma unroll
+                for (int k = 0; k < 2 * D; ++k) {
+                    if (!join[k]) continue;
+                    int slot = atomicAdd(&s_tail, 1);
+                    a.queue[slot] = (int32_t)v[k];
+                    atomicMin(&s_min, (int32_t)v[k]);
                 }
             }
             __syncthreads();
