@@ -104,6 +104,9 @@ int plq_device_count(int *count);
 
 /* Gpu::new (src/device.rs:42-78): PLQ_ENODEV when no device is present. */
 int plq_ctx_create(int device_ordinal, plq_ctx **out);
+/* Chains, ensembles and servers copy the context's record when they are
+   created, so a context may be destroyed before them (a garbage collector may
+   finalize a Gpu before the chains made from it). */
 void plq_ctx_destroy(plq_ctx *ctx);
 
 /* ------------------------------------------------ host-side helpers */

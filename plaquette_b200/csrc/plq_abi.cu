@@ -235,7 +235,7 @@ static u128 to_u128(uint64_t lo, uint64_t hi) {
 
 void chain_free(plq_chain *c) {
     if (!c) return;
-    if (c->ctx) cudaSetDevice(c->ctx->device);
+    if (c->ctx) plq_enter_device(c->ctx->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->obs_stream) cudaStreamSynchronize(c->obs_stream);
     cluster_free(c);
@@ -294,10 +294,11 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
                                                 std::to_string(start[i]) + ", not below q = " + std::to_string(q));
         }
     }
-    PLQ_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(ctx->device), "cudaSetDevice");
 
     plq_chain *c = new plq_chain();
-    c->ctx = ctx;
+    c->ctx_copy = *ctx;
+    c->ctx = &c->ctx_copy;
     c->desc = *desc;
     c->q = desc->model == PLQ_POTTS ? desc->q : 2;
     c->d = desc->d;
@@ -598,7 +599,7 @@ static int run_sweeps(plq_chain *c, uint64_t sweeps) {
 
 extern "C" int plq_chain_advance(plq_chain *c, uint64_t sweeps) {
     if (!c) return plq_fail(PLQ_EINVAL, "chain is NULL");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     return run_sweeps(c, sweeps);
 }
 
@@ -639,7 +640,7 @@ static int ensure_io(plq_chain *c) {
 
 extern "C" int plq_chain_read(plq_chain *c, uint8_t *out) {
     if (!c || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     if (c->link) {
         int rc = ensure_io(c);
         if (rc == PLQ_OK) rc = state_to_host_order(c, c->d_io);
@@ -672,7 +673,7 @@ extern "C" int plq_chain_axis_pair_sums(plq_chain *c, int64_t *out, int64_t capa
     if (capacity < entries)
         return plq_fail(PLQ_EINVAL, "output holds " + std::to_string(capacity) + " entries, " +
                                         std::to_string(entries) + " needed");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     int rc = ensure_meas(c, entries);
     if (rc != PLQ_OK) return rc;
     // the (mu, r >= 1) pairs: all mu values, then all r values
@@ -716,7 +717,7 @@ extern "C" int plq_chain_polyakov(plq_chain *c, int32_t dir, int64_t *sum, int64
     if (!c || !sum || !lines) return plq_fail(PLQ_EINVAL, "NULL argument");
     if (!c->link) return plq_fail(PLQ_EINVAL, "the Polyakov loop is a gauge measurement");
     if (dir < 0 || dir >= c->d) return plq_fail(PLQ_EINVAL, "direction out of range");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     int rc = ensure_meas(c, 1);
     if (rc != PLQ_OK) return rc;
     cudaError_t e = launch_polyakov(c->d_state, c->g, dir, c->d_meas, c->stream);
@@ -747,7 +748,7 @@ extern "C" int plq_chain_wilson(plq_chain *c, int32_t max_side, int64_t *totals,
     if (capacity < entries)
         return plq_fail(PLQ_EINVAL, "totals hold " + std::to_string(capacity) + " entries, " +
                                         std::to_string(entries) + " needed");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     int rc = ensure_meas(c, entries);
     if (rc != PLQ_OK) return rc;
     if (!c->d_loop_bits)
@@ -775,7 +776,7 @@ extern "C" int plq_chain_wilson(plq_chain *c, int32_t max_side, int64_t *totals,
 
 extern "C" int plq_chain_primaries(plq_chain *c, int64_t *out, int32_t *n_out) {
     if (!c) return plq_fail(PLQ_EINVAL, "NULL argument");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     int np = primaries_count(c->desc.model, c->q);
     cudaError_t e = launch_primaries(c->d_state, c->g, c->desc.model, c->q, c->d_obs, c->stream);
     c->launches++;
@@ -793,7 +794,7 @@ extern "C" int plq_chain_next(plq_chain *c, uint8_t *out_states, int64_t *out_pr
 
 extern "C" int plq_chain_next_batch(plq_chain *c, int64_t count, uint8_t *out_states, int64_t *out_primaries) {
     if (!c || count < 0) return plq_fail(PLQ_EINVAL, "bad arguments");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     const int np = primaries_count(c->desc.model, c->q);
     // snapshot capacity: the reference clamps its staging batch by the
     // device's buffer limit (device.rs:268-274); here by 1 GiB of snapshots.
@@ -862,7 +863,7 @@ extern "C" int plq_chain_next_batch(plq_chain *c, int64_t count, uint8_t *out_st
 
 extern "C" int plq_chain_sync(plq_chain *c) {
     if (!c) return plq_fail(PLQ_EINVAL, "chain is NULL");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     return check_status(c);
 }
 
@@ -873,7 +874,7 @@ extern "C" uint64_t plq_chain_sweeps_done(plq_chain *c) { return c ? c->sweeps_d
 extern "C" int plq_chain_stream_position(plq_chain *c, uint64_t *out) {
     if (!c || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
     if (c->desc.rng != PLQ_RNG_STREAM) return plq_fail(PLQ_EINVAL, "not a PCG-stream chain");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     uint64_t rel = c->host_pos;
     if (c->lookback || c->cluster) {
         unsigned long long pos[2];
@@ -891,7 +892,7 @@ extern "C" uint64_t plq_chain_launches(plq_chain *c) { return c ? c->launches : 
 extern "C" int plq_chain_cluster_labels(plq_chain *c, int32_t *out) {
     if (!c || !out) return plq_fail(PLQ_EINVAL, "NULL argument");
     if (!c->cluster) return plq_fail(PLQ_EINVAL, "not a cluster chain");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     int rc = cluster_labels(c, out);
     return rc == PLQ_OK ? check_status(c) : rc;
 }
@@ -899,7 +900,7 @@ extern "C" int plq_chain_cluster_labels(plq_chain *c, int32_t *out) {
 extern "C" int plq_chain_cluster_histogram(plq_chain *c, int64_t *hist, int32_t nbins) {
     if (!c || !hist) return plq_fail(PLQ_EINVAL, "NULL argument");
     if (!c->cluster) return plq_fail(PLQ_EINVAL, "not a cluster chain");
-    PLQ_CUDA(cudaSetDevice(c->ctx->device), "cudaSetDevice");
+    PLQ_CUDA(plq_enter_device(c->ctx->device), "cudaSetDevice");
     int rc = cluster_size_histogram(c, hist, nbins);
     return rc == PLQ_OK ? check_status(c) : rc;
 }

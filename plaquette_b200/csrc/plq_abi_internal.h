@@ -18,8 +18,21 @@ struct plq_ctx {
     size_t mem_total = 0;
 };
 
+// Makes `device` current and drops a non-sticky error that an unrelated
+// earlier runtime call left on this thread, so that the launch checks after it
+// report only their own launches.  A sticky (device) error cannot be cleared
+// and still fails every later call.
+inline cudaError_t plq_enter_device(int device) {
+    (void)cudaGetLastError();
+    return cudaSetDevice(device);
+}
+
 struct plq_chain {
-    plq_ctx *ctx = nullptr;
+    // The context's record, copied at creation: the chain stays valid if the
+    // caller destroys the context first (a garbage collector may finalize the
+    // two in either order).
+    plq_ctx ctx_copy;
+    plq_ctx *ctx = nullptr;  // = &ctx_copy
     plq_chain_desc desc;
     int q = 2, d = 1;
     bool link = false, cluster = false, lookback = false;

@@ -779,9 +779,15 @@ __global__ void __launch_bounds__(kBfsThreads) wolff_bfs_kernel(ClusterArgs a) {
 }
 
 // ------------------------------------------------------------ sizes
+// Cluster sizes: one atomic per distinct root among a warp's 32 sites (a big
+// cluster's root would otherwise take one atomic per site).
 __global__ void sizes_kernel(const int32_t *parent, int32_t *size, int64_t n) {
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&size[parent[s]], 1);
+    const int64_t n_pad = (n + 31) & ~(int64_t)31;  // whole warps per iteration: the match below is warp-wide
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n_pad; s += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t r = s < n ? parent[s] : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, r);
+        if (r >= 0 && (int)(threadIdx.x & 31u) == __ffs(peers) - 1) atomicAdd(&size[r], __popc(peers));
+    }
 }
 // Clusters per size bin [2^k, 2^(k+1)): counted per CTA in shared memory (bins
 // 0..31 cover every int32 size), one global atomic per bin per CTA.

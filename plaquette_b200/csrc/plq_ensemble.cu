@@ -377,7 +377,8 @@ __global__ void swap_kernel(EnsArgs e, unsigned long long att) { swap_phase(e, a
 }  // namespace
 
 struct plq_ensemble {
-    plq_ctx *ctx = nullptr;
+    plq_ctx ctx_copy;        // the context's record, copied at creation (outlives the caller's)
+    plq_ctx *ctx = nullptr;  // = &ctx_copy
     cudaStream_t stream = nullptr;
     std::vector<plq_chain_desc> descs;
     std::vector<EnsMember> members;            // host copies (device pointers inside)
@@ -554,10 +555,11 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
             return plq_fail(PLQ_EUNSUPPORTED,
                             "stream-mode Metropolis needs a device-wide scan per pass; ensembles run it keyed");
     }
-    cudaError_t ce = cudaSetDevice(ctx->device);
+    cudaError_t ce = plq_enter_device(ctx->device);
     if (ce != cudaSuccess) return ens_fail(ce, "cudaSetDevice");
     plq_ensemble *E = new plq_ensemble();
-    E->ctx = ctx;
+    E->ctx_copy = *ctx;
+    E->ctx = &E->ctx_copy;
     auto fail = [&](int code) {
         plq_ensemble_destroy(E);
         return code;
@@ -780,7 +782,7 @@ static int ens_status(plq_ensemble *E) {
 extern "C" int plq_ensemble_advance(plq_ensemble *E, uint64_t sweeps) {
     if (!E) return plq_fail(PLQ_EINVAL, "NULL ensemble");
     if (sweeps == 0) return PLQ_OK;
-    cudaError_t e = cudaSetDevice(E->ctx->device);
+    cudaError_t e = plq_enter_device(E->ctx->device);
     if (e != cudaSuccess) return ens_fail(e, "cudaSetDevice");
     // one persistent launch, captured once per (sweeps, configuration) and replayed
     if (!E->graph || E->graph_sweeps != sweeps || E->graph_ranks != E->ranks || E->graph_ctas != E->ctas_per_sm) {
@@ -817,7 +819,7 @@ extern "C" int plq_ensemble_advance(plq_ensemble *E, uint64_t sweeps) {
 
 extern "C" int plq_ensemble_advance_unbatched(plq_ensemble *E, uint64_t sweeps) {
     if (!E) return plq_fail(PLQ_EINVAL, "NULL ensemble");
-    cudaError_t e = cudaSetDevice(E->ctx->device);
+    cudaError_t e = plq_enter_device(E->ctx->device);
     if (e != cudaSuccess) return ens_fail(e, "cudaSetDevice");
     // host mirrors of the device-resident state the per-member launches need
     LaunchState ls;
@@ -892,7 +894,7 @@ extern "C" int plq_ensemble_set_config(plq_ensemble *E, int32_t ranks_per_thread
 extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t *ranks_out, int32_t *ctas_out,
                                  double *ms_per_sweep_out) {
     if (!E || trial_sweeps <= 0) return plq_fail(PLQ_EINVAL, "bad arguments");
-    cudaError_t e = cudaSetDevice(E->ctx->device);
+    cudaError_t e = plq_enter_device(E->ctx->device);
     if (e != cudaSuccess) return ens_fail(e, "cudaSetDevice");
     // snapshot: member states, PT slots, positions, launch state
     int64_t total = 0;
@@ -1035,7 +1037,7 @@ extern "C" uint64_t plq_ensemble_launches(plq_ensemble *E) { return E ? E->launc
 
 extern "C" void plq_ensemble_destroy(plq_ensemble *E) {
     if (!E) return;
-    if (E->ctx) cudaSetDevice(E->ctx->device);
+    if (E->ctx) plq_enter_device(E->ctx->device);
     if (E->stream) cudaStreamSynchronize(E->stream);
     drop_graph(E);
     for (void *p : E->allocs) cudaFree(p);
@@ -1081,7 +1083,8 @@ struct ServerJob {
 };
 
 struct plq_server {
-    plq_ctx *ctx = nullptr;
+    plq_ctx ctx_copy;        // the context's record, copied at creation (outlives the caller's)
+    plq_ctx *ctx = nullptr;  // = &ctx_copy
     uint64_t budget = 0, used = 0;
     int max_slots = 0;
     double tick_ms = 10.0;
@@ -1436,7 +1439,7 @@ void retire(plq_server *S, ServerJob *j, cudaStream_t stream) {
 }
 
 void worker_loop(plq_server *S) {
-    cudaSetDevice(S->ctx->device);
+    plq_enter_device(S->ctx->device);
     cudaStream_t stream = nullptr;
     cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
     TickBuffers B;
@@ -1547,12 +1550,13 @@ extern "C" int plq_server_create(plq_ctx *ctx, uint64_t budget_bytes, int32_t ma
     if (!ctx || !out || max_slots <= 0) return plq_fail(PLQ_EINVAL, "bad server arguments");
     *out = nullptr;
     plq_server *S = new plq_server();
-    S->ctx = ctx;
+    S->ctx_copy = *ctx;
+    S->ctx = &S->ctx_copy;
     S->max_slots = max_slots;
     S->tick_ms = tick_ms > 0 ? tick_ms : 10.0;
     if (budget_bytes == 0) {
         size_t free_b = 0, total_b = 0;
-        cudaSetDevice(ctx->device);
+        plq_enter_device(ctx->device);
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
             delete S;
             return plq_fail(PLQ_ECUDA, "cudaMemGetInfo failed");

@@ -262,3 +262,25 @@ def test_out_of_range_start_state_refused(gpu, pos, bad):
         plq.GpuChain(gpu, d, start)
     ok = np.ones(64 * 64, dtype=np.uint8)
     plq.GpuChain(gpu, d, ok).close()
+
+
+def test_chain_outlives_its_context():
+    """A garbage collector may finalize a context before a chain made from it
+    (a chain kept alive by a traceback cycle, say).  The chain copies the
+    context's record when it is created, so it keeps running after the
+    context is destroyed, and a new context's chains run cleanly after it."""
+    g = plq.Gpu.new()
+    d = plq.make_desc(plq.ISING, 2, (64, 64), plq.METROPOLIS, beta=0.44, seed=1, rng=plq.RNG_KEYED,
+                      sweeps_between=1, batch=1)
+    c = plq.GpuChain(g, d, None)
+    c.advance(2)
+    plq.lib().plq_ctx_destroy(g._h)  # the context goes first
+    g._h = None
+    c.advance(2)
+    first = next(c)
+    c.close()
+    g2 = plq.Gpu.new()
+    c2 = plq.GpuChain(g2, d, None)
+    c2.advance(4)
+    assert np.array_equal(next(c2), first)  # same seed, same keyed sweeps
+    c2.close()
