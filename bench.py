@@ -265,8 +265,8 @@ def run_product(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": prof.get("dram_bytes_per_launch"),
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes, "kernel": w[6],
-                     "note": "instruction-issue bound: the reference's per-site RNG costs more issue slots than "
-                             "HBM allows at 2 B/update (see DESIGN.md)"},
+                     "note": "instruction-issue bound: the reference's per-site RNG (a 128-bit LCG step or "
+                             "two 32-bit hashes per draw) costs more issue slots than HBM allows at 2 B/update"},
         "e2e": {"value": round(e2e_value, 3), "unit": "site updates/ns",
                 "h2d_bytes_per_step": N_SITES / args.steps,
                 "d2h_bytes_per_step": 8 * n_prim + N_SITES / args.steps,
