@@ -11,21 +11,24 @@
 //               axis-minor order (cluster.rs:44-62), placed by a device-wide
 //               exclusive scan (decoupled look-back) over agreeing bonds.
 //  2. labels -- lock-free union-find: every open bond unites its ends by
-//               hooking the larger root under the smaller with a CAS; the
-//               relabel pass then walks each site to its root (a short walk:
-//               sites point at their tile-local roots) and stores it.
-//               Roots only ever hook under smaller roots, so
-//               each component ends rooted at its minimum site: the canonical
-//               min-site label of the reference GPU (the fixed point of
-//               cluster_prelude.wgsl:113-147), and, ranked, the reference
-//               CPU's first-encounter compaction (cluster.rs:199-226).
+//               hooking the larger root under the smaller with a CAS, first
+//               inside 64x64 tiles in shared memory (tile_hook_kernel), then
+//               for the bonds that leave a tile (boundary_hook_kernel); the
+//               relabel pass walks each site to its root (a short walk: sites
+//               point at their tile-local roots) and stores it.  Roots only
+//               ever hook under smaller roots, so each component ends rooted
+//               at its minimum site: the canonical min-site label of the
+//               reference GPU (the fixed point of cluster_prelude.wgsl:113-147),
+//               and, ranked, the reference CPU's first-encounter compaction
+//               (cluster.rs:199-226).
 //  3. relabel -- keyed: per-root keyed draw (cluster_relabel.wgsl:39-90).
 //               PCG stream: clusters in root order draw next_below(q) (or the
-//               forced-change proposal) at consecutive positions; rand's
-//               range sampler occasionally takes a second draw, which shifts
-//               every later cluster -- those rare events are found and fixed
-//               up by re-running the (parallel) draw pass with the events
-//               known, in a short host loop.
+//               forced-change proposal) at consecutive positions, inside the
+//               rank scan; rand's range sampler occasionally takes a second
+//               draw, which shifts every later cluster -- those rare events
+//               are reported by the scan and fixed up by re-running the
+//               (parallel) draw pass with the events known, in a short host
+//               loop.
 //
 // Wolff on the keyed stream: the reference relabels the cluster of a keyed
 // seed site in the full decomposition (cluster_relabel.wgsl:55-66).  Here a
@@ -193,6 +196,8 @@ __device__ __forceinline__ int64_t take_chunk(const ClusterArgs &a, bool lookbac
 }
 
 // ------------------------------------------------------------- 1. bonds
+static_assert(kSitesPerThread == 8, "the bonds pass loads and stores a thread's sites as one 8-byte word");
+
 // High bit of each byte of the result set iff that byte of a equals that of b.
 __device__ __forceinline__ uint64_t bytes_equal(uint64_t a, uint64_t b) {
     const uint64_t e = a ^ b, lo7 = 0x7F7F7F7F7F7F7F7Full;
