@@ -96,6 +96,9 @@ extern "C" int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int
         n *= shape[i];
     }
     cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    // the caller's current device; drop a non-sticky error an unrelated earlier
+    // runtime call left on this thread, so the checks below see only our calls
+    (void)cudaGetLastError();
     unsigned char *scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc != PLQ_OK) return rc;
