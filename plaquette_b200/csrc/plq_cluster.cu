@@ -619,12 +619,22 @@ __global__ void __launch_bounds__(kThreads) root_rank_kernel(ClusterArgs a) {
     const int64_t s0 = chunk * kChunk + (int64_t)threadIdx.x * kSitesPerThread;
     int count = 0;
     uint32_t mask = 0;
+    if (s0 + kSitesPerThread <= n) {  // s0 is a multiple of 8: two aligned 16-byte loads
+        const int4 lo = *reinterpret_cast<const int4 *>(a.parent + s0);
+        const int4 hi = *reinterpret_cast<const int4 *>(a.parent + s0 + 4);
+        const int32_t par[kSitesPerThread] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
 #pragma unroll
-    for (int i = 0; i < kSitesPerThread; ++i) {
-        int64_t s = s0 + i;
-        if (s < n && a.parent[s] == (int32_t)s) {
-            mask |= 1u << i;
-            ++count;
+        for (int i = 0; i < kSitesPerThread; ++i)
+            if (par[i] == (int32_t)(s0 + i)) mask |= 1u << i;
+        count = __popc(mask);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kSitesPerThread; ++i) {
+            int64_t s = s0 + i;
+            if (s < n && a.parent[s] == (int32_t)s) {
+                mask |= 1u << i;
+                ++count;
+            }
         }
     }
     int total;
