@@ -326,6 +326,9 @@ __global__ void __launch_bounds__(FTHREADS, FusedCfg<Q, STREAM>::ctas)
         if (z >= z0) {
             const size_t zoff0 = (size_t)gz0 * plane_sites;
             const uint8_t *zM = ring + slot(z - 1) * plane_bytes;
+            // both runs first, then the stores: a store to dst between them would order the
+            // second run's shared-memory reads after it and keep the two draw chains apart
+            uint4 out1[FRUNS_PER_THREAD];
 #pragma unroll
             for (int k = 0; k < FRUNS_PER_THREAD; ++k) {
                 if (STREAM)
@@ -333,10 +336,12 @@ __global__ void __launch_bounds__(FTHREADS, FusedCfg<Q, STREAM>::ctas)
                                  ? jump(a.jump, a.base, a.off1 + ((zoff0 + (size_t)rgy[k] * L0 + rx[k]) >> 1))
                                  : apply(a.plane, st1[k]);
                 u128 st = st1[k];
-                uint4 o = update_run<Q, STREAM, HB>(a, tab, sM, zM, sC, rrow[k], rx[k], L0, (rgy[k] + gz0 + 1) & 1,
+                out1[k] = update_run<Q, STREAM, HB>(a, tab, sM, zM, sC, rrow[k], rx[k], L0, (rgy[k] + gz0 + 1) & 1,
                                                     (uint32_t)(zoff0 + (size_t)rgy[k] * L0 + rx[k]), st);
-                *reinterpret_cast<uint4 *>(a.dst + zoff0 + (size_t)rgy[k] * L0 + rx[k]) = o;
             }
+#pragma unroll
+            for (int k = 0; k < FRUNS_PER_THREAD; ++k)
+                *reinterpret_cast<uint4 *>(a.dst + zoff0 + (size_t)rgy[k] * L0 + rx[k]) = out1[k];
         }
     }
     if (z_abort != INT_MAX && t == 0) {
