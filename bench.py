@@ -10,8 +10,10 @@ data path).  `--workload` selects the other 512^3 single-lattice cases (3D
 Ising Metropolis on the keyed or the PCG stream, q=3 Potts heat bath keyed).
 
 Prints one JSON line (rank 0).  ``--impl reference`` times the reference's
-CPU algorithm (the C restatement in oracle/, single thread -- the reference
-has no threading) on bounded samples of the same workload instead.
+CPU algorithm (the C restatement in oracle/) on bounded samples of the same
+workload instead: the local sweeps on every host thread (one independent run
+of site indices per thread; the reference itself is sequential), the cluster
+moves on one thread.
 """
 from __future__ import annotations
 
@@ -588,7 +590,8 @@ def run_cluster(args):
                       "peak": measured_peak_hbm()[0], "unit": "GB/s",
                       "frac": round(alg * args.steps / (dev_ms * 1e-3) / 1e9 / measured_peak_hbm()[0], 4),
                       "traffic": None, "peak_source": measured_peak_hbm()[1],
-                      "algorithmic_bytes_per_launch": alg, "kernel": "bonds + union-find + flatten + relabel",
+                      "algorithmic_bytes_per_launch": alg,
+                      "kernel": "bonds + tile union-find + boundary unions + relabel",
                       "note": "10.5 B/site per sweep algorithmic minimum"} if not wolff else
                      {"bound": "latency", "achieved": None, "peak": None, "unit": None, "frac": None,
                       "traffic": None, "note": "frontier BFS: work proportional to the cluster, not the lattice"}),
@@ -600,10 +603,75 @@ def run_cluster(args):
         "gpu_launches": launches,
         "clocks": clock_info,
     }
+    if rank == 0 and args.cpu_baseline:
+        units_c, dt_c, sample = cluster_cpu_sample(args.workload, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(units_c / dt_c, 4), "unit": unit, "cores": 1, "kind": "port",
+                                "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def cluster_cpu_sample(name: str, seconds: float, warmup: int = 0, max_units: int = 1 << 30):
+    """The oracle's restatement of the reference cluster move on one host
+    thread (the reference is sequential), on the workload's lattice from the
+    same start: Swendsen-Wang sweeps, or keyed Wolff updates (the reference
+    GPU's seeded decomposition filter), for about `seconds` after `warmup`
+    untimed ones.  Returns (units, seconds, description)."""
+    from oracle import oracle
+    import plaquette_b200 as plq
+
+    extent, rng_name, shape, beta, what = CLUSTER_WORKLOADS[name]
+    lat = oracle.Lattice(shape)
+    model = oracle.Model.ising(1.0)
+    start, off = plq.hot_start(SEED, 2, lat.n_sites)
+    state = start.copy()
+    ext = oracle.ALL if extent == "all" else oracle.SEEDED
+    relabel = oracle.REDRAW if extent == "all" else oracle.FORCED
+    if rng_name == "stream":
+        r = oracle.PcgStream(SEED)
+        r.advance(off)
+
+        def step(k):
+            oracle.cluster_sweep(model, lat, state, ext, relabel, beta, r)
+    else:
+        s32 = oracle.fold_seed(SEED)
+
+        def step(k):
+            oracle.keyed_cluster_sweep(model, lat, state, ext, relabel, beta, s32, k)
+    for k in range(warmup):
+        step(k)
+    done = 0
+    t0 = time.perf_counter()
+    while done < max_units and (done == 0 or time.perf_counter() - t0 < seconds):
+        step(warmup + done)
+        done += 1
+    dt = time.perf_counter() - t0
+    what_unit = "sweeps" if extent == "all" else "single-cluster updates"
+    return done, dt, f"{done} {what_unit} of the {'x'.join(map(str, shape))} lattice on one host thread"
+
+
+def run_reference_cluster(args):
+    """The reference arm of a cluster workload: the oracle's cluster move on
+    one host thread, `steps` sweeps or updates after `warmup` untimed ones."""
+    world = _env_int("WORLD_SIZE", 1)
+    if _env_int("RANK", 0) != 0:
+        return
+    extent = CLUSTER_WORKLOADS[args.workload][0]
+    unit = "cluster updates/s" if extent == "seeded" else "SW sweeps/s"
+    units, dt, sample = cluster_cpu_sample(args.workload, float("inf"), warmup=args.warmup, max_units=args.steps)
+    value = units / dt
+    line = {
+        "metric": unit, "value": round(value, 4), "unit": unit, "n_gpus": world, "steps": units,
+        "warmup": args.warmup, "ms_per_step": round(dt / units * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": CLUSTER_WORKLOADS[args.workload][4], "name": args.workload,
+                   "step": "one sweep" if extent == "all" else "one single-cluster update"},
+        "cpu_baseline": {"value": round(value, 4), "unit": unit, "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -620,10 +688,7 @@ def main():
     if args.warmup < 3 and args.impl == "product":
         args.warmup = 3
     if args.impl == "reference" and args.workload in CLUSTER_WORKLOADS:
-        if _env_int("RANK", 0) == 0:
-            print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the single-lattice "
-                                                                  "local sweep; cluster moves are measured on the "
-                                                                  "product arm only"}), flush=True)
+        run_reference_cluster(args)
     elif args.impl == "reference" and args.workload == ENSEMBLE_WORKLOAD:
         if _env_int("RANK", 0) == 0:
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble (one chain "
