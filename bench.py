@@ -486,6 +486,11 @@ def run_ensemble(args):
         "gpu_launches": launches,
         "clocks": clock_info,
     }
+    if rank == 0 and args.cpu_baseline:
+        cv, threads, n_members, _, dt_c = ensemble_cpu_sample(steps=6, warmup=1)
+        line["cpu_baseline"] = {"value": round(cv, 6), "unit": "site updates/ns", "cores": threads, "kind": "port",
+                                "sample": f"6 sweeps of all {n_members} members on {threads} threads "
+                                          f"({dt_c:.1f} s; tempering swaps left out)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ens.close()
@@ -652,6 +657,71 @@ def cluster_cpu_sample(name: str, seconds: float, warmup: int = 0, max_units: in
     return done, dt, f"{done} {what_unit} of the {'x'.join(map(str, shape))} lattice on one host thread"
 
 
+def ensemble_cpu_sample(steps: int, warmup: int):
+    """The batched-ensemble members on the host: the reference runs one chain
+    at a time, so each member's keyed sweep is the oracle's restatement of the
+    reference GPU checkerboard, the members spread over every host thread (one
+    member per thread at a time; lattices of one shape share their neighbour
+    and staple tables).  A step is one sweep of every member; the tempering
+    swaps (every 10 sweeps, a few hundred energy comparisons) are left out.
+    Returns (site updates/ns, threads, members, variables, seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle
+    import plaquette_b200 as plq
+    from plaquette_b200.ensemble import batched_workload_spec
+
+    descs, starts, _ = batched_workload_spec()
+    lattices, members = {}, []
+    for d, start in zip(descs, starts):
+        shape = tuple(int(d.shape[i]) for i in range(d.d))
+        gauge = d.model == plq.GAUGE
+        if (shape, gauge) not in lattices:
+            lattices[(shape, gauge)] = oracle.Lattice(shape, staples=gauge)
+        model = oracle.Model.gauge(d.j) if gauge else oracle.Model.ising(d.j, d.h)
+        kernel = oracle.HEATBATH if d.updater == plq.HEATBATH else oracle.METROPOLIS
+        members.append((model, lattices[(shape, gauge)], start.copy(), kernel, d.beta, oracle.fold_seed(d.seed)))
+    n_vars = sum(len(m[2]) for m in members)
+    threads = _host_threads()
+    # largest members first, so the pool ends evenly
+    order = sorted(range(len(members)), key=lambda i: -len(members[i][2]))
+
+    def one(i, k):
+        model, lat, cfg, kernel, beta, s32 = members[i]
+        oracle.keyed_local_sweep(model, lat, cfg, kernel, beta, s32, k)
+
+    with ThreadPoolExecutor(threads) as ex:
+        for k in range(warmup):
+            list(ex.map(lambda i: one(i, k), order))
+        t0 = time.perf_counter()
+        for k in range(warmup, warmup + steps):
+            list(ex.map(lambda i: one(i, k), order))
+        dt = time.perf_counter() - t0
+    return n_vars * steps / dt / 1e9, threads, len(members), n_vars, dt
+
+
+def run_reference_ensemble(args):
+    """The reference arm of the batched ensemble (ensemble_cpu_sample)."""
+    world = _env_int("WORLD_SIZE", 1)
+    if _env_int("RANK", 0) != 0:
+        return
+    value, threads, n_members, n_vars, dt = ensemble_cpu_sample(args.steps, args.warmup)
+    unit = "site updates/ns"
+    line = {
+        "metric": unit, "value": round(value, 6), "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "the batched-ensemble members (64 4D Z2 gauge lattices + 256 3D Ising replicas), "
+                               "one keyed sweep each per step", "name": ENSEMBLE_WORKLOAD,
+                   "members": n_members, "variables": n_vars,
+                   "step": "one sweep of every member (tempering swaps left out)"},
+        "cpu_baseline": {"value": round(value, 6), "unit": unit, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} sweeps of all {n_members} members on {threads} threads"},
+        "e2e": {"value": round(value, 6), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_cluster(args):
     """The reference arm of a cluster workload: the oracle's cluster move on
     one host thread, `steps` sweeps or updates after `warmup` untimed ones."""
@@ -690,10 +760,7 @@ def main():
     if args.impl == "reference" and args.workload in CLUSTER_WORKLOADS:
         run_reference_cluster(args)
     elif args.impl == "reference" and args.workload == ENSEMBLE_WORKLOAD:
-        if _env_int("RANK", 0) == 0:
-            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble (one chain "
-                                                                  "at a time on the CPU); time a single-lattice "
-                                                                  "workload for the reference arm"}), flush=True)
+        run_reference_ensemble(args)
     elif args.impl == "reference":
         run_reference(args)
     elif args.workload == ENSEMBLE_WORKLOAD:

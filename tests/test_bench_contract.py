@@ -1,7 +1,8 @@
 """bench.py's reference arm runs on the host cores alone, so its JSON line is
 checked here: the keys the benchmark contract asks for, a CPU baseline that
 describes the run, an end-to-end figure with no host-device copies, and the
-cluster workloads timed on one thread (the reference is sequential)."""
+cluster workloads timed on one thread (the reference is sequential), the
+ensemble's members spread over the host threads."""
 import json
 import os
 import subprocess
@@ -47,6 +48,7 @@ def test_reference_arm_cluster_workloads(workload, steps, unit):
     assert d["config"]["name"] == workload
 
 
-def test_reference_arm_ensemble_is_unavailable():
-    d = _line("--impl", "reference", "--workload", "ensemble-config4", "--steps", "3", "--warmup", "3")
-    assert d["impl"] == "reference" and d["unavailable"]
+def test_reference_arm_ensemble():
+    d = _line("--impl", "reference", "--workload", "ensemble-config4", "--steps", "2", "--warmup", "1")
+    _common(d, 2, 1, "site updates/ns")
+    assert d["config"]["members"] == 320 and d["config"]["variables"] == 48615936
