@@ -40,7 +40,8 @@ def test_reference_arm_default_workload():
 
 
 @pytest.mark.parametrize("workload,steps,unit", [("wolff-128-keyed", 3, "cluster updates/s"),
-                                                 ("sw-4096-stream", 1, "SW sweeps/s")])
+                                                 ("sw-4096-stream", 1, "SW sweeps/s"),
+                                                 ("sw-4096-keyed", 1, "SW sweeps/s")])
 def test_reference_arm_cluster_workloads(workload, steps, unit):
     d = _line("--impl", "reference", "--workload", workload, "--steps", str(steps), "--warmup", "1")
     _common(d, steps, 1, unit)
