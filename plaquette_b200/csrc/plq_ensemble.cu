@@ -1133,7 +1133,7 @@ void job_release(ServerJob *j) {
 }
 
 // Allocate and upload a job's resident state (worker thread, device current).
-int job_admit(plq_server *S, ServerJob *j, cudaStream_t stream) {
+int job_admit(ServerJob *j, cudaStream_t stream) {
     const plq_chain_desc &d = j->desc;
     EnsMember &mem = j->mem;
     std::memset(&mem, 0, sizeof mem);
@@ -1463,7 +1463,7 @@ void worker_loop(plq_server *S) {
             }
         }
         for (ServerJob *j : admit) {
-            int rc = job_admit(S, j, stream);
+            int rc = job_admit(j, stream);
             std::lock_guard<std::mutex> lock(S->mu);
             if (rc != PLQ_OK) {
                 S->used -= j->footprint;
