@@ -468,25 +468,30 @@ __global__ void __launch_bounds__(kThreads) boundary_hook_kernel(ClusterArgs a) 
     const int T0 = tile_extent(L0), T1 = D >= 2 ? tile_extent(L1) : 1;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (T0 < L0) {  // sites with x = k*T0 + T0-1: n / T0 of them
-        for (int64_t c = t0; c < n / T0; c += stride) {
-            const int64_t s = c * T0 + (T0 - 1);
-            if (!(a.bonds[s] & 1u)) continue;
-            int32_t x[D];
-            site_coords<D>(a.g, s, x);
-            unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, 0), a.cap, a.ctrl);
+    // the two families in one index space, so a thread makes at most one union of them:
+    // candidates c < nx are sites with x = k*T0 + T0-1 (n / T0 of them), the rest the sites of
+    // rows with y = k*T1 + T1-1 (n / T1)
+    const int64_t nx = T0 < L0 ? n / T0 : 0;
+    const int64_t ny = D >= 2 && T1 < L1 ? n / T1 : 0;
+    const int64_t per_row = L0;
+    for (int64_t c = t0; c < nx + ny; c += stride) {
+        int64_t s;
+        int mu;
+        if (c < nx) {
+            s = c * T0 + (T0 - 1);
+            mu = 0;
+        } else {
+            const int64_t cy = c - nx;
+            const int64_t row = fdiv((uint32_t)cy, a.g.dm[0], a.g.dl[0]);  // index among the selected rows
+            s = (row * T1 + (T1 - 1)) * per_row + (cy - row * per_row);
+            mu = 1;
         }
-    }
-    if (D >= 2 && T1 < L1) {  // rows with y = k*T1 + T1-1: n / T1 sites
-        const int64_t per_row = L0;
-        for (int64_t c = t0; c < n / T1; c += stride) {
-            const int64_t row = fdiv((uint32_t)c, a.g.dm[0], a.g.dl[0]);  // index among the selected rows
-            const int64_t s = (row * T1 + (T1 - 1)) * per_row + (c - row * per_row);
-            if (!(a.bonds[s] & 2u)) continue;
-            int32_t x[D];
-            site_coords<D>(a.g, s, x);
-            unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, 1), a.cap, a.ctrl);
-        }
+        if (!((a.bonds[s] >> mu) & 1u)) continue;
+        int32_t x[D];
+        site_coords<D>(a.g, s, x);
+        // compile-time directions keep the coordinates in registers
+        const int64_t nb = mu == 0 ? nbr_plus(a.g, s, x, 0) : nbr_plus(a.g, s, x, D >= 2 ? 1 : 0);
+        unite(a.parent, (int32_t)s, (int32_t)nb, a.cap, a.ctrl);
     }
     if (D >= 3) {
         for (int64_t s = t0; s < n; s += stride) {
