@@ -1,13 +1,21 @@
 """Throughput benchmark of the lattice Monte Carlo hot path on B200.
 
-Default workload (one GPU): 3D q=3 Potts, 512^3 periodic, u8 states drawn
-uniformly from the seed exactly as the reference's hot start does (RandRng +
-Configuration::hot), beta = 0.5505, checkerboard heat bath on the reference
-CPU stream (PCG64) -- bit-exact with the reference's CPU path.  One step =
-one sweep of the lattice (134,217,728 site updates).  Under torchrun each rank
-runs its own lattice (independent replicas, weak scaling; no collective on the
-data path).  `--workload` selects the other 512^3 single-lattice cases (3D
-Ising Metropolis on the keyed or the PCG stream, q=3 Potts heat bath keyed).
+Default workload (one GPU): the batched ensemble -- 64 4D Z2 gauge lattices
+(L 8/12/16/24 x 16, beta 0.40-0.48, link heat bath) beside 256 3D Ising
+replicas in five parallel-tempering ladders (L 16-64, beta 0.20-0.24,
+Metropolis, swaps every 10 sweeps), keyed stream, in one persistent
+graph-captured launch per step, timed against the same sweeps with one
+launch per lattice per colour pass.  One step = one tempering interval (10
+sweeps of every member); the L2 cache is flushed between steps (the 49 MB
+ensemble would otherwise stay resident).  The same run measures, as nested
+records, the other configurations: 3D q=3 Potts 512^3 heat bath and 3D Ising
+512^3 Metropolis (single-lattice HBM roofline), Swendsen-Wang 4096^2 over 500
+sweeps, Wolff 128^3 over 10^5 single-cluster updates, and the serving loop at
+the full job mix.  `--workload` runs one of them alone as the line.
+
+Under torchrun each rank runs its own copy of the workload (independent
+replicas, weak scaling; no collective on the data path; times are the max
+over ranks).  `--gpus N` without torchrun launches N ranks itself.
 
 Prints one JSON line (rank 0).  ``--impl reference`` times the reference's
 CPU algorithm (the C restatement in oracle/) on bounded samples of the same
@@ -176,28 +184,55 @@ def _desc(plq, w, seed, offset):
                          sweeps_between=1, batch=plq.GPU_BATCH)
 
 
-def run_product(args):
-    import numpy as np
+class Ctx:
+    """One rank's view of the job: rank numbers, the process group (None at
+    N=1), its device and the library's context on it."""
+
+    def __init__(self):
+        import torch
+
+        import plaquette_b200 as plq
+
+        self.world, self.rank, self.local, self.pg = dist_setup()
+        torch.cuda.set_device(self.local)
+        self.gpu = plq.Gpu.new(self.local)
+        if self.gpu is None:
+            raise RuntimeError("no CUDA device")
+
+    def close(self):
+        if self.pg is not None:
+            self.pg.destroy_process_group()
+
+
+def traffic_record(name):
+    """roofline.traffic from the committed ncu summary of this kernel (not
+    measured in this run), with its source named."""
+    prof = profiled_traffic().get(name, {})
+    if not prof:
+        return None, None
+    return prof.get("dram_bytes_per_launch"), (f"copied from {prof.get('summary')} (one ncu capture of this "
+                                                f"kernel, {prof.get('captured', 'date in the summary')}); "
+                                                "not measured in this run")
+
+
+def measure_local(name, steps, warmup, ctx, e2e=True):
+    """One 512^3 single-lattice workload: K sweeps timed with CUDA events on
+    the chain's stream (inputs larger than L2), then, if asked, the same
+    sweeps end to end through the public API."""
     import torch
 
     import plaquette_b200 as plq
     from plaquette_b200 import observables as obs
 
-    w = WORKLOADS[args.workload]
-    world, rank, local, pg = dist_setup()
-    torch.cuda.set_device(local)
-    gpu = plq.Gpu.new(local)
-    if gpu is None:
-        raise RuntimeError("no CUDA device")
-    seed = SEED + rank
-    q = w[1]
-    start, offset = plq.hot_start(seed, q, N_SITES)
+    w = WORKLOADS[name]
+    world, local, pg, gpu = ctx.world, ctx.local, ctx.pg, ctx.gpu
+    seed = SEED + ctx.rank
+    start, offset = plq.hot_start(seed, w[1], N_SITES)
 
-    # ---- device-resident throughput: K sweeps timed with CUDA events on the chain's stream
     desc = _desc(plq, w, seed, offset)
     chain = plq.GpuChain(gpu, desc, start)
     stream = torch.cuda.ExternalStream(chain.cuda_stream, device=f"cuda:{local}")
-    chain.advance(args.warmup)
+    chain.advance(warmup)
     chain.sync()
     clocks = ClockSampler(local)
     clocks.start()
@@ -207,7 +242,7 @@ def run_product(args):
     launches0 = chain.launches
     t_wall0 = time.time()
     ev0.record(stream)
-    chain.advance(args.steps)
+    chain.advance(steps)
     ev1.record(stream)
     ev1.synchronize()
     t_wall1 = time.time()
@@ -215,26 +250,44 @@ def run_product(args):
     dev_ms = ev0.elapsed_time(ev1)
     clock_info = clocks.stop(t_wall0, t_wall1)
     chain.sync()
+    path = chain.path
+    chain.close()
     dev_ms_max = max_over_ranks(pg, dev_ms, local)
     barrier(pg, local)
 
-    sites_total = N_SITES * world * args.steps
-    value = whole_job_rate(world, N_SITES, args.steps, dev_ms_max)
-    ms_per_step = dev_ms_max / args.steps
+    sites_total = N_SITES * world * steps
+    value = whole_job_rate(world, N_SITES, steps, dev_ms_max)
     per_launch_ms = dev_ms / max(1, launches)
     alg_bytes = BYTES_PER_UPDATE * N_SITES // w[7]  # per launch
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    prof = profiled_traffic().get(args.workload, {})
+    traffic, traffic_src = traffic_record(name)
+    line = {
+        "metric": "site updates/ns", "value": round(value, 3), "unit": "site updates/ns", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": round(dev_ms_max / steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": w[5], "name": name, "sites_per_gpu": N_SITES, "step": "one sweep",
+                   "l2": "inputs larger than L2 (134 MB state per lattice, two buffers for the out-of-place sweep)",
+                   "parallelism": f"independent lattice per GPU x{world}", "path": path},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes, "kernel": w[6],
+                     "note": "instruction-issue bound: the reference's per-site RNG (a 128-bit LCG step or "
+                             "two 32-bit hashes per draw) costs more issue slots than HBM allows at 2 B/update"},
+        "gpu_launches": launches,
+        "clocks": clock_info,
+    }
+    if not e2e:
+        return line
 
-    # ---- end to end through the public API: pinned host start in, samples and final state out
+    # end to end through the public API: pinned host start in, samples and final state out
     pinned = torch.empty(N_SITES, dtype=torch.uint8).pin_memory()
     pinned.numpy()[:] = start
     out_pinned = torch.empty(N_SITES, dtype=torch.uint8).pin_memory()
     barrier(pg, local)
     t0 = time.perf_counter()
     echain = plq.GpuChain(gpu, desc, pinned.numpy())
-    _, prims = echain.next_batch(args.steps, states=False)
+    _, prims = echain.next_batch(steps, states=False)
     plq.check(plq.lib().plq_chain_read(echain._h, out_pinned.data_ptr()))
     # per-sweep energy and order-parameter histograms (1024 bins) from the exact primaries
     model = obs.POTTS if w[0] == "potts" else obs.ISING
@@ -242,49 +295,27 @@ def run_product(args):
     hist_e = obs.histogram(ser["e"], HIST_BINS, -3.0, 3.0)
     hist_m = obs.histogram(ser["m"], HIST_BINS, 0.0, 1.0)
     t1 = time.perf_counter()
-    assert int(hist_e.sum()) == int(hist_m.sum()) == args.steps
+    assert int(hist_e.sum()) == int(hist_m.sum()) == steps
     e2e_s = max_over_ranks(pg, t1 - t0, local)
-    e2e_value = sites_total / (e2e_s * 1e9)
     n_prim = len(prims[0])
     echain.close()
+    line["e2e"] = {"value": round(sites_total / (e2e_s * 1e9), 3), "unit": "site updates/ns",
+                   "h2d_bytes_per_step": N_SITES / steps,
+                   "d2h_bytes_per_step": 8 * n_prim + N_SITES / steps,
+                   "what": "chain create from a pinned host start, K samples of one sweep each with their device "
+                           "primaries read back, per-sweep E/N and order-parameter histograms "
+                           f"({HIST_BINS} bins), final configuration read back"}
+    return line
 
-    line = {
-        "metric": "site updates/ns",
-        "value": round(value, 3),
-        "unit": "site updates/ns",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(ms_per_step, 5),
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "u8",
-        "data": "synthetic",
-        "config": {"workload": w[5], "name": args.workload, "sites_per_gpu": N_SITES, "step": "one sweep",
-                   "l2": "inputs larger than L2 (134 MB state per lattice, two buffers for the out-of-place sweep)",
-                   "parallelism": f"independent lattice per GPU x{world}", "path": chain.path},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": prof.get("dram_bytes_per_launch"),
-                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes, "kernel": w[6],
-                     "note": "instruction-issue bound: the reference's per-site RNG (a 128-bit LCG step or "
-                             "two 32-bit hashes per draw) costs more issue slots than HBM allows at 2 B/update"},
-        "e2e": {"value": round(e2e_value, 3), "unit": "site updates/ns",
-                "h2d_bytes_per_step": N_SITES / args.steps,
-                "d2h_bytes_per_step": 8 * n_prim + N_SITES / args.steps,
-                "what": "chain create from a pinned host start, K samples of one sweep each with their device "
-                        "primaries read back, per-sweep E/N and order-parameter histograms "
-                        f"({HIST_BINS} bins), final configuration read back"},
-        "gpu_launches": launches,
-        "clocks": clock_info,
-    }
-    if rank == 0 and args.cpu_baseline:
+
+def run_product(args):
+    ctx = Ctx()
+    line = measure_local(args.workload, args.steps, args.warmup, ctx)
+    if ctx.rank == 0 and args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_seconds)
-    if rank == 0:
+    if ctx.rank == 0:
         print(json.dumps(line), flush=True)
-    chain.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    ctx.close()
 
 
 def _oracle_setup(name):
@@ -390,112 +421,195 @@ def run_reference(args):
 
 
 ENSEMBLE_WORKLOAD = "ensemble-config4"
+PT_EVERY = 10           # tempering interval: one bench step
+L2_FLUSH_BYTES = 256 << 20  # written between timed steps: twice the 126 MB L2
 
 
-def run_ensemble(args):
-    """The batched ensemble (64 4D gauge lattices + 256 3D Ising replicas in
-    five tempering ladders): one persistent graph-captured launch per advance,
-    timed against the same sweeps with one launch per lattice per colour pass."""
+def timed_steps(stream, fn, steps, sweeps_per_step, flush):
+    """`steps` calls of fn(sweeps_per_step), each bracketed by CUDA events on
+    `stream`, with an L2 flush (a 256 MB write on the same stream) before
+    each, outside the events.  Returns the summed device milliseconds."""
+    import torch
+
+    pairs = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(sweeps_per_step)
+        e1.record(stream)
+        pairs.append((e0, e1))
+    pairs[-1][1].synchronize()
+    return sum(e0.elapsed_time(e1) for e0, e1 in pairs)
+
+
+def measure_ensemble(steps, warmup, ctx):
+    """The batched ensemble: one persistent graph-captured launch per step
+    (10 sweeps of every member, one tempering phase), timed against the same
+    sweeps with one launch per lattice per colour pass."""
     import numpy as np
     import torch
 
     import plaquette_b200 as plq
     from plaquette_b200.ensemble import batched_workload_spec, build_ensemble
 
-    world, rank, local, pg = dist_setup()
-    torch.cuda.set_device(local)
-    gpu = plq.Gpu.new(local)
-    if gpu is None:
-        raise RuntimeError("no CUDA device")
-    seed = SEED + rank
+    world, local, pg, gpu = ctx.world, ctx.local, ctx.pg, ctx.gpu
+    seed = SEED + ctx.rank
     descs, starts, ladders = batched_workload_spec(seed)
     n_vars = int(sum(len(x) for x in starts))
-    ens = build_ensemble(gpu, descs, starts, ladders, seed)
+    ens = build_ensemble(gpu, descs, starts, ladders, seed, pt_every=PT_EVERY)
     stream = torch.cuda.ExternalStream(ens.cuda_stream, device=f"cuda:{local}")
-    ens.advance(args.warmup)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(warmup):
+        ens.advance(PT_EVERY)
     ens.sync()
-
-    def timed(fn, sweeps):
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        fn(sweeps)
-        ev1.record(stream)
-        ev1.synchronize()
-        return ev0.elapsed_time(ev1)
 
     clocks = ClockSampler(local)
     clocks.start()
     barrier(pg, local)
     launches0 = ens.launches
     t_wall0 = time.time()
-    batched_ms = timed(ens.advance, args.steps)
+    batched_ms = timed_steps(stream, ens.advance, steps, PT_EVERY, flush)
     t_wall1 = time.time()
     launches = ens.launches - launches0
     clock_info = clocks.stop(t_wall0, t_wall1)
-    k_unb = min(args.steps, 50)
-    unbatched_ms = timed(ens.advance_unbatched, k_unb)
+    k_unb = min(steps, 5)
+    unbatched_ms = timed_steps(stream, ens.advance_unbatched, k_unb, PT_EVERY, flush)
     batched_ms_max = max_over_ranks(pg, batched_ms, local)
     unbatched_ms_max = max_over_ranks(pg, unbatched_ms, local)
 
     # identical observables: a second ensemble from the same seeds, every sweep per-lattice
-    ref = build_ensemble(gpu, descs, starts, ladders, seed)
-    ref.advance_unbatched(args.warmup + args.steps + k_unb)
-    same = all(np.array_equal(ens.primaries(m), ref.primaries(m)) for m in range(ens.n)) and \
+    ref = build_ensemble(gpu, descs, starts, ladders, seed, pt_every=PT_EVERY)
+    ref.advance_unbatched((warmup + steps + k_unb) * PT_EVERY)
+    same = all(np.array_equal(a, b) for a, b in zip(ens.primaries_all(), ref.primaries_all())) and \
         np.array_equal(ens.betas(), ref.betas())
     ref.close()
+    ens.close()
 
-    # end to end through the public API: host starts in, every member's primaries out
+    # end to end through the public API: starts from pinned host memory in; after every step
+    # every member's primaries and beta out
+    pinned = torch.empty(n_vars, dtype=torch.uint8).pin_memory()
+    views, off = [], 0
+    for st in starts:
+        v = pinned.numpy()[off:off + len(st)]
+        v[:] = st
+        views.append(v)
+        off += len(st)
     barrier(pg, local)
     t0 = time.perf_counter()
-    e2 = build_ensemble(gpu, descs, starts, ladders, seed)
-    e2.advance(args.steps)
-    prims = [e2.primaries(m) for m in range(e2.n)]
+    e2 = build_ensemble(gpu, descs, views, ladders, seed, pt_every=PT_EVERY)
+    n_prim = 0
+    for _ in range(steps):
+        e2.advance(PT_EVERY)
+        prims = e2.primaries_all()
+        betas = e2.betas()
+        n_prim = sum(len(p) for p in prims)
     t1 = time.perf_counter()
+    assert len(betas) == e2.n
     e2.close()
     e2e_s = max_over_ranks(pg, t1 - t0, local)
 
-    value = n_vars * world * args.steps / (batched_ms_max * 1e-3) / 1e9
-    unb_value = n_vars * world * k_unb / (unbatched_ms_max * 1e-3) / 1e9
-    alg_bytes = BYTES_PER_UPDATE * n_vars  # per ensemble sweep
-    achieved = alg_bytes * args.steps / (batched_ms * 1e-3) / 1e9
+    updates = n_vars * world * steps * PT_EVERY
+    value = updates / (batched_ms_max * 1e-3) / 1e9
+    unb_value = n_vars * world * k_unb * PT_EVERY / (unbatched_ms_max * 1e-3) / 1e9
+    alg_bytes = BYTES_PER_UPDATE * n_vars * PT_EVERY  # per launch (one step)
+    achieved = alg_bytes * steps / (batched_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    line = {
+    traffic, traffic_src = traffic_record(ENSEMBLE_WORKLOAD)
+    return {
         "metric": "site updates/ns", "value": round(value, 3), "unit": "site updates/ns", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(batched_ms_max / args.steps, 5),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "steps": steps, "warmup": warmup, "ms_per_step": round(batched_ms_max / steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": "64 4D Z2 gauge lattices (L 8/12/16/24 x 16, beta 0.40-0.48, link heat bath) + "
                                "256 3D Ising replicas (L 16-64, five ladders, beta 0.20-0.24 geometric, "
                                "Metropolis, tempering swaps every 10 sweeps), keyed stream, hot starts",
-                   "name": ENSEMBLE_WORKLOAD, "members": ens.n, "variables": n_vars,
-                   "step": "one ensemble sweep (every member one sweep)",
-                   "l2": "the whole ensemble (49 MB) fits in L2; no flush between sweeps",
+                   "name": ENSEMBLE_WORKLOAD, "members": len(descs), "variables": n_vars,
+                   "step": f"one tempering interval: {PT_EVERY} sweeps of every member and one swap phase, one "
+                           "graph-captured persistent launch",
+                   "l2": "L2 flushed between timed steps (a 256 MB write outside the timed events); the 49 MB "
+                         "ensemble is L2-resident within a step",
                    "parallelism": f"independent ensemble per GPU x{world}"},
-        "per_lattice_launches": {"value": round(unb_value, 3), "sweeps": k_unb,
-                                 "ms_per_step": round(unbatched_ms_max / k_unb, 5)},
+        "per_lattice_launches": {"value": round(unb_value, 3), "steps": k_unb,
+                                 "ms_per_step": round(unbatched_ms_max / k_unb, 5),
+                                 "what": "the same sweeps and swaps with one launch per lattice per colour pass"},
         "batched_over_per_lattice": round(value / unb_value, 2),
         "identical_observables": bool(same),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": alg_bytes * args.steps, "kernel": "ensemble_kernel",
-                     "note": "one launch runs all timed sweeps; the ensemble is L2-resident"},
-        "e2e": {"value": round(n_vars * world * args.steps / (e2e_s * 1e9), 3), "unit": "site updates/ns",
-                "h2d_bytes_per_step": n_vars / args.steps,
-                "d2h_bytes_per_step": 8 * sum(len(p) for p in prims) / args.steps,
-                "what": "ensemble create from host starts, K sweeps, every member's primaries read back"},
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes,
+                     "kernel": "ensemble_kernel",
+                     "note": "2 B per variable update; the ensemble (49 MB) is read from HBM once per step and "
+                             "then served from L2"},
+        "e2e": {"value": round(updates / (e2e_s * 1e9), 3), "unit": "site updates/ns",
+                "h2d_bytes_per_step": n_vars / steps,
+                "d2h_bytes_per_step": 8 * n_prim + 8 * len(descs),
+                "what": "ensemble create from pinned host starts, then K steps each followed by every member's "
+                        "primaries and beta read back"},
         "gpu_launches": launches,
         "clocks": clock_info,
     }
-    if rank == 0 and args.cpu_baseline:
+
+
+def measure_serving(rate, n_jobs, ctx):
+    """The serving loop at one Poisson arrival rate over the full job mix
+    (100-5000 sweeps per job)."""
+    from plaquette_b200.serving import run_poisson
+
+    barrier(ctx.pg, ctx.local)
+    r = run_poisson(ctx.gpu, rate, n_jobs, seed=int(rate) + 7 * ctx.rank, sweeps_scale=1.0)
+    p99 = max_over_ranks(ctx.pg, r["p99_ms"], ctx.local)
+    return {"metric": "job p99 ms", "value": round(p99, 2), "unit": "ms", "higher_is_better": False,
+            "p50_ms": round(r["p50_ms"], 2), "mean_ms": round(r["mean_ms"], 2),
+            "rate_jobs_per_s": rate, "jobs": n_jobs,
+            "site_updates_per_ns_busy": round(r["site_updates_per_ns_busy"], 2), "ticks": r["ticks"],
+            "wall_s": round(r["wall_s"], 2),
+            "config": {"workload": "Poisson arrivals of mixed jobs: 50% 2D/3D Ising Metropolis (2D L 32-1024, "
+                                   "3D L 16-256), 30% 3D Potts q=3/4 heat bath, 20% 4D Z2 gauge heat bath (L 8-24), "
+                                   "beta within 2% of the transition, 100-5000 sweeps each (full range), keyed"}}
+
+
+RECORD_WORKLOADS = ("potts3-512-hb-stream", "ising-512-metro-keyed", "ising-512-metro-stream",
+                    "sw-4096-keyed", "sw-4096-stream", "wolff-128-keyed")
+
+
+def _record(line):
+    keep = ("metric", "value", "unit", "ms_per_step", "steps", "higher_is_better", "roofline", "e2e",
+            "size_histogram_log2", "gpu_launches", "clocks")
+    out = {k: line[k] for k in keep if k in line}
+    out["workload"] = line["config"]["workload"]
+    return out
+
+
+def run_ensemble(args):
+    ctx = Ctx()
+    line = measure_ensemble(args.steps, args.warmup, ctx)
+    if args.records:
+        records = {}
+        for name in RECORD_WORKLOADS:
+            try:
+                if name in WORKLOADS:
+                    rec = measure_local(name, args.steps, args.warmup, ctx, e2e=(name == "potts3-512-hb-stream"))
+                else:
+                    steps, _ = CLUSTER_RECORD_STEPS[name]
+                    rec = measure_cluster(name, steps, 3, ctx, e2e=False)
+                records[name] = _record(rec)
+            except Exception as exc:  # one failing record must not hide the others
+                records[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        try:
+            records["serving-10-jobs-per-s"] = measure_serving(10.0, 60, ctx)
+        except Exception as exc:
+            records["serving-10-jobs-per-s"] = {"error": f"{type(exc).__name__}: {exc}"}
+        line["records"] = records
+    if ctx.rank == 0 and args.cpu_baseline:
         cv, threads, n_members, _, dt_c = ensemble_cpu_sample(steps=6, warmup=1)
         line["cpu_baseline"] = {"value": round(cv, 6), "unit": "site updates/ns", "cores": threads, "kind": "port",
                                 "sample": f"6 sweeps of all {n_members} members on {threads} threads "
                                           f"({dt_c:.1f} s; tempering swaps left out)"}
-    if rank == 0:
+    if ctx.rank == 0:
         print(json.dumps(line), flush=True)
-    ens.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    ctx.close()
 
 
 CLUSTER_WORKLOADS = {
@@ -512,7 +626,11 @@ CLUSTER_WORKLOADS = {
 }
 
 
-def run_cluster(args):
+# record steps: (steps, units per step) -- SW over the configuration's 500 sweeps, Wolff over 10^5 updates
+CLUSTER_RECORD_STEPS = {"sw-4096-keyed": (500, 1), "sw-4096-stream": (500, 1), "wolff-128-keyed": (100, 1000)}
+
+
+def measure_cluster(name, steps, warmup, ctx, e2e=True):
     """Cluster moves: Swendsen-Wang sweeps/s (labels, size histogram each
     sweep available) or Wolff single-cluster updates/s."""
     import numpy as np
@@ -520,13 +638,9 @@ def run_cluster(args):
 
     import plaquette_b200 as plq
 
-    extent, rng_name, shape, beta, what = CLUSTER_WORKLOADS[args.workload]
-    world, rank, local, pg = dist_setup()
-    torch.cuda.set_device(local)
-    gpu = plq.Gpu.new(local)
-    if gpu is None:
-        raise RuntimeError("no CUDA device")
-    seed = SEED + rank
+    extent, rng_name, shape, beta, what = CLUSTER_WORKLOADS[name]
+    world, local, pg, gpu = ctx.world, ctx.local, ctx.pg, ctx.gpu
+    seed = SEED + ctx.rank
     n = int(np.prod(shape))
     start, offset = plq.hot_start(seed, 2, n)
     rng = plq.RNG_STREAM if rng_name == "stream" else plq.RNG_KEYED
@@ -535,14 +649,14 @@ def run_cluster(args):
     wolff = extent == "seeded"
     per_step = 1000 if wolff else 1  # Wolff: one step = 1000 single-cluster updates
 
-    def make():
+    def make(st):
         d = plq.make_desc(plq.ISING, 2, shape, plq.CLUSTER, beta=beta, seed=seed, rng=rng, stream_offset=offset,
                           sweeps_between=per_step, batch=1, extent=ext, relabel=relabel)
-        return plq.GpuClusterChain(gpu, d, start)
+        return plq.GpuClusterChain(gpu, d, st)
 
-    chain = make()
+    chain = make(start)
     stream = torch.cuda.ExternalStream(chain.cuda_stream, device=f"cuda:{local}")
-    chain.advance(args.warmup * per_step)
+    chain.advance(warmup * per_step)
     chain.sync()
     clocks = ClockSampler(local)
     clocks.start()
@@ -552,7 +666,7 @@ def run_cluster(args):
     launches0 = chain.launches
     t_wall0 = time.time()
     ev0.record(stream)
-    chain.advance(args.steps * per_step)
+    chain.advance(steps * per_step)
     ev1.record(stream)
     ev1.synchronize()
     t_wall1 = time.time()
@@ -560,10 +674,37 @@ def run_cluster(args):
     launches = chain.launches - launches0
     clock_info = clocks.stop(t_wall0, t_wall1)
     dev_ms = max_over_ranks(pg, ev0.elapsed_time(ev1), local)
-    units = args.steps * per_step * world
+    units = steps * per_step * world
     value = units / (dev_ms * 1e-3)
     hist = chain.size_histogram(32)
     chain.close()
+    unit = "cluster updates/s" if wolff else "SW sweeps/s"
+    alg = 10.5 * n if not wolff else None  # SW: spins r+w, bond bits r+w, labels w+r (bytes per sweep)
+    peak, peak_kind = measured_peak_hbm()
+    line = {
+        "metric": unit, "value": round(value, 2), "unit": unit, "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": round(dev_ms / steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": what, "name": name, "sites": n,
+                   "step": "1000 single-cluster updates" if wolff else "one Swendsen-Wang sweep",
+                   "l2": "state, bonds and labels (16.8 M sites: 101 MB) stream through L2 every sweep" if not wolff
+                   else "cluster work only; the 2.1 MB lattice stays in L2",
+                   "parallelism": f"independent lattice per GPU x{world}"},
+        "roofline": ({"bound": "hbm", "achieved": round(alg * steps / (dev_ms * 1e-3) / 1e9, 1),
+                      "peak": peak, "unit": "GB/s",
+                      "frac": round(alg * steps / (dev_ms * 1e-3) / 1e9 / peak, 4),
+                      "traffic": None, "peak_source": peak_kind,
+                      "algorithmic_bytes_per_launch": alg,
+                      "kernel": "bonds + tile union-find + boundary unions + relabel",
+                      "note": "10.5 B/site per sweep algorithmic minimum"} if not wolff else
+                     {"bound": "latency", "achieved": None, "peak": None, "unit": None, "frac": None,
+                      "traffic": None, "note": "frontier BFS: work proportional to the cluster, not the lattice"}),
+        "size_histogram_log2": [int(x) for x in hist[:24]],
+        "gpu_launches": launches,
+        "clocks": clock_info,
+    }
+    if not e2e:
+        return line
 
     # end to end: chain from a pinned host start, K steps, size histogram and final configuration back
     pinned = torch.empty(n, dtype=torch.uint8).pin_memory()
@@ -571,51 +712,30 @@ def run_cluster(args):
     out_pinned = torch.empty(n, dtype=torch.uint8).pin_memory()
     barrier(pg, local)
     t0 = time.perf_counter()
-    d = plq.make_desc(plq.ISING, 2, shape, plq.CLUSTER, beta=beta, seed=seed, rng=rng, stream_offset=offset,
-                      sweeps_between=per_step, batch=1, extent=ext, relabel=relabel)
-    ec = plq.GpuClusterChain(gpu, d, pinned.numpy())
-    ec.advance(args.steps * per_step)
-    h2 = ec.size_histogram(32)
+    ec = make(pinned.numpy())
+    ec.advance(steps * per_step)
+    ec.size_histogram(32)
     plq.check(plq.lib().plq_chain_read(ec._h, out_pinned.data_ptr()))
     t1 = time.perf_counter()
     ec.close()
     e2e_s = max_over_ranks(pg, t1 - t0, local)
-    unit = "cluster updates/s" if wolff else "SW sweeps/s"
-    alg = 10.5 * n if not wolff else None  # SW: spins r+w, bond bits r+w, labels w+r (bytes per sweep)
-    line = {
-        "metric": unit, "value": round(value, 2), "unit": unit, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": what, "name": args.workload, "sites": n,
-                   "step": "1000 single-cluster updates" if wolff else "one Swendsen-Wang sweep",
-                   "l2": "state, bonds and labels (16.8 M sites: 101 MB) stream through L2 every sweep" if not wolff
-                   else "cluster work only; the 2.1 MB lattice stays in L2",
-                   "parallelism": f"independent lattice per GPU x{world}"},
-        "roofline": ({"bound": "hbm", "achieved": round(alg * args.steps / (dev_ms * 1e-3) / 1e9, 1),
-                      "peak": measured_peak_hbm()[0], "unit": "GB/s",
-                      "frac": round(alg * args.steps / (dev_ms * 1e-3) / 1e9 / measured_peak_hbm()[0], 4),
-                      "traffic": None, "peak_source": measured_peak_hbm()[1],
-                      "algorithmic_bytes_per_launch": alg,
-                      "kernel": "bonds + tile union-find + boundary unions + relabel",
-                      "note": "10.5 B/site per sweep algorithmic minimum"} if not wolff else
-                     {"bound": "latency", "achieved": None, "peak": None, "unit": None, "frac": None,
-                      "traffic": None, "note": "frontier BFS: work proportional to the cluster, not the lattice"}),
-        "size_histogram_log2": [int(x) for x in hist[:24]],
-        "e2e": {"value": round(units / e2e_s, 2), "unit": unit, "h2d_bytes_per_step": n / args.steps,
-                "d2h_bytes_per_step": (n + 8 * 32) / args.steps,
-                "what": "chain create from a pinned host start, K steps, cluster-size histogram and final "
-                        "configuration read back"},
-        "gpu_launches": launches,
-        "clocks": clock_info,
-    }
-    if rank == 0 and args.cpu_baseline:
+    line["e2e"] = {"value": round(units / e2e_s, 2), "unit": unit, "h2d_bytes_per_step": n / steps,
+                   "d2h_bytes_per_step": (n + 8 * 32) / steps,
+                   "what": "chain create from a pinned host start, K steps, cluster-size histogram and final "
+                           "configuration read back"}
+    return line
+
+
+def run_cluster(args):
+    ctx = Ctx()
+    line = measure_cluster(args.workload, args.steps, args.warmup, ctx)
+    if ctx.rank == 0 and args.cpu_baseline:
         units_c, dt_c, sample = cluster_cpu_sample(args.workload, args.cpu_seconds)
-        line["cpu_baseline"] = {"value": round(units_c / dt_c, 4), "unit": unit, "cores": 1, "kind": "port",
-                                "sample": sample}
-    if rank == 0:
+        line["cpu_baseline"] = {"value": round(units_c / dt_c, 4), "unit": line["unit"], "cores": 1,
+                                "kind": "port", "sample": sample}
+    if ctx.rank == 0:
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    ctx.close()
 
 
 def cluster_cpu_sample(name: str, seconds: float, warmup: int = 0, max_units: int = 1 << 30):
@@ -744,17 +864,34 @@ def run_reference_cluster(args):
     print(json.dumps(line), flush=True)
 
 
+def spawn_ranks(n: int) -> int:
+    """`bench.py --gpus N` outside torchrun: relaunch this command as N ranks
+    on this node (127.0.0.1 rendezvous) and return their exit status."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
-    ap.add_argument("--workload", default="potts3-512-hb-stream",
-                    choices=sorted(WORKLOADS) + [ENSEMBLE_WORKLOAD] + sorted(CLUSTER_WORKLOADS))
+    ap.add_argument("--workload", default=ENSEMBLE_WORKLOAD,
+                    choices=[ENSEMBLE_WORKLOAD] + sorted(WORKLOADS) + sorted(CLUSTER_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-records", dest="records", action="store_false",
+                    help="ensemble workload: skip the nested records of the other configurations")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     if args.warmup < 3 and args.impl == "product":
         args.warmup = 3
     if args.impl == "reference" and args.workload in CLUSTER_WORKLOADS:

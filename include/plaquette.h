@@ -93,6 +93,11 @@ typedef struct plq_chain_desc {
     uint64_t stream_offset;     /* stream: next_u64 draws already consumed (e.g. the hot start) */
     int64_t sweeps_between;     /* sweeps per `next` (device.rs:590-701) */
     int64_t batch;              /* samples per device round-trip (GPU_BATCH, device.rs:501) */
+    uint64_t sweep_offset;      /* sweeps already run: the keyed stream's sweep counter (the RNG key
+                                   `sweeps_done`, device.rs:216-217) starts here, so a keyed chain
+                                   re-created from a read-back configuration with sweep_offset = its
+                                   sweeps so far continues bit-identically; counted in
+                                   plq_chain_sweeps_done on both streams.  Normally 0. */
 } plq_chain_desc;
 
 /* ------------------------------------------------------- library */
@@ -165,6 +170,7 @@ int plq_chain_wilson(plq_chain *chain, int32_t max_side, int64_t *totals, int64_
 int plq_chain_sync(plq_chain *chain);
 /* Device status word: PLQ_OK, or PLQ_ECAP / PLQ_EDEVICE after a fault. */
 int plq_chain_status(plq_chain *chain);
+/* Sweeps run so far, sweep_offset included (the keyed stream's next sweep key). */
 uint64_t plq_chain_sweeps_done(plq_chain *chain);
 /* Stream mode: next_u64 draws consumed so far (stream_offset included). */
 int plq_chain_stream_position(plq_chain *chain, uint64_t *out);
@@ -193,7 +199,8 @@ void plq_chain_destroy(plq_chain *chain);
  * chains -- any mix of models, dimensions <= 4, uneven shapes, betas and
  * seeds, local updaters on the keyed stream or heat bath on the PCG stream --
  * advanced together.  Member m evolves exactly as plq_chain_create(desc[m],
- * starts[m]) would; starts may be NULL (all members cold) or hold NULLs. */
+ * starts[m]) would; starts may be NULL (all members cold) or hold NULLs.
+ * Members share one sweep counter, so their sweep_offset must be equal. */
 typedef struct plq_ensemble plq_ensemble;
 int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc *members, const uint8_t *const *starts,
                         plq_ensemble **out);
@@ -218,6 +225,10 @@ int plq_ensemble_tune(plq_ensemble *e, int32_t trial_sweeps, int32_t *ranks_out,
 int plq_ensemble_sync(plq_ensemble *e);
 int plq_ensemble_read(plq_ensemble *e, int32_t member, uint8_t *out_states);
 int plq_ensemble_primaries(plq_ensemble *e, int32_t member, int64_t *out, int32_t *n_out);
+/* Every member's primaries at once (one replayed launch sequence and one
+ * copy): member m's int64 primaries, as plq_chain_primaries, at
+ * out[m * stride ...]; counts[m] (may be NULL) receives how many. */
+int plq_ensemble_primaries_all(plq_ensemble *e, int64_t *out, int32_t stride, int32_t *counts);
 /* Current beta of every member (parallel tempering moves them). */
 int plq_ensemble_betas(plq_ensemble *e, double *beta_of_member);
 int64_t plq_ensemble_n_vars(plq_ensemble *e);
@@ -270,7 +281,12 @@ void plq_server_destroy(plq_server *s);
  * that overlap on the GPU race and must not be issued.  The first call on a
  * device looks up the array's device address.  Runs on `cuda_stream` (NULL =
  * the default stream) and returns after it drained; *stream_position_out (may
- * be NULL) receives stream_offset plus the draws consumed. */
+ * be NULL) receives stream_offset plus the draws consumed.  The array keeps
+ * the jump table of the last seed and the decision table of the last
+ * couplings used on that device: a call with another seed or other couplings
+ * copies those tables (about 64 KiB) from pageable host memory, which waits
+ * for the work already queued on `cuda_stream`; a repeated call with the same
+ * seed and couplings copies nothing. */
 #define PLQ_NOALLOC_MAX_SITES 134217728
 int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int64_t *shape, double j, double h,
                                  double beta, uint64_t seed, uint64_t stream_offset, uint64_t sweeps,

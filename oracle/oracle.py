@@ -138,6 +138,11 @@ def lib():
         L.orc_polyakov_sum.restype = C.c_int64
         L.orc_wilson_totals.argtypes = [P(_Lattice), u8p, C.c_int32, i64p, i64p]
         L.orc_wilson_totals.restype = C.c_int32
+        L.orc_pt_exp.argtypes = [C.c_double]
+        L.orc_pt_exp.restype = C.c_double
+        L.orc_pt_swap_phase.argtypes = [C.c_int32, P(C.c_int32), P(C.c_double), i64p, P(C.c_double), C.c_uint32,
+                                        C.c_uint64]
+        L.orc_pt_swap_phase.restype = C.c_int32
     return _lib
 
 
@@ -378,3 +383,19 @@ def wilson_totals(lat: Lattice, cfg: np.ndarray, max_side: int) -> tuple[np.ndar
     got = lib().orc_wilson_totals(C.byref(lat.lat), _u8(cfg), max_side, _i64(totals), _i64(placements))
     assert got == mx
     return totals.reshape(mx + 1, mx + 1), int(placements[0])
+
+
+def pt_exp(x: float) -> float:
+    """The tempering decision's e^x (x <= 0) from basic operations only."""
+    return lib().orc_pt_exp(x)
+
+
+def pt_swap_phase(member_of_slot: np.ndarray, beta_of_member: np.ndarray, energy: np.ndarray,
+                  j_of_member: np.ndarray, seed32: int, att: int) -> int:
+    """One swap phase of one ladder (attempt `att`), in place on the int32
+    slot table and the float64 betas; returns the swaps accepted."""
+    assert member_of_slot.dtype == np.int32 and beta_of_member.dtype == np.float64
+    assert energy.dtype == np.int64 and j_of_member.dtype == np.float64
+    return lib().orc_pt_swap_phase(len(member_of_slot), member_of_slot.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   beta_of_member.ctypes.data_as(C.POINTER(C.c_double)), _i64(energy),
+                                   j_of_member.ctypes.data_as(C.POINTER(C.c_double)), seed32 & 0xFFFFFFFF, att)

@@ -923,3 +923,60 @@ int32_t orc_wilson_totals(const orc_lattice *lat, const uint8_t *cfg, int32_t ma
     *placements = (int64_t)d * (d - 1) * lat->n_sites;
     return mx;
 }
+
+/* ================================================== parallel tempering */
+
+/* ln2 = PT_LN2_HI + PT_LN2_LO, PT_LN2_HI with 32 significant bits (so n * PT_LN2_HI
+ * is exact for |n| < 2^21); 1/k! rounded to double. */
+#define PT_INV_LN2 1.4426950408889634
+#define PT_LN2_HI 0.6931471803691238
+#define PT_LN2_LO 1.9082149292705877e-10
+
+double orc_pt_exp(double x) {
+    static const double inv_fact[15] = {
+        1.0, 1.0, 0.5, 0.16666666666666666, 0.041666666666666664, 0.008333333333333333,
+        0.001388888888888889, 0.0001984126984126984, 2.48015873015873e-05, 2.7557319223985893e-06,
+        2.755731922398589e-07, 2.505210838544172e-08, 2.08767569878681e-09, 1.6059043836821613e-10,
+        1.1470745597729725e-11};
+    if (!(x > -708.0)) return 0.0;
+    double t = x * PT_INV_LN2;
+    double n = floor(t + 0.5);
+    double hi = n * PT_LN2_HI;
+    double lo = n * PT_LN2_LO;
+    double r = (x - hi) - lo;
+    double p = inv_fact[14];
+    for (int k = 13; k >= 0; --k) p = p * r + inv_fact[k];
+    uint64_t bits = (uint64_t)((int64_t)n + 1023) << 52;
+    double scale;
+    memcpy(&scale, &bits, sizeof scale);
+    return p * scale;
+}
+
+static uint32_t keyed24(uint32_t seed, uint32_t variable, uint32_t sweep) {
+    uint32_t k = orc_lowbias32(seed ^ variable);
+    k = orc_lowbias32(k ^ (sweep * 0x9e3779b9u));
+    return k >> 8;
+}
+
+int32_t orc_pt_swap_phase(int32_t k_slots, int32_t *member_of_slot, double *beta_of_member,
+                          const int64_t *energy, const double *j_of_member, uint32_t seed32, uint64_t att) {
+    int32_t accepted = 0;
+    for (int32_t k = (int32_t)(att & 1u); k + 1 < k_slots; k += 2) {
+        int32_t m1 = member_of_slot[k], m2 = member_of_slot[k + 1];
+        double b1 = beta_of_member[m1], b2 = beta_of_member[m2];
+        double e1 = -(j_of_member[m1] * (double)energy[m1]);
+        double e2 = -(j_of_member[m2] * (double)energy[m2]);
+        double delta = (b1 - b2) * (e1 - e2);
+        uint32_t h1 = keyed24(seed32 ^ 0x6a09e667u, (uint32_t)k, (uint32_t)att);
+        uint32_t h2 = keyed24(seed32 ^ 0xbb67ae85u, (uint32_t)k, (uint32_t)att);
+        double u = ((double)h1 + (double)h2 * 5.9604644775390625e-8) * 5.9604644775390625e-8;
+        if (delta >= 0.0 || u < orc_pt_exp(delta)) {
+            beta_of_member[m1] = b2;
+            beta_of_member[m2] = b1;
+            member_of_slot[k] = m2;
+            member_of_slot[k + 1] = m1;
+            ++accepted;
+        }
+    }
+    return accepted;
+}

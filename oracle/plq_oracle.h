@@ -159,6 +159,26 @@ int64_t orc_polyakov_sum(const orc_lattice *lat, const uint8_t *cfg, int32_t dir
 int32_t orc_wilson_totals(const orc_lattice *lat, const uint8_t *cfg, int32_t max_side, int64_t *totals,
                           int64_t *placements);
 
+/* -------------------------------------------------- parallel tempering */
+/* The reference has no tempering; this restates the batched-ensemble swap
+ * rule of this backend so its decisions are checked independently.
+ *
+ * orc_pt_exp: e^x for x <= 0 from IEEE basic operations only, each rounded
+ * on its own: x = n ln2 + r (n = floor(x/ln2 + 1/2), ln2 split in a 32-bit
+ * high part and a low part after Cody and Waite), e^r by its Taylor
+ * polynomial to degree 14 in Horner form, times 2^n; 0 below x = -708. */
+double orc_pt_exp(double x);
+/* One swap phase of one ladder, attempt `att`: for slots k = att & 1,
+ * att & 1 + 2, ... with k + 1 < k_slots, members m1 = slot[k] and
+ * m2 = slot[k + 1] at betas b1, b2 with energies E = -J * energy (the bond,
+ * agreement or plaquette sum; no field) exchange betas and slots when
+ * delta = (b1 - b2)(E1 - E2) >= 0 or u < orc_pt_exp(delta), where
+ * u = (h1 + h2 2^-24) 2^-24 with h1, h2 the 24-bit keyed hashes of
+ * (seed32 ^ 0x6a09e667, k, att) and (seed32 ^ 0xbb67ae85, k, att).
+ * Returns the number of accepted swaps. */
+int32_t orc_pt_swap_phase(int32_t k_slots, int32_t *member_of_slot, double *beta_of_member,
+                          const int64_t *energy, const double *j_of_member, uint32_t seed32, uint64_t att);
+
 #ifdef __cplusplus
 }
 #endif

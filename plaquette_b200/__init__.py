@@ -77,6 +77,7 @@ class ChainDesc(C.Structure):
         ("stream_offset", C.c_uint64),
         ("sweeps_between", C.c_int64),
         ("batch", C.c_int64),
+        ("sweep_offset", C.c_uint64),
     ]
 
 
@@ -216,7 +217,7 @@ class Gpu:
 
 def make_desc(model, q, shape, updater, *, beta, j=1.0, h=0.0, offsets=None, seed=0, rng=RNG_STREAM,
               stream_offset=0, sweeps_between=1, batch=GPU_BATCH, extent=EXTENT_ALL,
-              relabel=RELABEL_REDRAW, flags=0) -> ChainDesc:
+              relabel=RELABEL_REDRAW, flags=0, sweep_offset=0) -> ChainDesc:
     d = ChainDesc()
     d.model = model
     d.q = q
@@ -238,6 +239,7 @@ def make_desc(model, q, shape, updater, *, beta, j=1.0, h=0.0, offsets=None, see
     d.sweeps_between = sweeps_between
     d.batch = batch
     d.flags = flags
+    d.sweep_offset = sweep_offset
     return d
 
 

@@ -300,6 +300,7 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
     c->ctx_copy = *ctx;
     c->ctx = &c->ctx_copy;
     c->desc = *desc;
+    c->sweeps_done = desc->sweep_offset;  // the keyed stream's sweep key resumes here
     c->q = desc->model == PLQ_POTTS ? desc->q : 2;
     c->d = desc->d;
     c->link = desc->model == PLQ_GAUGE;

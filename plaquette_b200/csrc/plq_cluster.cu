@@ -887,6 +887,14 @@ ClusterArgs cluster_args(plq_chain *c) {
     return a;
 }
 
+// The range of the per-cluster label draw: next_below(q) to redraw
+// (src/updater.rs:512), propose's next_below(q - 1) for the forced change
+// (:515, :659-668; a range of 1 at q = 2, which consumes nothing).
+bool label_range_is_power_of_two(const plq_chain *c) {
+    const uint32_t range = c->desc.relabel == PLQ_RELABEL_FORCED ? (uint32_t)c->q - 1u : (uint32_t)c->q;
+    return (range & (range - 1u)) == 0u;
+}
+
 template <int D>
 int sweep_d(plq_chain *c, uint64_t sweeps) {
     ClusterDev *cd = static_cast<ClusterDev *>(c->cl);
@@ -923,6 +931,16 @@ int sweep_d(plq_chain *c, uint64_t sweeps) {
         if (!stream) {
             relabel_keyed_kernel<<<gs, kThreads, 0, c->stream>>>(a);
             c->launches++;
+        } else if (label_range_is_power_of_two(c)) {
+            // rand's range sampler never takes a second draw for a power-of-two range
+            // (x * 2^k leaves its low word a multiple of 2^k, never inside the rejection
+            // zone above 2^32 - 2^k): the labels drawn by the rank pass are final and the
+            // sweep needs no round-trip to the host
+            lookback(a);
+            root_rank_kernel<D><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
+            apply_fresh_kernel<<<gs, kThreads, 0, c->stream>>>(a);
+            finish_pos_kernel<<<1, 1, 0, c->stream>>>(c->d_ctrl, 0);
+            c->launches += 3;
         } else {
             lookback(a);
             const int none = 0x7FFFFFFF;

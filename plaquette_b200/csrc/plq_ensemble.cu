@@ -287,7 +287,41 @@ __device__ void energy_phase(const EnsArgs &e) {
     }
 }
 
+// e^x for x <= 0 from IEEE basic operations only, each rounded on its own
+// (explicit _rn intrinsics: no contraction into fused multiply-adds), so the
+// tempering decision is a pure function a host restates bit for bit.
+// x = n ln2 + r with n = floor(x/ln2 + 1/2) and ln2 split after Cody and
+// Waite into a 32-significant-bit high part (n * high is exact) and a low
+// part; e^r (|r| <= 0.347) by its Taylor polynomial to degree 14 in Horner
+// form (truncation below 2^-60 relative); then times 2^n.  Below x = -708 the
+// result is 0 (2^n would leave the normal range).
+__device__ double pt_exp(double x) {
+    if (!(x > -708.0)) return 0.0;
+    const double n = floor(__dadd_rn(__dmul_rn(x, 1.4426950408889634), 0.5));
+    const double r = __dsub_rn(__dsub_rn(x, __dmul_rn(n, 0.6931471803691238)), __dmul_rn(n, 1.9082149292705877e-10));
+    double p = 1.1470745597729725e-11;  // 1/14!
+    p = __dadd_rn(__dmul_rn(p, r), 1.6059043836821613e-10);
+    p = __dadd_rn(__dmul_rn(p, r), 2.08767569878681e-09);
+    p = __dadd_rn(__dmul_rn(p, r), 2.505210838544172e-08);
+    p = __dadd_rn(__dmul_rn(p, r), 2.755731922398589e-07);
+    p = __dadd_rn(__dmul_rn(p, r), 2.7557319223985893e-06);
+    p = __dadd_rn(__dmul_rn(p, r), 2.48015873015873e-05);
+    p = __dadd_rn(__dmul_rn(p, r), 0.0001984126984126984);
+    p = __dadd_rn(__dmul_rn(p, r), 0.001388888888888889);
+    p = __dadd_rn(__dmul_rn(p, r), 0.008333333333333333);
+    p = __dadd_rn(__dmul_rn(p, r), 0.041666666666666664);
+    p = __dadd_rn(__dmul_rn(p, r), 0.16666666666666666);
+    p = __dadd_rn(__dmul_rn(p, r), 0.5);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0);
+    p = __dadd_rn(__dmul_rn(p, r), 1.0);
+    return __dmul_rn(p, __longlong_as_double((long long)(n + 1023.0) << 52));
+}
+
 // Swap attempts of every ladder (one thread per pair); attempt index `att`.
+// Energies E = -J * (bond, agreement or plaquette sum); the pair at slots
+// (k, k+1) exchanges betas when (b_k - b_k+1)(E_k - E_k+1) >= 0 or a keyed
+// uniform u < e^((b_k - b_k+1)(E_k - E_k+1)); even pairs on even attempts,
+// odd pairs on odd ones.
 __device__ void swap_phase(const EnsArgs &e, unsigned long long att) {
     for (int l = 0; l < e.n_ladders; ++l) {
         const LadderDev &L = e.ladders[l];
@@ -295,13 +329,14 @@ __device__ void swap_phase(const EnsArgs &e, unsigned long long att) {
         for (int k = parity + 2 * (int)threadIdx.x; k + 1 < L.k; k += 2 * (int)blockDim.x) {
             int m1 = L.member_of_slot[k], m2 = L.member_of_slot[k + 1];
             double b1 = e.tsets[e.ts_of_member[m1]].beta, b2 = e.tsets[e.ts_of_member[m2]].beta;
-            double E1 = -e.members[m1].j * (double)e.energy[m1];
-            double E2 = -e.members[m2].j * (double)e.energy[m2];
-            double delta = (b1 - b2) * (E1 - E2);
+            double E1 = -__dmul_rn(e.members[m1].j, (double)e.energy[m1]);
+            double E2 = -__dmul_rn(e.members[m2].j, (double)e.energy[m2]);
+            double delta = __dmul_rn(__dsub_rn(b1, b2), __dsub_rn(E1, E2));
             uint32_t h1 = keyed24(L.seed32 ^ 0x6a09e667u, (uint32_t)k, (uint32_t)att);
             uint32_t h2 = keyed24(L.seed32 ^ 0xbb67ae85u, (uint32_t)k, (uint32_t)att);
-            double u = ((double)h1 + (double)h2 * 5.9604644775390625e-8) * 5.9604644775390625e-8;
-            if (delta >= 0.0 || u < exp(delta)) {
+            double u = __dmul_rn(__dadd_rn((double)h1, __dmul_rn((double)h2, 5.9604644775390625e-8)),
+                                 5.9604644775390625e-8);
+            if (delta >= 0.0 || u < pt_exp(delta)) {
                 int32_t t1 = e.ts_of_member[m1];
                 e.ts_of_member[m1] = e.ts_of_member[m2];
                 e.ts_of_member[m2] = t1;
@@ -413,6 +448,10 @@ struct plq_ensemble {
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_sweeps = 0;
     int graph_ranks = 0, graph_ctas = 0;
+    // every member's primaries: one device buffer, the launches captured once
+    long long *d_prims_all = nullptr;
+    std::vector<int64_t> prims_offset;  // member m's first entry
+    cudaGraphExec_t prims_graph = nullptr;
 };
 
 namespace {
@@ -554,6 +593,8 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         if (d.rng == PLQ_RNG_STREAM && d.updater == PLQ_METROPOLIS)
             return plq_fail(PLQ_EUNSUPPORTED,
                             "stream-mode Metropolis needs a device-wide scan per pass; ensembles run it keyed");
+        if (d.sweep_offset != descs[0].sweep_offset)
+            return plq_fail(PLQ_EINVAL, "ensemble members share one sweep counter: every sweep_offset must be equal");
     }
     cudaError_t ce = plq_enter_device(ctx->device);
     if (ce != cudaSuccess) return ens_fail(ce, "cudaSetDevice");
@@ -675,6 +716,8 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
     std::vector<long long> zeros(n, 0);
     LaunchState ls;
     std::memset(&ls, 0, sizeof ls);
+    ls.sweep = descs[0].sweep_offset;  // the keyed sweep key resumes here
+    E->sweeps_done = descs[0].sweep_offset;
     Control ctrl;
     std::memset(&ctrl, 0, sizeof ctrl);
     ce = dev_upload(E, E->members.data(), E->members.size(), &E->d_members);
@@ -938,6 +981,7 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
         cudaStreamSynchronize(E->stream);
     };
     snapshot(true);
+    const uint64_t done0 = E->sweeps_done;
     int best_r = E->ranks, best_c = E->ctas_per_sm;
     double best = 1e300;
     cudaEvent_t t0, t1;
@@ -969,7 +1013,7 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
     cudaEventDestroy(t1);
     snapshot(false);
     cudaFree(backup);
-    E->sweeps_done = 0;
+    E->sweeps_done = done0;
     int rc = plq_ensemble_set_config(E, best_r, best_c);
     if (rc != PLQ_OK) return rc;
     if (ranks_out) *ranks_out = best_r;
@@ -1016,6 +1060,57 @@ extern "C" int plq_ensemble_primaries(plq_ensemble *E, int32_t m, int64_t *out, 
     return ens_status(E);
 }
 
+extern "C" int plq_ensemble_primaries_all(plq_ensemble *E, int64_t *out, int32_t stride, int32_t *counts) {
+    if (!E || !out || stride < 1) return plq_fail(PLQ_EINVAL, "bad arguments");
+    const size_t n = E->members.size();
+    cudaError_t e = plq_enter_device(E->ctx->device);
+    if (e != cudaSuccess) return ens_fail(e, "cudaSetDevice");
+    if (!E->prims_graph) {
+        // one buffer for all members, and every member's measurement launches
+        // captured once (the state buffers never move)
+        E->prims_offset.assign(n + 1, 0);
+        for (size_t m = 0; m < n; ++m)
+            E->prims_offset[m + 1] =
+                E->prims_offset[m] + primaries_count(E->members[m].a.model, E->members[m].a.q);
+        e = cudaMalloc((void **)&E->d_prims_all, sizeof(long long) * (size_t)E->prims_offset[n]);
+        if (e != cudaSuccess) return ens_fail(e, "primaries buffer");
+        E->allocs.push_back(E->d_prims_all);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal);
+        for (size_t m = 0; m < n && e == cudaSuccess; ++m) {
+            const EnsMember &mem = E->members[m];
+            e = launch_primaries(mem.a.state, mem.a.g, mem.a.model, mem.a.q, E->d_prims_all + E->prims_offset[m],
+                                 E->stream);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(E->stream, &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&E->prims_graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            E->prims_graph = nullptr;
+            return ens_fail(e, "primaries graph");
+        }
+    }
+    for (size_t m = 0; m < n; ++m) {
+        const int64_t np = E->prims_offset[m + 1] - E->prims_offset[m];
+        if (np > stride) return plq_fail(PLQ_EINVAL, "stride is below a member's primaries count");
+    }
+    std::vector<long long> host((size_t)E->prims_offset[n]);
+    e = cudaGraphLaunch(E->prims_graph, E->stream);
+    E->launches++;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(host.data(), E->d_prims_all, sizeof(long long) * host.size(), cudaMemcpyDeviceToHost,
+                            E->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
+    if (e != cudaSuccess) return ens_fail(e, "primaries of every member");
+    for (size_t m = 0; m < n; ++m) {
+        const int64_t np = E->prims_offset[m + 1] - E->prims_offset[m];
+        for (int64_t i = 0; i < np; ++i) out[(int64_t)m * stride + i] = host[(size_t)(E->prims_offset[m] + i)];
+        if (counts) counts[m] = (int32_t)np;
+    }
+    return ens_status(E);
+}
+
 extern "C" int plq_ensemble_betas(plq_ensemble *E, double *beta_of_member) {
     if (!E || !beta_of_member) return plq_fail(PLQ_EINVAL, "bad arguments");
     std::vector<int32_t> ts(E->members.size());
@@ -1040,6 +1135,7 @@ extern "C" void plq_ensemble_destroy(plq_ensemble *E) {
     if (E->ctx) plq_enter_device(E->ctx->device);
     if (E->stream) cudaStreamSynchronize(E->stream);
     drop_graph(E);
+    if (E->prims_graph) cudaGraphExecDestroy(E->prims_graph);
     for (void *p : E->allocs) cudaFree(p);
     if (E->stream) cudaStreamDestroy(E->stream);
     delete E;
@@ -1581,6 +1677,7 @@ extern "C" int plq_server_submit(plq_server *S, const plq_chain_desc *desc, cons
                         "stream)");
     ServerJob *j = new ServerJob();
     j->desc = *desc;
+    j->msweep = desc->sweep_offset;  // the job's keyed sweep key resumes here
     j->sweeps = sweeps;
     j->want_states = want_states != 0;
     j->footprint = job_footprint(*desc);

@@ -20,6 +20,15 @@
 // different streams, or from different host threads -- race on it and must
 // not be issued.  The first call on each device takes the array's device
 // address (cudaGetSymbolAddress) with that device current.
+//
+// The host-side tables are built in a per-thread buffer (not on the caller's
+// stack: the jump table is 64 KiB and embedding hosts often run small-stack
+// worker threads).  The library remembers, per device, which seed's jump
+// table and which couplings' decision table the array holds, and copies a
+// table only when it differs: a repeated call with the same seed and
+// couplings enqueues no host-to-device copy.  A copy that does happen comes
+// from pageable memory, so it waits for the work already queued on the
+// caller's stream.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -50,24 +59,46 @@ static_assert(sizeof(Control) <= 256, "control block slot");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
+
+// What the array on one device holds: its device address, and which jump
+// table (by the stream's increment) and decision table (by its parameters)
+// the last successful call left in it.
+struct DeviceScratch {
+    unsigned char *ptr;
+    bool jump_valid;
+    uint64_t inc_lo, inc_hi;
+    bool table_valid;
+    int32_t d;
+    uint64_t j_bits, h_bits, beta_bits;
+};
 std::mutex g_setup_mu;
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
+DeviceScratch g_dev[kMaxDevices] = {};
+
+// The host-side jump table of the calling thread.
+thread_local AffineHost t_jump_host[kJumpDigits * kJumpRadix];
+
+uint64_t bits_of(double x) {
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof b);
+    return b;
+}
 
 // Once per device, with that device current: the array's device address.
-int scratch_for_current_device(unsigned char **out) {
+int scratch_for_current_device(int *dev_out, unsigned char **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return plq_fail(PLQ_ENODEV, "device ordinal above the supported range");
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_dev[dev].ptr) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr)
             return plq_fail(PLQ_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
+        g_dev[dev].ptr = static_cast<unsigned char *>(p);
     }
-    *out = g_scratch_ptr[dev];
+    *dev_out = dev;
+    *out = g_dev[dev].ptr;
     return PLQ_OK;
 }
 
@@ -100,10 +131,12 @@ extern "C" int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int
     // runtime call left on this thread, so the checks below see only our calls
     (void)cudaGetLastError();
     unsigned char *scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
+    int dev = 0;
+    int rc = scratch_for_current_device(&dev, &scratch);
     if (rc != PLQ_OK) return rc;
 
-    // host-side tables, on the stack
+    // host-side tables: the decision table (at most 64 entries) on the stack,
+    // the 64 KiB jump table in this thread's buffer
     ModelParams p;
     std::memset(&p, 0, sizeof p);
     p.model = PLQ_ISING;
@@ -114,7 +147,7 @@ extern "C" int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int
     p.h = h;
     uint64_t metro[kTableEntries];
     if (q2_metro53_into(p, metro, kTableEntries) < 0) return plq_fail(PLQ_EINVAL, "decision table too large");
-    AffineHost jump_host[kJumpDigits * kJumpRadix];  // 64 KiB on the caller's stack
+    AffineHost *jump_host = t_jump_host;
     uint64_t slo, shi, ilo, ihi;
     pcg_seed_from_u64(seed, slo, shi, ilo, ihi);
     jump_table_into(ilo, ihi, jump_host);
@@ -124,9 +157,21 @@ extern "C" int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int
     base = pcg_step(base, inc);
 
     const int64_t n_chunks = local_chunks(n);
-    cudaError_t e;
-    e = cudaMemcpyAsync(scratch, jump_host, kJumpBytes, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess)
+    // copy only the tables the array does not hold already; a table about to
+    // be rewritten counts as absent until this call has succeeded
+    bool need_jump, need_table;
+    const uint64_t jb = bits_of(j), hb = bits_of(h), bb = bits_of(beta);
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        DeviceScratch &r = g_dev[dev];
+        need_jump = !(r.jump_valid && r.inc_lo == ilo && r.inc_hi == ihi);
+        need_table = !(r.table_valid && r.d == d && r.j_bits == jb && r.h_bits == hb && r.beta_bits == bb);
+        if (need_jump) r.jump_valid = false;
+        if (need_table) r.table_valid = false;
+    }
+    cudaError_t e = cudaSuccess;
+    if (need_jump) e = cudaMemcpyAsync(scratch, jump_host, kJumpBytes, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && need_table)
         e = cudaMemcpyAsync(scratch + kTableOffset, metro, sizeof metro, cudaMemcpyHostToDevice, stream);
     // the parts that must start at zero: control block and descriptors
     if (e == cudaSuccess) e = cudaMemsetAsync(scratch + kControlOffset, 0, sizeof(Control), stream);
@@ -172,6 +217,18 @@ extern "C" int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int
     e = cudaMemcpyAsync(&host_ctrl, scratch + kControlOffset, sizeof host_ctrl, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return plq_fail(PLQ_ECUDA, std::string("read-back: ") + cudaGetErrorString(e));
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        DeviceScratch &r = g_dev[dev];
+        r.jump_valid = true;
+        r.inc_lo = ilo;
+        r.inc_hi = ihi;
+        r.table_valid = true;
+        r.d = d;
+        r.j_bits = jb;
+        r.h_bits = hb;
+        r.beta_bits = bb;
+    }
     if (host_ctrl.status)
         return plq_fail(PLQ_EDEVICE, "device status word " + std::to_string(host_ctrl.status));
     if (stream_position_out) *stream_position_out = stream_offset + host_ctrl.pos[passes & 1];

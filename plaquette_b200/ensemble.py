@@ -27,6 +27,7 @@ extra_signatures({
     "plq_ensemble_sync": ([C.c_void_p], C.c_int),
     "plq_ensemble_read": ([C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
     "plq_ensemble_primaries": ([C.c_void_p, C.c_int32, C.c_void_p, _P(C.c_int32)], C.c_int),
+    "plq_ensemble_primaries_all": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
     "plq_ensemble_betas": ([C.c_void_p, C.c_void_p], C.c_int),
     "plq_ensemble_n_vars": ([C.c_void_p], C.c_int64),
     "plq_ensemble_cuda_stream": ([C.c_void_p], C.c_void_p),
@@ -100,6 +101,14 @@ class Ensemble:
         n = C.c_int32()
         check(lib().plq_ensemble_primaries(self._h, m, out.ctypes.data, C.byref(n)))
         return out[: n.value].copy()
+
+    def primaries_all(self) -> list[np.ndarray]:
+        """Every member's primaries in one device round-trip."""
+        stride = 66
+        out = np.zeros((self.n, stride), dtype=np.int64)
+        counts = np.zeros(self.n, dtype=np.int32)
+        check(lib().plq_ensemble_primaries_all(self._h, out.ctypes.data, stride, counts.ctypes.data))
+        return [out[m, : counts[m]].copy() for m in range(self.n)]
 
     def betas(self) -> np.ndarray:
         out = np.empty(self.n, dtype=np.float64)

@@ -107,3 +107,36 @@ def test_no_device_here_is_none_or_context():
     g = plq.Gpu.new()
     if plq.device_count() == 0:
         assert g is None
+
+
+def test_descriptor_layout_matches_the_header(tmp_path):
+    """The ctypes descriptor has the C struct's size and field offsets
+    (gcc on include/plaquette.h)."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    fields = [f[0] for f in plq.ChainDesc._fields_]
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "plaquette.h"', "int main(void) {",
+             '  printf("%zu\\n", sizeof(plq_chain_desc));']
+    lines += [f'  printf("%zu\\n", offsetof(plq_chain_desc, {f}));' for f in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got[0] == C.sizeof(plq.ChainDesc)
+    assert got[1:] == [getattr(plq.ChainDesc, f).offset for f in fields]
+
+
+def test_integration_binding_lists_every_entry_point():
+    """The Rust extern block a maintainer would add names every entry point
+    of the header."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    block = text[text.index('extern "C" {'):]
+    block = block[:block.index("\n}\n")]
+    bound = set(re.findall(r"pub fn (plq_[a-z0-9_]+)\(", block))
+    assert set(declared_symbols()) <= bound, sorted(set(declared_symbols()) - bound)

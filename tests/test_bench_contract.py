@@ -33,10 +33,24 @@ def _common(d, steps, warmup, unit):
     assert d["e2e"] == {"value": d["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
-def test_reference_arm_default_workload():
-    d = _line("--impl", "reference", "--steps", "3", "--warmup", "3")
+def test_reference_arm_default_workload_is_the_ensemble():
+    d = _line("--impl", "reference", "--steps", "1", "--warmup", "1")
+    _common(d, 1, 1, "site updates/ns")
+    assert d["config"]["name"] == "ensemble-config4"
+
+
+def test_reference_arm_single_lattice():
+    d = _line("--impl", "reference", "--workload", "potts3-512-hb-stream", "--steps", "3", "--warmup", "3")
     _common(d, 3, 3, "site updates/ns")
     assert d["config"]["name"] == "potts3-512-hb-stream"
+
+
+def test_gpus_flag_spawns_the_ranks_itself():
+    """`--gpus 2` outside torchrun relaunches itself as two ranks; rank 0
+    alone prints the reference arm's line."""
+    d = _line("--impl", "reference", "--gpus", "2", "--workload", "wolff-128-keyed", "--steps", "2", "--warmup",
+              "1", timeout=600)
+    assert d["n_gpus"] == 2 and d["config"]["name"] == "wolff-128-keyed"
 
 
 @pytest.mark.parametrize("workload,steps,unit", [("wolff-128-keyed", 3, "cluster updates/s"),

@@ -139,3 +139,14 @@ def test_four_site_members_match_their_own_chains(gpu):
         c.advance(6)
     for m, c in enumerate(chains):
         assert np.array_equal(ens.read(m), c.read()), m
+
+
+def test_primaries_of_every_member_at_once(gpu):
+    descs, starts = _members()
+    ens = Ensemble(gpu, descs, starts)
+    for sweeps in (0, 4, 3):
+        ens.advance(sweeps) if sweeps else None
+        every = ens.primaries_all()
+        assert len(every) == ens.n
+        for m in range(ens.n):
+            assert list(every[m]) == list(ens.primaries(m)), (sweeps, m)
