@@ -453,13 +453,19 @@ def measure_ensemble(steps, warmup, ctx):
     import torch
 
     import plaquette_b200 as plq
-    from plaquette_b200.ensemble import batched_workload_spec, build_ensemble
+    from plaquette_b200.ensemble import batched_workload_spec, build_ensemble, tune_entries
 
     world, local, pg, gpu = ctx.world, ctx.local, ctx.pg, ctx.gpu
     seed = SEED + ctx.rank
     descs, starts, ladders = batched_workload_spec(seed)
     n_vars = int(sum(len(x) for x in starts))
     ens = build_ensemble(gpu, descs, starts, ladders, seed, pt_every=PT_EVERY)
+    # the autotuner: a work-item shape per member shape, then the launch shape (state restored after)
+    t_tune = time.perf_counter()
+    tuned_r, tuned_c, tuned_ms = ens.tune(PT_EVERY)
+    tuning = {"launch": {"ranks_per_thread": tuned_r, "ctas_per_sm": tuned_c,
+                         "ms_per_sweep": round(tuned_ms, 5)},
+              "shapes": tune_entries(), "seconds": round(time.perf_counter() - t_tune, 2)}
     stream = torch.cuda.ExternalStream(ens.cuda_stream, device=f"cuda:{local}")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(warmup):
@@ -482,6 +488,7 @@ def measure_ensemble(steps, warmup, ctx):
 
     # identical observables: a second ensemble from the same seeds, every sweep per-lattice
     ref = build_ensemble(gpu, descs, starts, ladders, seed, pt_every=PT_EVERY)
+    ref.set_config(tuned_r, tuned_c)
     ref.advance_unbatched((warmup + steps + k_unb) * PT_EVERY)
     same = all(np.array_equal(a, b) for a, b in zip(ens.primaries_all(), ref.primaries_all())) and \
         np.array_equal(ens.betas(), ref.betas())
@@ -500,6 +507,7 @@ def measure_ensemble(steps, warmup, ctx):
     barrier(pg, local)
     t0 = time.perf_counter()
     e2 = build_ensemble(gpu, descs, views, ladders, seed, pt_every=PT_EVERY)
+    e2.set_config(tuned_r, tuned_c)
     n_prim = 0
     for _ in range(steps):
         e2.advance(PT_EVERY)
@@ -536,6 +544,7 @@ def measure_ensemble(steps, warmup, ctx):
                                  "what": "the same sweeps and swaps with one launch per lattice per colour pass"},
         "batched_over_per_lattice": round(value / unb_value, 2),
         "identical_observables": bool(same),
+        "tuning": tuning,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes,

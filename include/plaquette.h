@@ -216,12 +216,33 @@ int plq_ensemble_advance(plq_ensemble *e, uint64_t sweeps);
 /* The same sweeps with one launch per member per colour pass (the
  * per-lattice baseline); identical results. */
 int plq_ensemble_advance_unbatched(plq_ensemble *e, uint64_t sweeps);
-/* Work-item shape of the persistent launch: ranks per thread (2, 4, 8) and
- * CTAs per SM; the autotuner times the candidates on a snapshot of the
- * ensemble (restored afterwards) and keeps the fastest. */
+/* Launch shape of the persistent kernel: ranks per thread of the generic
+ * pass body (2, 4, 8) and CTAs per SM. */
 int plq_ensemble_set_config(plq_ensemble *e, int32_t ranks_per_thread, int32_t ctas_per_sm);
+/* The autotuner (the reference has one fixed shape, a workgroup of 64,
+ * src/device.rs:96-106).  On a snapshot of the ensemble (restored
+ * afterwards): (1) for every member shape -- (model, q, d, extents,
+ * updater, stream) -- the members of that shape alone at 1, 2, 4 and 8
+ * four-site words per thread, the fastest kept for them and recorded in a
+ * process-wide table that later ensembles and served jobs of that shape
+ * use; (2) the whole ensemble over the generic body's ranks per thread and
+ * CTAs per SM.  Returns the launch shape chosen in (2) and its time per
+ * sweep. */
 int plq_ensemble_tune(plq_ensemble *e, int32_t trial_sweeps, int32_t *ranks_out, int32_t *ctas_out,
                       double *ms_per_sweep_out);
+/* Member m's work-item shape: four-site words per thread (0: the generic body). */
+int plq_ensemble_member_config(plq_ensemble *e, int32_t member, int32_t *words_per_thread);
+/* The process-wide tuning table, one entry per member shape tuned so far;
+ * *n_out = the number of entries (at most `capacity` are written). */
+typedef struct plq_tune_entry {
+    int32_t model, q, d, updater, rng;
+    int32_t words_per_thread;   /* the fastest measured */
+    int64_t shape[4];
+    int32_t members;            /* members of this shape in the tuned ensemble */
+    int32_t pad;
+    double ms_per_sweep;        /* those members alone, at that shape */
+} plq_tune_entry;
+int plq_tune_entries(plq_tune_entry *out, int32_t capacity, int32_t *n_out);
 int plq_ensemble_sync(plq_ensemble *e);
 int plq_ensemble_read(plq_ensemble *e, int32_t member, uint8_t *out_states);
 int plq_ensemble_primaries(plq_ensemble *e, int32_t member, int64_t *out, int32_t *n_out);

@@ -64,7 +64,9 @@ struct EnsMember {
     int link;          // variables on links
     int passes;        // colour passes per sweep
     int64_t n_vars;
-    int64_t chunks[2]; // unused slot kept for alignment
+    int wpt;           // four-site body: words per thread of a work item (the tuned shape)
+    int pad_;
+    int64_t reserved_;
     double j;
     int ladder;
 };
@@ -75,6 +77,41 @@ struct LadderDev {
     uint32_t seed32;
     int32_t *member_of_slot;  // k entries
 };
+
+// The autotuner's table: the work-item shape (four-site words per thread)
+// measured fastest for each member shape -- (model, q, d, extents, updater,
+// stream) -- in this process.  Ensembles and served jobs created later take
+// their members' shapes from it (4 where a shape was never tuned).
+struct ShapeKey {
+    int32_t model, q, d, updater, rng;
+    int32_t L[4];
+    bool operator<(const ShapeKey &o) const { return std::memcmp(this, &o, sizeof *this) < 0; }
+};
+struct TuneEntry {
+    int wpt;
+    double ms_per_sweep;  // the members of this shape alone, at that shape
+    int members;
+};
+std::mutex g_tune_mu;
+std::map<ShapeKey, TuneEntry> g_tuned;
+
+ShapeKey shape_key(const plq_chain_desc &d) {
+    ShapeKey k;
+    std::memset(&k, 0, sizeof k);
+    k.model = d.model;
+    k.q = d.model == PLQ_POTTS ? d.q : 2;
+    k.d = d.d;
+    k.updater = d.updater;
+    k.rng = d.rng;
+    for (int i = 0; i < d.d && i < 4; ++i) k.L[i] = (int32_t)d.shape[i];
+    return k;
+}
+
+int tuned_wpt(const plq_chain_desc &d) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(shape_key(d));
+    return it == g_tuned.end() ? kWordsPerThread : it->second.wpt;
+}
 
 // Device-resident launch state, advanced by the kernel itself so a captured
 // graph replays without new parameters.
@@ -94,6 +131,7 @@ struct EnsArgs {
     unsigned long long *msweep;  // per-member sweep counters (serving), or null: all share ls->sweep
     const int32_t *item_member;
     const int32_t *item_chunk;
+    const int8_t *item_pass;   // colour pass of the item (link members: 2 * direction + parity)
     const int64_t *sp_begin;
     int n_sp;
     const int32_t *e_item_member;
@@ -140,36 +178,36 @@ __device__ void grid_barrier(const EnsArgs &e) {
     __syncthreads();
 }
 
-template <int D, int R>
-__device__ void run_words(const LocalArgs &a, int link, int64_t chunk) {
+template <int D>
+__device__ void run_words(const LocalArgs &a, int link, int64_t chunk, int R) {
     const bool st = a.jump != nullptr;
     if (link) {
         if (D >= 2) {
-            if (st) link_words_chunk<D, true, R>(a, chunk);
-            else link_words_chunk<D, false, R>(a, chunk);
+            if (st) link_words_chunk<D, true>(a, chunk, R);
+            else link_words_chunk<D, false>(a, chunk, R);
         }
     } else if (a.q == 3) {
-        if (st) site_words_chunk<D, 3, true, R>(a, chunk);
-        else site_words_chunk<D, 3, false, R>(a, chunk);
+        if (st) site_words_chunk<D, 3, true>(a, chunk, R);
+        else site_words_chunk<D, 3, false>(a, chunk, R);
     } else if (a.q == 4) {
-        if (st) site_words_chunk<D, 4, true, R>(a, chunk);
-        else site_words_chunk<D, 4, false, R>(a, chunk);
+        if (st) site_words_chunk<D, 4, true>(a, chunk, R);
+        else site_words_chunk<D, 4, false>(a, chunk, R);
     } else {
-        if (st) site_words_chunk<D, 2, true, R>(a, chunk);
-        else site_words_chunk<D, 2, false, R>(a, chunk);
+        if (st) site_words_chunk<D, 2, true>(a, chunk, R);
+        else site_words_chunk<D, 2, false>(a, chunk, R);
     }
 }
 
 // WORDS_ONLY: every member runs four sites at a time, so the generic body is
 // compiled out (far fewer registers, more CTAs per SM).
 template <int R, bool WORDS_ONLY>
-__device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk) {
+__device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk, int wpt) {
     if (WORDS_ONLY || a.words) {
         switch (d) {
-            case 1: run_words<1, R>(a, link, chunk); break;
-            case 2: run_words<2, R>(a, link, chunk); break;
-            case 3: run_words<3, R>(a, link, chunk); break;
-            case 4: run_words<4, R>(a, link, chunk); break;
+            case 1: run_words<1>(a, link, chunk, wpt); break;
+            case 2: run_words<2>(a, link, chunk, wpt); break;
+            case 3: run_words<3>(a, link, chunk, wpt); break;
+            case 4: run_words<4>(a, link, chunk, wpt); break;
             default: break;
         }
         return;
@@ -194,7 +232,7 @@ __device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk) {
 }
 
 // The pass-specific fields of member m's arguments (already copied into sa)
-// for super-phase sp of sweep index `sweep`.
+// for colour pass `sp` of sweep index `sweep`.
 __device__ void item_pass_fields(const EnsArgs &e, int m, int sp, unsigned long long sweep_in_launch, LocalArgs &sa) {
     const EnsMember &mem = e.members[m];
     const TableSet &ts = e.tsets[e.ts_of_member[m]];
@@ -354,8 +392,14 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
     for (unsigned long long t = 0; t < e.sweeps; ++t) {
         for (int sp = 0; sp < e.n_sp; ++sp) {
-            int last_m = -1;  // the arguments in shared memory (same member, same pass: reuse them)
-            for (int64_t i = e.sp_begin[sp] + blockIdx.x; i < e.sp_begin[sp + 1]; i += gridDim.x) {
+            // a contiguous block of the super-phase's items per CTA: neighbouring items
+            // mostly share a member, so its arguments stay in shared memory
+            const int64_t b0 = e.sp_begin[sp], b1 = e.sp_begin[sp + 1];
+            const int64_t per = (b1 - b0 + gridDim.x - 1) / gridDim.x;
+            const int64_t lo = b0 + (int64_t)blockIdx.x * per;
+            const int64_t hi = lo + per < b1 ? lo + per : b1;
+            int last_m = -1;  // the arguments in shared memory (a member has one pass per super-phase)
+            for (int64_t i = lo; i < hi; ++i) {
                 int m = e.item_member[i];
                 if (m != last_m) {
                     // the member's arguments into shared memory, one 32-bit word per thread, then
@@ -365,11 +409,11 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
                     uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
                     for (int k = threadIdx.x; k < (int)(sizeof(LocalArgs) / 4); k += blockDim.x) dst[k] = src[k];
                     __syncthreads();
-                    if (threadIdx.x == 0) item_pass_fields(e, m, sp, t, sa);
+                    if (threadIdx.x == 0) item_pass_fields(e, m, e.item_pass[i], t, sa);
                     __syncthreads();
                     last_m = m;
                 }
-                run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i]);
+                run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i], e.members[m].wpt);
             }
             grid_barrier(e);
         }
@@ -437,6 +481,7 @@ struct plq_ensemble {
     int ctas_per_sm = 2;
     bool words_only = false;  // every member runs four sites at a time
     int32_t *d_item_member = nullptr, *d_item_chunk = nullptr;
+    int8_t *d_item_pass = nullptr;
     int64_t *d_sp_begin = nullptr;
     int n_sp = 0;
     int32_t *d_e_member = nullptr, *d_e_chunk = nullptr;
@@ -476,27 +521,52 @@ void drop_graph(plq_ensemble *E) {
     E->graph = nullptr;
 }
 
-int build_items(plq_ensemble *E) {
-    std::vector<int32_t> im, ic;
-    std::vector<int64_t> spb;
-    int max_passes = 0;
-    for (auto &m : E->members) max_passes = std::max(max_passes, m.passes);
-    const int64_t chunk = (int64_t)kEnsThreads * E->ranks;
-    for (int sp = 0; sp < max_passes; ++sp) {
+// Work items of one sweep of members `ids`, by super-phase; member indices
+// are relative to lo, and super-phase bounds are appended to spb (the last
+// one too).  With S super-phases (the most colour passes of any member),
+// pass p of a member with P passes runs in super-phases [p S / P,
+// (p + 1) S / P), its chunks split evenly over them: a site lattice's two
+// colours each spread over half the super-phases, a 4D gauge lattice's eight
+// passes one per super-phase, so every super-phase holds a similar share of
+// the sweep and each pass still ends (at a grid barrier) before the member's
+// next pass begins.  A member's items hold 256 * wpt four-site words (256 *
+// ranks colour ranks in the generic body).  Returns S.
+int append_items(const EnsMember *mems, const std::vector<size_t> &ids, size_t lo, int ranks,
+                 std::vector<int32_t> &im, std::vector<int32_t> &ic, std::vector<int8_t> &ip,
+                 std::vector<int64_t> &spb) {
+    int S = 0;
+    for (size_t m : ids) S = std::max(S, mems[m].passes);
+    for (int sp = 0; sp < S; ++sp) {
         spb.push_back((int64_t)im.size());
-        for (size_t m = 0; m < E->members.size(); ++m) {
-            if (sp >= E->members[m].passes) continue;
-            const LocalArgs &ma = E->members[m].a;
-            // work per item: 256 * ranks colour ranks, or 256 * ranks four-site words
+        for (size_t m : ids) {
+            const int P = mems[m].passes;
+            const LocalArgs &ma = mems[m].a;
+            const int64_t chunk = (int64_t)kEnsThreads * (ma.words ? mems[m].wpt : ranks);
             const int64_t units = ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2;
-            int64_t nc = (units + chunk - 1) / chunk;
-            for (int64_t c = 0; c < nc; ++c) {
-                im.push_back((int32_t)m);
-                ic.push_back((int32_t)c);
+            const int64_t nc = (units + chunk - 1) / chunk;
+            for (int p = 0; p < P; ++p) {
+                const int p0 = p * S / P, p1 = (p + 1) * S / P;
+                if (sp < p0 || sp >= p1) continue;
+                const int64_t c0 = (int64_t)(sp - p0) * nc / (p1 - p0), c1 = (int64_t)(sp - p0 + 1) * nc / (p1 - p0);
+                for (int64_t c = c0; c < c1; ++c) {
+                    im.push_back((int32_t)(m - lo));
+                    ic.push_back((int32_t)c);
+                    ip.push_back((int8_t)p);
+                }
             }
         }
     }
     spb.push_back((int64_t)im.size());
+    return S;
+}
+
+int build_items(plq_ensemble *E) {
+    std::vector<int32_t> im, ic;
+    std::vector<int8_t> ip;
+    std::vector<int64_t> spb;
+    std::vector<size_t> all(E->members.size());
+    for (size_t m = 0; m < all.size(); ++m) all[m] = m;
+    const int max_passes = append_items(E->members.data(), all, 0, E->ranks, im, ic, ip, spb);
     std::vector<int32_t> em, ec;
     for (auto &l : E->ladders)
         for (int32_t m : l) {
@@ -506,7 +576,7 @@ int build_items(plq_ensemble *E) {
                 ec.push_back((int32_t)c);
             }
         }
-    void *old[] = {E->d_item_member, E->d_item_chunk, E->d_sp_begin, E->d_e_member, E->d_e_chunk};
+    void *old[] = {E->d_item_member, E->d_item_chunk, E->d_item_pass, E->d_sp_begin, E->d_e_member, E->d_e_chunk};
     for (void *p : old)
         if (p) {
             cudaFree(p);
@@ -514,6 +584,7 @@ int build_items(plq_ensemble *E) {
         }
     cudaError_t e = dev_upload(E, im.data(), im.size(), &E->d_item_member);
     if (e == cudaSuccess) e = dev_upload(E, ic.data(), ic.size(), &E->d_item_chunk);
+    if (e == cudaSuccess) e = dev_upload(E, ip.data(), ip.size(), &E->d_item_pass);
     if (e == cudaSuccess) e = dev_upload(E, spb.data(), spb.size(), &E->d_sp_begin);
     if (e == cudaSuccess) e = dev_upload(E, em.data(), em.size(), &E->d_e_member);
     if (e == cudaSuccess) e = dev_upload(E, ec.data(), ec.size(), &E->d_e_chunk);
@@ -535,6 +606,7 @@ EnsArgs ens_args(plq_ensemble *E, uint64_t sweeps) {
     a.pos = E->d_pos;
     a.item_member = E->d_item_member;
     a.item_chunk = E->d_item_chunk;
+    a.item_pass = E->d_item_pass;
     a.sp_begin = E->d_sp_begin;
     a.n_sp = E->n_sp;
     a.e_item_member = E->d_e_member;
@@ -639,6 +711,7 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         a.seed32 = plq_fold_seed(d.seed);
         a.words = !(d.flags & PLQ_FLAG_GENERIC_PASS) &&
                   words_eligible(d.model, q, d.d, a.g.L, d.updater, d.rng) ? 1 : 0;
+        mem.wpt = tuned_wpt(d);
         // state (links: direction planes)
         uint8_t *st = nullptr;
         ce = cudaMalloc((void **)&st, (size_t)mem.n_vars);
@@ -987,9 +1060,97 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
-    for (int r : {2, 4, 8}) {
-        int maxc = max_ctas_per_sm(r, E->words_only);
-        for (int c = 1; c <= std::min(maxc, 4); c *= 2) {
+
+    // 1. per member shape: the members of that shape alone at 1, 2, 4 and 8
+    //    words per thread (one direct cooperative launch of trial_sweeps sweeps
+    //    after a one-sweep warm-up, each from the snapshot); the fastest is kept
+    std::map<ShapeKey, std::vector<size_t>> groups;
+    for (size_t m = 0; m < E->members.size(); ++m)
+        if (E->members[m].a.words) groups[shape_key(E->descs[m])].push_back(m);
+    for (auto &kv : groups) {
+        const std::vector<size_t> &ids = kv.second;
+        int best_w = E->members[ids[0]].wpt;
+        double best_g = 1e300;
+        for (int wpt : {1, 2, 4, 8}) {
+            for (size_t m : ids) E->members[m].wpt = wpt;
+            std::vector<int32_t> im, ic;
+            std::vector<int8_t> ip;
+            std::vector<int64_t> spb;
+            const int n_sp = append_items(E->members.data(), ids, 0, E->ranks, im, ic, ip, spb);
+            int32_t *d_im = nullptr, *d_ic = nullptr;
+            int8_t *d_ip = nullptr;
+            int64_t *d_spb = nullptr;
+            e = cudaMalloc((void **)&d_im, im.size() * sizeof(int32_t));
+            if (e == cudaSuccess) e = cudaMalloc((void **)&d_ic, ic.size() * sizeof(int32_t));
+            if (e == cudaSuccess) e = cudaMalloc((void **)&d_ip, ip.size() * sizeof(int8_t));
+            if (e == cudaSuccess) e = cudaMalloc((void **)&d_spb, spb.size() * sizeof(int64_t));
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(E->d_members, E->members.data(), E->members.size() * sizeof(EnsMember),
+                                    cudaMemcpyHostToDevice, E->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_im, im.data(), im.size() * sizeof(int32_t), cudaMemcpyHostToDevice, E->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_ic, ic.data(), ic.size() * sizeof(int32_t), cudaMemcpyHostToDevice, E->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_ip, ip.data(), ip.size() * sizeof(int8_t), cudaMemcpyHostToDevice, E->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_spb, spb.data(), spb.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                    E->stream);
+            float ms = 0;
+            for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // warm-up, then timed
+                snapshot(false);
+                EnsArgs a = ens_args(E, rep == 0 ? 1 : (uint64_t)trial_sweeps);
+                a.item_member = d_im;
+                a.item_chunk = d_ic;
+                a.item_pass = d_ip;
+                a.sp_begin = d_spb;
+                a.n_sp = n_sp;
+                a.n_ladders = 0;
+                a.pt_every = 0;
+                void *params[] = {&a};
+                dim3 grid((unsigned)(E->ctx->sm_count * E->ctas_per_sm));
+                cudaEventRecord(t0, E->stream);
+                e = cudaLaunchCooperativeKernel(kernel_ptr(E->ranks, E->words_only), grid, dim3(kEnsThreads), params,
+                                                0, E->stream);
+                cudaEventRecord(t1, E->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+                if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
+            }
+            cudaFree(d_im);
+            cudaFree(d_ic);
+            cudaFree(d_ip);
+            cudaFree(d_spb);
+            if (e != cudaSuccess) break;
+            if (ms < best_g) {
+                best_g = ms;
+                best_w = wpt;
+            }
+        }
+        for (size_t m : ids) E->members[m].wpt = best_w;
+        if (e != cudaSuccess) break;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tuned[kv.first] = TuneEntry{best_w, best_g / trial_sweeps, (int)ids.size()};
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(E->d_members, E->members.data(), E->members.size() * sizeof(EnsMember),
+                            cudaMemcpyHostToDevice, E->stream);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        snapshot(false);
+        cudaFree(backup);
+        return ens_fail(e, "tune");
+    }
+
+    // 2. the whole ensemble: ranks per thread of the generic body (none to choose
+    //    when every member runs four sites at a time) and CTAs per SM
+    std::vector<int> rs = E->words_only ? std::vector<int>{E->ranks} : std::vector<int>{2, 4, 8};
+    for (int r : rs) {
+        const int maxc = max_ctas_per_sm(r, E->words_only);
+        std::vector<int> cs;
+        for (int c : {1, 2, 4, maxc})
+            if (c >= 1 && c <= maxc && std::find(cs.begin(), cs.end(), c) == cs.end()) cs.push_back(c);
+        for (int c : cs) {
             if (plq_ensemble_set_config(E, r, c) != PLQ_OK) continue;
             snapshot(false);
             if (plq_ensemble_advance(E, 1) != PLQ_OK) continue;  // warm-up (and graph build)
@@ -1020,6 +1181,37 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
     if (ctas_out) *ctas_out = best_c;
     if (ms_per_sweep_out) *ms_per_sweep_out = best / trial_sweeps;
     return ens_status(E);
+}
+
+extern "C" int plq_ensemble_member_config(plq_ensemble *E, int32_t m, int32_t *words_per_thread) {
+    if (!E || !words_per_thread || m < 0 || m >= (int32_t)E->members.size())
+        return plq_fail(PLQ_EINVAL, "bad arguments");
+    *words_per_thread = E->members[m].a.words ? E->members[m].wpt : 0;
+    return PLQ_OK;
+}
+
+extern "C" int plq_tune_entries(plq_tune_entry *out, int32_t capacity, int32_t *n_out) {
+    if (!n_out || capacity < 0 || (capacity > 0 && !out)) return plq_fail(PLQ_EINVAL, "bad arguments");
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    int32_t n = 0;
+    for (const auto &kv : g_tuned) {
+        if (n < capacity) {
+            plq_tune_entry &t = out[n];
+            std::memset(&t, 0, sizeof t);
+            t.model = kv.first.model;
+            t.q = kv.first.q;
+            t.d = kv.first.d;
+            t.updater = kv.first.updater;
+            t.rng = kv.first.rng;
+            for (int i = 0; i < 4; ++i) t.shape[i] = kv.first.L[i];
+            t.words_per_thread = kv.second.wpt;
+            t.members = kv.second.members;
+            t.ms_per_sweep = kv.second.ms_per_sweep;
+        }
+        ++n;
+    }
+    *n_out = n;
+    return PLQ_OK;
 }
 
 extern "C" int plq_ensemble_sync(plq_ensemble *E) {
@@ -1260,6 +1452,7 @@ int job_admit(ServerJob *j, cudaStream_t stream) {
     a.seed32 = plq_fold_seed(d.seed);
     a.words = !(d.flags & PLQ_FLAG_GENERIC_PASS) &&
               words_eligible(d.model, q, d.d, a.g.L, d.updater, d.rng) ? 1 : 0;
+    mem.wpt = tuned_wpt(d);
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void **p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(p, bytes);
@@ -1346,12 +1539,13 @@ struct TickBuffers {
     int32_t *ts = nullptr;
     unsigned long long *pos = nullptr, *msweep = nullptr;
     int32_t *im = nullptr, *ic = nullptr;
+    int8_t *ip = nullptr;
     int64_t *spb = nullptr;
     LaunchState *ls = nullptr;
     Control *ctrl = nullptr;
     size_t cap_members = 0, cap_items = 0;
     void release() {
-        void *ps[] = {members, tsets, ts, pos, msweep, im, ic, spb, ls, ctrl};
+        void *ps[] = {members, tsets, ts, pos, msweep, im, ic, ip, spb, ls, ctrl};
         for (void *p : ps)
             if (p) cudaFree(p);
         *this = TickBuffers();
@@ -1384,31 +1578,13 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
     // body needs the registers (2 CTAs per SM instead of 1)
     const int ranks_w = 4, ranks_g = 2;
     std::vector<int32_t> im, ic;
+    std::vector<int8_t> ip;
     std::vector<int64_t> spb;
-    // work items of members [lo, hi), member indices relative to lo; returns the super-phase count
-    auto build = [&](size_t lo, size_t hi, int ranks) {
-        const int64_t chunk = (int64_t)kEnsThreads * ranks;
-        int max_passes = 0;
-        for (size_t k = lo; k < hi; ++k) max_passes = std::max(max_passes, mems[k].passes);
-        for (int sp = 0; sp < max_passes; ++sp) {
-            spb.push_back((int64_t)im.size());
-            for (size_t k = lo; k < hi; ++k) {
-                if (sp >= mems[k].passes) continue;
-                const LocalArgs &ma = mems[k].a;
-                const int64_t units = ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2;
-                const int64_t nc = (units + chunk - 1) / chunk;
-                for (int64_t c = 0; c < nc; ++c) {
-                    im.push_back((int32_t)(k - lo));
-                    ic.push_back((int32_t)c);
-                }
-            }
-        }
-        spb.push_back((int64_t)im.size());
-        return max_passes;
-    };
-    const int sp_w = build(0, nw, ranks_w);
+    std::vector<size_t> ids_w, ids_g;
+    for (size_t k = 0; k < n; ++k) (k < nw ? ids_w : ids_g).push_back(k);
+    const int sp_w = nw ? append_items(mems.data(), ids_w, 0, ranks_w, im, ic, ip, spb) : 0;
     const size_t spb_g = spb.size();
-    const int sp_g = build(nw, n, ranks_g);
+    const int sp_g = n > nw ? append_items(mems.data(), ids_g, nw, ranks_g, im, ic, ip, spb) : 0;
     cudaError_t e = cudaSuccess;
     if (!B.ls) {
         e = cudaMalloc((void **)&B.ls, sizeof(LaunchState));
@@ -1433,10 +1609,12 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
     if (e == cudaSuccess && B.cap_items < im.size() + 1) {
         cudaFree(B.im);
         cudaFree(B.ic);
+        cudaFree(B.ip);
         cudaFree(B.spb);
         size_t c = std::max<size_t>(im.size() + 1, 2 * B.cap_items);
         e = cudaMalloc((void **)&B.im, c * sizeof(int32_t));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B.ic, c * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.ip, c * sizeof(int8_t));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B.spb, 64 * sizeof(int64_t));
         B.cap_items = c;
     }
@@ -1450,6 +1628,7 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
     if (!im.empty()) {
         cudaMemcpyAsync(B.im, im.data(), im.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
         cudaMemcpyAsync(B.ic, ic.data(), ic.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
+        cudaMemcpyAsync(B.ip, ip.data(), ip.size() * sizeof(int8_t), cudaMemcpyHostToDevice, stream);
     }
     cudaMemcpyAsync(B.spb, spb.data(), spb.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream);
     // one cooperative launch per member group; item indices in the second group's
@@ -1466,6 +1645,7 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         a.msweep = B.msweep + lo;
         a.item_member = B.im;
         a.item_chunk = B.ic;
+        a.item_pass = B.ip;
         a.sp_begin = B.spb + spb_off;
         a.n_sp = n_sp;
         a.ls = B.ls;

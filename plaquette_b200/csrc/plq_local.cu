@@ -31,9 +31,9 @@ namespace plq {
 template <int D, bool LINK, int Q, bool STREAM>
 __global__ void __launch_bounds__(kWordThreads) word_pass_kernel(LocalArgs a) {
     if (LINK)
-        link_words_chunk<D, STREAM, kWordsPerThread>(a, blockIdx.x);
+        link_words_chunk<D, STREAM>(a, blockIdx.x, kWordsPerThread);
     else
-        site_words_chunk<D, Q, STREAM, kWordsPerThread>(a, blockIdx.x);
+        site_words_chunk<D, Q, STREAM>(a, blockIdx.x, kWordsPerThread);
 }
 
 int64_t word_chunks(int64_t n_sites) {

@@ -130,8 +130,8 @@ __device__ __forceinline__ uint32_t word_update(const LocalArgs &a, uint32_t C, 
 }
 
 // Sites (Ising, Potts q <= 3, Potts q = 4 heat bath): one chunk of a colour pass, R words per thread.
-template <int D, int Q, bool STREAM, int R>
-__device__ __forceinline__ void site_words_chunk(const LocalArgs &a, int64_t chunk) {
+template <int D, int Q, bool STREAM>
+__device__ __forceinline__ void site_words_chunk(const LocalArgs &a, int64_t chunk, int R) {
     const uint32_t n_words = (uint32_t)(a.g.n_sites / 4);
     const uint32_t w0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
     if (w0 >= n_words) return;
@@ -204,9 +204,9 @@ __device__ __forceinline__ void site_words_chunk(const LocalArgs &a, int64_t chu
     }
 }
 
-// Z2 links of direction a.dir: one chunk of a (direction, parity) pass.
-template <int D, bool STREAM, int R>
-__device__ __forceinline__ void link_words_chunk(const LocalArgs &a, int64_t chunk) {
+// Z2 links of direction a.dir: one chunk of a (direction, parity) pass, R words per thread.
+template <int D, bool STREAM>
+__device__ __forceinline__ void link_words_chunk(const LocalArgs &a, int64_t chunk, int R) {
     const uint32_t n = (uint32_t)a.g.n_sites;
     const uint32_t n_words = n / 4;
     const uint32_t w0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;

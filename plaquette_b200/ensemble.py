@@ -28,6 +28,8 @@ extra_signatures({
     "plq_ensemble_read": ([C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
     "plq_ensemble_primaries": ([C.c_void_p, C.c_int32, C.c_void_p, _P(C.c_int32)], C.c_int),
     "plq_ensemble_primaries_all": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
+    "plq_ensemble_member_config": ([C.c_void_p, C.c_int32, _P(C.c_int32)], C.c_int),
+    "plq_tune_entries": ([C.c_void_p, C.c_int32, _P(C.c_int32)], C.c_int),
     "plq_ensemble_betas": ([C.c_void_p, C.c_void_p], C.c_int),
     "plq_ensemble_n_vars": ([C.c_void_p], C.c_int64),
     "plq_ensemble_cuda_stream": ([C.c_void_p], C.c_void_p),
@@ -81,6 +83,12 @@ class Ensemble:
         check(lib().plq_ensemble_tune(self._h, trial_sweeps, C.byref(r), C.byref(c), C.byref(ms)))
         return r.value, c.value, ms.value
 
+    def member_config(self, m: int) -> int:
+        """Member m's four-site words per thread (0: the generic body)."""
+        w = C.c_int32()
+        check(lib().plq_ensemble_member_config(self._h, m, C.byref(w)))
+        return w.value
+
     def sync(self):
         check(lib().plq_ensemble_sync(self._h))
 
@@ -122,6 +130,25 @@ class Ensemble:
     @property
     def launches(self) -> int:
         return int(lib().plq_ensemble_launches(self._h))
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("model", C.c_int32), ("q", C.c_int32), ("d", C.c_int32), ("updater", C.c_int32),
+                ("rng", C.c_int32), ("words_per_thread", C.c_int32), ("shape", C.c_int64 * 4),
+                ("members", C.c_int32), ("pad", C.c_int32), ("ms_per_sweep", C.c_double)]
+
+
+def tune_entries() -> list[dict]:
+    """The process-wide tuning table: one entry per member shape tuned so far."""
+    n = C.c_int32()
+    check(lib().plq_tune_entries(None, 0, C.byref(n)))
+    arr = (TuneEntry * max(1, n.value))()
+    check(lib().plq_tune_entries(arr, n.value, C.byref(n)))
+    names = {0: "ising", 1: "potts", 2: "gauge"}
+    return [{"model": names.get(t.model, t.model), "q": t.q, "shape": list(t.shape)[: t.d],
+             "updater": ["metropolis", "heatbath", "cluster"][t.updater], "rng": ["stream", "keyed"][t.rng],
+             "words_per_thread": t.words_per_thread, "members": t.members,
+             "ms_per_sweep_alone": round(t.ms_per_sweep, 5)} for t in arr[: n.value]]
 
 
 def batched_workload_spec(seed: int = 20260718):

@@ -150,3 +150,41 @@ def test_primaries_of_every_member_at_once(gpu):
         assert len(every) == ens.n
         for m in range(ens.n):
             assert list(every[m]) == list(ens.primaries(m)), (sweeps, m)
+
+
+def test_tuner_chooses_a_shape_per_member_shape(gpu):
+    """The autotuner picks four-site words per thread for every member shape
+    (timed alone), records them in the process-wide table, and a later
+    ensemble of those shapes starts from them; results stay those of each
+    member's own chain."""
+    from plaquette_b200.ensemble import tune_entries
+
+    specs = [((16, 16, 16), plq.ISING, plq.METROPOLIS, 0.22), ((8, 8, 8, 8), plq.GAUGE, plq.HEATBATH, 0.44),
+             ((32, 32), plq.ISING, plq.HEATBATH, 0.44)]
+    names = {plq.ISING: "ising", plq.GAUGE: "gauge"}
+    upds = {plq.METROPOLIS: "metropolis", plq.HEATBATH: "heatbath"}
+    descs, starts = [], []
+    for i, (shape, kind, upd, beta) in enumerate(specs * 2):
+        n = int(np.prod(shape)) * (len(shape) if kind == plq.GAUGE else 1)
+        starts.append(plq.hot_start(70 + i, 2, n)[0])
+        descs.append(plq.make_desc(kind, 2, shape, upd, beta=beta, seed=70 + i, rng=plq.RNG_KEYED, batch=1))
+    ens = Ensemble(gpu, descs, starts)
+    ens.tune(3)
+    table = {(e["model"], tuple(e["shape"]), e["updater"]): e for e in tune_entries()}
+    for shape, kind, upd, _ in specs:
+        key = (names[kind], shape, upds[upd])
+        assert key in table, key
+        assert table[key]["words_per_thread"] in (1, 2, 4, 8) and table[key]["members"] == 2
+        assert table[key]["ms_per_sweep_alone"] > 0
+    for m, d in enumerate(descs):
+        key = (names[d.model], tuple(d.shape[: d.d]), upds[d.updater])
+        assert ens.member_config(m) == table[key]["words_per_thread"]
+    later = Ensemble(gpu, descs, starts)
+    assert [later.member_config(m) for m in range(len(descs))] == [ens.member_config(m) for m in range(len(descs))]
+    chains = [plq.GpuChain(gpu, d, s) for d, s in zip(descs, starts)]
+    ens.advance(5)
+    later.advance(5)
+    for m, c in enumerate(chains):
+        c.advance(5)
+        assert np.array_equal(ens.read(m), c.read()), m
+        assert np.array_equal(later.read(m), c.read()), m
