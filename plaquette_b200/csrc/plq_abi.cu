@@ -163,10 +163,6 @@ extern "C" int plq_chain_validate(const plq_chain_desc *d) {
                                                 (d->model == PLQ_GAUGE ? "link" : "site") +
                                                 " checkerboard needs even lattice extents, got " +
                                                 shape_string(d));
-        if (d->model == PLQ_POTTS && d->q > 2 && d->updater == PLQ_METROPOLIS && d->rng == PLQ_RNG_STREAM)
-            return plq_fail(PLQ_EUNSUPPORTED,
-                            "Potts Metropolis at q >= 3 on the PCG stream draws its proposal through "
-                            "rand's range sampler; this device path runs it on the keyed stream only");
         return PLQ_OK;
     }
     if (d->updater == PLQ_CLUSTER) {
@@ -577,6 +573,9 @@ int local_sweep(plq_chain *c) {
             s.epoch = a.epoch;
             s.pos_in = a.pos_in;
             e = launch_scan_metro(s, c->d, c->stream);
+        } else if (c->lookback && c->desc.model == PLQ_POTTS && c->q > 2) {
+            // the proposal's draw count depends on its own value: a sequential walk
+            e = launch_potts_metro_walk(a, c->stream);
         } else {
             e = launch_local_pass(a, c->link, c->lookback, c->stream);
             if (c->lookback) c->tickets_issued += (uint64_t)c->n_chunks;

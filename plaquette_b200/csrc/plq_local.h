@@ -12,6 +12,9 @@ int64_t local_chunks(int64_t n_sites);
 int64_t word_chunks(int64_t n_sites);
 // One colour pass: sites (link=false) or the links of direction a.dir.
 cudaError_t launch_local_pass(const LocalArgs &a, bool link, bool lookback, cudaStream_t stream);
+// One colour pass of Potts Metropolis (q >= 3) on the PCG stream: the
+// sequential walk (plq_walk.cu); start and end positions in a.ctrl->pos.
+cudaError_t launch_potts_metro_walk(const LocalArgs &a, cudaStream_t stream);
 
 // Exact integer primaries of a configuration into out (int64, zeroed by the
 // launcher): Ising {bond_sum, spin_sum}, Potts {agree, counts[q]}, gauge

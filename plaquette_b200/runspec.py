@@ -15,8 +15,9 @@ reference's messages (src/config.rs:189-249, src/models/ising/run_config.rs:
 `Chain` under the checkerboard schedule, hot start drawn from the seeded
 generator first); `backend = "gpu"` maps to the keyed stream of the reference
 GPU kernels.  What this device path cannot run is refused with a reason: the
-random schedule (a sequential walk), Wolff on the PCG stream (the FIFO draw
-order of `grow_cluster`), and Potts Metropolis on the PCG stream for q >= 3.
+random schedule (a sequential walk) and Wolff on the PCG stream (the FIFO draw
+order of `grow_cluster`).  Potts Metropolis at q >= 3 on the PCG stream runs
+as a sequential walk on one warp (exact, at one thread's speed).
 """
 from __future__ import annotations
 
@@ -202,9 +203,6 @@ def parse(text: str, model: int, q: int | None = None) -> RunSpec:
     if updater == "wolff" and rng == RNG_STREAM:
         raise ConfigError("Wolff on the CPU stream draws in grow_cluster's sequential FIFO order; run it with "
                           'backend = "gpu" (the keyed stream)')
-    if model == POTTS and q >= 3 and updater == "metropolis" and rng == RNG_STREAM:
-        raise ConfigError("Potts Metropolis at q >= 3 on the CPU stream draws its proposal through rand's range "
-                          'sampler; run it with backend = "gpu" (the keyed stream)')
     kernel = {"metropolis": METROPOLIS, "heat_bath": HEATBATH}.get(updater, CLUSTER)
     extent = EXTENT_SEEDED if updater == "wolff" else EXTENT_ALL
     relabel = RELABEL_FORCED if updater == "wolff" else RELABEL_REDRAW

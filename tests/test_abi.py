@@ -81,8 +81,8 @@ def test_other_contracts():
         plq.validate(_desc(model=plq.GAUGE, shape=(4,)))
     with pytest.raises(plq.ContractError, match="at least two states"):
         plq.validate(_desc(model=plq.POTTS, q=1))
-    with pytest.raises(plq.UnsupportedError):
-        plq.validate(_desc(model=plq.POTTS, q=3, rng=plq.RNG_STREAM))
+    # Potts Metropolis at q >= 3 on the PCG stream is valid (the sequential walk)
+    plq.validate(_desc(model=plq.POTTS, q=3, rng=plq.RNG_STREAM))
 
 
 @pytest.mark.parametrize("seed,q,n", [(20260718, 2, 4096), (7, 3, 5000), (1, 5, 777)])

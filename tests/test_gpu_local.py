@@ -83,8 +83,6 @@ CASES = [
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{['ising','potts','gauge'][c[0]]}{c[1]}-{'x'.join(map(str, c[2]))}")
 def test_sweeps_bit_exact(oracle, gpu, case, kernel, rng_mode):
     kind, q, shape, beta, extra = case
-    if kind == plq.POTTS and q > 2 and kernel == plq.METROPOLIS and rng_mode == plq.RNG_STREAM:
-        pytest.skip("Potts q>=3 Metropolis runs on the keyed stream only")
     got, want, *_ = run_pair(oracle, gpu, kind, q, shape, kernel, rng_mode, beta, 7, **extra)
     assert np.array_equal(got, want)
 
@@ -284,3 +282,39 @@ def test_chain_outlives_its_context():
     c2.advance(4)
     assert np.array_equal(next(c2), first)  # same seed, same keyed sweeps
     c2.close()
+
+
+def test_potts_stream_metropolis_second_draw(oracle, gpu):
+    """Potts Metropolis on the PCG stream draws its proposal with
+    next_below(q - 1) (src/updater.rs:659-668), which takes a second draw when
+    the first lands in rand's rejection zone (probability (q - 2) / 2^32).  At
+    seed 13 the draw at stream position 7064085 does so for q = 64, so a chain
+    starting there must consume it on its first proposal -- and stay bit-exact
+    with the CPU walk, configurations and stream position."""
+    q, shape, seed, offset, beta = 64, (8, 8), 13, 7064085, 0.9
+    probe = oracle.PcgStream(seed)
+    probe.advance(offset)
+    probe.next_below(q - 1)
+    assert probe.draws == offset + 2  # the first proposal takes two draws
+    lat = oracle.Lattice(shape)
+    model = oracle.Model.potts(q, 1.0)
+    start = np.random.default_rng(5).integers(0, q, 64).astype(np.uint8)
+    d = plq.make_desc(plq.POTTS, q, shape, plq.METROPOLIS, beta=beta, seed=seed, rng=plq.RNG_STREAM,
+                      stream_offset=offset, sweeps_between=3, batch=1)
+    chain = plq.GpuChain(gpu, d, start)
+    got = next(chain)
+    r = oracle.PcgStream(seed)
+    r.advance(offset)
+    want = start.copy()
+    oracle.local_sweeps(model, lat, want, plq.METROPOLIS, beta, r, 3)
+    assert np.array_equal(got, want)
+    assert chain.stream_position() == r.draws
+
+
+@pytest.mark.parametrize("q,shape", [(3, (64, 32)), (4, (16, 8, 8)), (7, (6, 6, 4, 4))], ids=str)
+def test_potts_stream_metropolis_larger_lattices(oracle, gpu, q, shape):
+    """The sequential walk over groups of 32 ranks, with a partial last group,
+    across many sweeps; the q = 3 heat bath beside it is unchanged."""
+    got, want, chain, *_ = run_pair(oracle, gpu, plq.POTTS, q, shape, plq.METROPOLIS, plq.RNG_STREAM, 0.8, 5)
+    assert chain.path == "lookback"
+    assert np.array_equal(got, want)

@@ -74,7 +74,6 @@ def test_defaults_and_mapping():
     # what this device path refuses, with its reason
     (_cfg(drop=("schedule",)), plq.ISING, "the random schedule is a sequential walk"),
     (_cfg('updater = "wolff"', drop=("schedule",)), plq.ISING, "Wolff on the CPU stream"),
-    (_cfg(), plq.POTTS, "Potts Metropolis at q >= 3 on the CPU stream"),
     (_cfg("h = [0.1, 0.2]"), plq.POTTS, "h names 2 offsets but the run has q = 3 labels"),
 ])
 def test_validation_messages(text, model, msg):
@@ -95,3 +94,8 @@ def test_hot_start_is_drawn_from_the_seeded_generator(oracle):
     r = oracle.PcgStream(7)
     want = oracle.hot_start(256, 2, r)
     assert (cfg == want).all() and off == r.draws
+
+
+def test_potts_metropolis_on_the_cpu_stream_is_accepted():
+    s = runspec.parse(_cfg(), plq.POTTS, q=3)
+    assert s.desc.rng == plq.RNG_STREAM and s.desc.updater == plq.METROPOLIS and s.desc.q == 3
