@@ -210,6 +210,21 @@ int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc *members, 
  * pairs, then odd pairs) with min(1, exp((b_i - b_i+1)(E_i - E_i+1))). */
 int plq_ensemble_add_ladder(plq_ensemble *e, int32_t k, const int32_t *member_ids, const double *betas,
                             int32_t every, uint64_t seed);
+/* Member m runs at `beta` from its next sweep (its decision tables rebuilt in
+ * place); refused for members of a ladder, whose betas the ladder moves.
+ * Used where tempering spans ranks: every rank decides the swaps with
+ * plq_tempering_swap_phase and sets the betas of the members it holds. */
+int plq_ensemble_set_beta(plq_ensemble *e, int32_t member, double beta);
+/* The ladder's swap rule on the host, identical bit for bit to the device's
+ * (one header defines both): one phase of attempt `attempt` over k_slots
+ * slots -- pairs (k, k+1) from k = attempt & 1 in steps of 2 -- given every
+ * member's energy integer (bond, agreement or plaquette sum) and coupling;
+ * accepted pairs exchange their betas in beta_of_member and their members in
+ * member_of_slot.  `ladder_seed` is folded as plq_ensemble_add_ladder folds
+ * it.  *accepted_out (may be NULL) = the swaps taken. */
+int plq_tempering_swap_phase(int32_t k_slots, int32_t *member_of_slot, double *beta_of_member,
+                             const int64_t *energy, const double *j_of_member, uint64_t ladder_seed,
+                             uint64_t attempt, int32_t *accepted_out);
 /* `sweeps` sweeps of every member (and the swaps they reach) in one
  * persistent cooperative launch, captured once into a CUDA graph and replayed. */
 int plq_ensemble_advance(plq_ensemble *e, uint64_t sweeps);

@@ -40,6 +40,7 @@
 #include "plq_geom.cuh"
 #include "plq_local.h"
 #include "plq_local_impl.cuh"
+#include "plq_pt.cuh"
 #include "plq_tables.h"
 #include "plq_words.cuh"
 
@@ -325,36 +326,6 @@ __device__ void energy_phase(const EnsArgs &e) {
     }
 }
 
-// e^x for x <= 0 from IEEE basic operations only, each rounded on its own
-// (explicit _rn intrinsics: no contraction into fused multiply-adds), so the
-// tempering decision is a pure function a host restates bit for bit.
-// x = n ln2 + r with n = floor(x/ln2 + 1/2) and ln2 split after Cody and
-// Waite into a 32-significant-bit high part (n * high is exact) and a low
-// part; e^r (|r| <= 0.347) by its Taylor polynomial to degree 14 in Horner
-// form (truncation below 2^-60 relative); then times 2^n.  Below x = -708 the
-// result is 0 (2^n would leave the normal range).
-__device__ double pt_exp(double x) {
-    if (!(x > -708.0)) return 0.0;
-    const double n = floor(__dadd_rn(__dmul_rn(x, 1.4426950408889634), 0.5));
-    const double r = __dsub_rn(__dsub_rn(x, __dmul_rn(n, 0.6931471803691238)), __dmul_rn(n, 1.9082149292705877e-10));
-    double p = 1.1470745597729725e-11;  // 1/14!
-    p = __dadd_rn(__dmul_rn(p, r), 1.6059043836821613e-10);
-    p = __dadd_rn(__dmul_rn(p, r), 2.08767569878681e-09);
-    p = __dadd_rn(__dmul_rn(p, r), 2.505210838544172e-08);
-    p = __dadd_rn(__dmul_rn(p, r), 2.755731922398589e-07);
-    p = __dadd_rn(__dmul_rn(p, r), 2.7557319223985893e-06);
-    p = __dadd_rn(__dmul_rn(p, r), 2.48015873015873e-05);
-    p = __dadd_rn(__dmul_rn(p, r), 0.0001984126984126984);
-    p = __dadd_rn(__dmul_rn(p, r), 0.001388888888888889);
-    p = __dadd_rn(__dmul_rn(p, r), 0.008333333333333333);
-    p = __dadd_rn(__dmul_rn(p, r), 0.041666666666666664);
-    p = __dadd_rn(__dmul_rn(p, r), 0.16666666666666666);
-    p = __dadd_rn(__dmul_rn(p, r), 0.5);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0);
-    p = __dadd_rn(__dmul_rn(p, r), 1.0);
-    return __dmul_rn(p, __longlong_as_double((long long)(n + 1023.0) << 52));
-}
-
 // Swap attempts of every ladder (one thread per pair); attempt index `att`.
 // Energies E = -J * (bond, agreement or plaquette sum); the pair at slots
 // (k, k+1) exchanges betas when (b_k - b_k+1)(E_k - E_k+1) >= 0 or a keyed
@@ -366,15 +337,9 @@ __device__ void swap_phase(const EnsArgs &e, unsigned long long att) {
         const int parity = (int)(att & 1ull);
         for (int k = parity + 2 * (int)threadIdx.x; k + 1 < L.k; k += 2 * (int)blockDim.x) {
             int m1 = L.member_of_slot[k], m2 = L.member_of_slot[k + 1];
-            double b1 = e.tsets[e.ts_of_member[m1]].beta, b2 = e.tsets[e.ts_of_member[m2]].beta;
-            double E1 = -__dmul_rn(e.members[m1].j, (double)e.energy[m1]);
-            double E2 = -__dmul_rn(e.members[m2].j, (double)e.energy[m2]);
-            double delta = __dmul_rn(__dsub_rn(b1, b2), __dsub_rn(E1, E2));
-            uint32_t h1 = keyed24(L.seed32 ^ 0x6a09e667u, (uint32_t)k, (uint32_t)att);
-            uint32_t h2 = keyed24(L.seed32 ^ 0xbb67ae85u, (uint32_t)k, (uint32_t)att);
-            double u = __dmul_rn(__dadd_rn((double)h1, __dmul_rn((double)h2, 5.9604644775390625e-8)),
-                                 5.9604644775390625e-8);
-            if (delta >= 0.0 || u < pt_exp(delta)) {
+            const double b1 = e.tsets[e.ts_of_member[m1]].beta, b2 = e.tsets[e.ts_of_member[m2]].beta;
+            if (pt_accept(b1, b2, e.energy[m1], e.energy[m2], e.members[m1].j, e.members[m2].j, L.seed32,
+                          (uint32_t)k, (uint32_t)att)) {
                 int32_t t1 = e.ts_of_member[m1];
                 e.ts_of_member[m1] = e.ts_of_member[m2];
                 e.ts_of_member[m2] = t1;
@@ -811,6 +776,58 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
     return PLQ_OK;
 }
 
+namespace {
+
+// Member m's current table set (the host copy) rebuilt at `beta`, in place:
+// the table sizes depend on the model and shape only, so the device buffers
+// (and every captured launch that reads them) stay.
+int rebuild_tables(plq_ensemble *E, int32_t m, double beta) {
+    const plq_chain_desc &d = E->descs[m];
+    ModelParams p;
+    std::memset(&p, 0, sizeof p);
+    p.model = d.model;
+    p.q = d.model == PLQ_POTTS ? d.q : 2;
+    p.d = d.d;
+    p.beta = beta;
+    p.j = d.j;
+    p.h = d.h;
+    for (int a = 0; a < PLQ_MAX_Q; ++a) p.offsets[a] = d.offsets[a];
+    Tables t;
+    std::string err;
+    if (!build_tables(p, d.updater, d.rng, t, err)) return plq_fail(PLQ_EUNSUPPORTED, err);
+    TableSet &ts = E->tsets[E->ts_of_member[m]];
+    ts.beta = beta;
+    const size_t bytes53 = t.hb53.size() * 8, bytes24 = t.hb24.size() * 4, m53 = t.metro53.size() * 8,
+                 m24 = t.metro24.size() * 4;
+    cudaError_t ce = cudaSuccess;
+    if (bytes53) ce = cudaMemcpyAsync((void *)ts.hb53, t.hb53.data(), bytes53, cudaMemcpyHostToDevice, E->stream);
+    if (ce == cudaSuccess && bytes24)
+        ce = cudaMemcpyAsync((void *)ts.hb24, t.hb24.data(), bytes24, cudaMemcpyHostToDevice, E->stream);
+    if (ce == cudaSuccess && m53)
+        ce = cudaMemcpyAsync((void *)ts.metro53, t.metro53.data(), m53, cudaMemcpyHostToDevice, E->stream);
+    if (ce == cudaSuccess && m24)
+        ce = cudaMemcpyAsync((void *)ts.metro24, t.metro24.data(), m24, cudaMemcpyHostToDevice, E->stream);
+    if (ce == cudaSuccess && E->d_tsets)
+        ce = cudaMemcpyAsync(E->d_tsets + E->ts_of_member[m], &ts, sizeof ts, cudaMemcpyHostToDevice, E->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
+    if (ce != cudaSuccess) return ens_fail(ce, "member tables");
+    return PLQ_OK;
+}
+
+}  // namespace
+
+extern "C" int plq_ensemble_set_beta(plq_ensemble *E, int32_t m, double beta) {
+    if (!E || m < 0 || m >= (int32_t)E->members.size()) return plq_fail(PLQ_EINVAL, "bad arguments");
+    if (E->members[m].ladder >= 0)
+        return plq_fail(PLQ_EINVAL, "the beta of a member in a tempering ladder belongs to its ladder");
+    cudaError_t ce = plq_enter_device(E->ctx->device);
+    if (ce != cudaSuccess) return ens_fail(ce, "cudaSetDevice");
+    const int rc = rebuild_tables(E, m, beta);
+    if (rc != PLQ_OK) return rc;
+    E->descs[m].beta = beta;
+    return PLQ_OK;
+}
+
 extern "C" int plq_ensemble_add_ladder(plq_ensemble *E, int32_t k, const int32_t *member_ids, const double *betas,
                                        int32_t every, uint64_t seed) {
     if (!E || k < 2 || !member_ids || !betas || every <= 0) return plq_fail(PLQ_EINVAL, "bad ladder arguments");
@@ -831,33 +848,9 @@ extern "C" int plq_ensemble_add_ladder(plq_ensemble *E, int32_t k, const int32_t
     }
     // slot i of the ladder runs at betas[i]: rebuild member i's table set at that beta
     for (int32_t i = 0; i < k; ++i) {
-        int32_t m = ids[i];
-        plq_chain_desc d = E->descs[m];
-        d.beta = betas[i];
-        ModelParams p;
-        std::memset(&p, 0, sizeof p);
-        p.model = d.model;
-        p.q = d.model == PLQ_POTTS ? d.q : 2;
-        p.d = d.d;
-        p.beta = d.beta;
-        p.j = d.j;
-        Tables t;
-        std::string err;
-        if (!build_tables(p, d.updater, d.rng, t, err)) return plq_fail(PLQ_EUNSUPPORTED, err);
-        TableSet &ts = E->tsets[E->ts_of_member[m]];
-        ts.beta = betas[i];
-        size_t bytes53 = t.hb53.size() * 8, bytes24 = t.hb24.size() * 4, m53 = t.metro53.size() * 8,
-               m24 = t.metro24.size() * 4;
-        cudaError_t ce = cudaSuccess;
-        if (bytes53) ce = cudaMemcpyAsync((void *)ts.hb53, t.hb53.data(), bytes53, cudaMemcpyHostToDevice, E->stream);
-        if (ce == cudaSuccess && bytes24)
-            ce = cudaMemcpyAsync((void *)ts.hb24, t.hb24.data(), bytes24, cudaMemcpyHostToDevice, E->stream);
-        if (ce == cudaSuccess && m53)
-            ce = cudaMemcpyAsync((void *)ts.metro53, t.metro53.data(), m53, cudaMemcpyHostToDevice, E->stream);
-        if (ce == cudaSuccess && m24)
-            ce = cudaMemcpyAsync((void *)ts.metro24, t.metro24.data(), m24, cudaMemcpyHostToDevice, E->stream);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
-        if (ce != cudaSuccess) return ens_fail(ce, "ladder tables");
+        const int32_t m = ids[i];
+        const int rc = rebuild_tables(E, m, betas[i]);
+        if (rc != PLQ_OK) return rc;
         E->members[m].ladder = (int)E->ladders.size();
     }
     int32_t *d_slots = nullptr;
@@ -1181,6 +1174,29 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
     if (ctas_out) *ctas_out = best_c;
     if (ms_per_sweep_out) *ms_per_sweep_out = best / trial_sweeps;
     return ens_status(E);
+}
+
+extern "C" int plq_tempering_swap_phase(int32_t k_slots, int32_t *member_of_slot, double *beta_of_member,
+                                        const int64_t *energy, const double *j_of_member, uint64_t ladder_seed,
+                                        uint64_t attempt, int32_t *accepted_out) {
+    if (k_slots < 0 || (k_slots > 0 && (!member_of_slot || !beta_of_member || !energy || !j_of_member)))
+        return plq_fail(PLQ_EINVAL, "bad arguments");
+    const uint32_t seed32 = plq_fold_seed(ladder_seed);
+    int32_t accepted = 0;
+    for (int32_t k = (int32_t)(attempt & 1u); k + 1 < k_slots; k += 2) {
+        const int32_t m1 = member_of_slot[k], m2 = member_of_slot[k + 1];
+        const double b1 = beta_of_member[m1], b2 = beta_of_member[m2];
+        if (pt_accept(b1, b2, energy[m1], energy[m2], j_of_member[m1], j_of_member[m2], seed32, (uint32_t)k,
+                      (uint32_t)attempt)) {
+            beta_of_member[m1] = b2;
+            beta_of_member[m2] = b1;
+            member_of_slot[k] = m2;
+            member_of_slot[k + 1] = m1;
+            ++accepted;
+        }
+    }
+    if (accepted_out) *accepted_out = accepted;
+    return PLQ_OK;
 }
 
 extern "C" int plq_ensemble_member_config(plq_ensemble *E, int32_t m, int32_t *words_per_thread) {

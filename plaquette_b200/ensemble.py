@@ -29,6 +29,9 @@ extra_signatures({
     "plq_ensemble_primaries": ([C.c_void_p, C.c_int32, C.c_void_p, _P(C.c_int32)], C.c_int),
     "plq_ensemble_primaries_all": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p], C.c_int),
     "plq_ensemble_member_config": ([C.c_void_p, C.c_int32, _P(C.c_int32)], C.c_int),
+    "plq_ensemble_set_beta": ([C.c_void_p, C.c_int32, C.c_double], C.c_int),
+    "plq_tempering_swap_phase": ([C.c_int32, _P(C.c_int32), _P(C.c_double), _P(C.c_int64), _P(C.c_double),
+                                  C.c_uint64, C.c_uint64, _P(C.c_int32)], C.c_int),
     "plq_tune_entries": ([C.c_void_p, C.c_int32, _P(C.c_int32)], C.c_int),
     "plq_ensemble_betas": ([C.c_void_p, C.c_void_p], C.c_int),
     "plq_ensemble_n_vars": ([C.c_void_p], C.c_int64),
@@ -83,6 +86,10 @@ class Ensemble:
         check(lib().plq_ensemble_tune(self._h, trial_sweeps, C.byref(r), C.byref(c), C.byref(ms)))
         return r.value, c.value, ms.value
 
+    def set_beta(self, m: int, beta: float) -> None:
+        """Member m runs at `beta` from its next sweep (members outside ladders)."""
+        check(lib().plq_ensemble_set_beta(self._h, m, beta))
+
     def member_config(self, m: int) -> int:
         """Member m's four-site words per thread (0: the generic body)."""
         w = C.c_int32()
@@ -130,6 +137,21 @@ class Ensemble:
     @property
     def launches(self) -> int:
         return int(lib().plq_ensemble_launches(self._h))
+
+
+def swap_phase(member_of_slot: np.ndarray, beta_of_member: np.ndarray, energy: np.ndarray, j_of_member: np.ndarray,
+               ladder_seed: int, attempt: int) -> int:
+    """The ladder's swap rule on the host (plq_tempering_swap_phase), in place
+    on the int32 slot table and the float64 betas; returns the swaps taken."""
+    assert member_of_slot.dtype == np.int32 and beta_of_member.dtype == np.float64
+    assert energy.dtype == np.int64 and j_of_member.dtype == np.float64
+    acc = C.c_int32()
+    check(lib().plq_tempering_swap_phase(len(member_of_slot), member_of_slot.ctypes.data_as(_P(C.c_int32)),
+                                         beta_of_member.ctypes.data_as(_P(C.c_double)),
+                                         energy.ctypes.data_as(_P(C.c_int64)),
+                                         j_of_member.ctypes.data_as(_P(C.c_double)), ladder_seed, attempt,
+                                         C.byref(acc)))
+    return acc.value
 
 
 class TuneEntry(C.Structure):

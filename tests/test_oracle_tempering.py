@@ -85,3 +85,27 @@ def test_favourable_exchange_is_always_taken_and_pairs_alternate(oracle):
     slots = np.array([0, 1], dtype=np.int32)
     beta = np.array([0.1, 0.5])
     assert oracle.pt_swap_phase(slots, beta, np.array([0, 3000], dtype=np.int64), np.ones(2), 9, 0) == 0
+
+
+def test_library_host_rule_equals_the_oracle(oracle):
+    """plq_tempering_swap_phase (the rule the device kernel uses, evaluated
+    on the host for tempering across ranks) against the oracle's
+    restatement, with the ladder seed folded as plq_ensemble_add_ladder
+    folds it."""
+    import plaquette_b200 as plq
+    from plaquette_b200.ensemble import swap_phase
+
+    rng = np.random.default_rng(29)
+    for trial in range(300):
+        k = int(rng.integers(2, 10))
+        n = k + 3
+        slots = rng.permutation(n)[:k].astype(np.int32)
+        beta = rng.uniform(0.1, 0.7, n)
+        energy = rng.integers(-5000, 5000, n).astype(np.int64)
+        j = rng.choice([1.0, 0.8, 1.3], n)
+        seed, att = int(rng.integers(0, 2 ** 63)), int(rng.integers(0, 100))
+        a_slots, a_beta = slots.copy(), beta.copy()
+        b_slots, b_beta = slots.copy(), beta.copy()
+        na = swap_phase(a_slots, a_beta, energy, j, seed, att)
+        nb = oracle.pt_swap_phase(b_slots, b_beta, energy, j, plq.fold_seed(seed), att)
+        assert na == nb and list(a_slots) == list(b_slots) and list(a_beta) == list(b_beta), trial
