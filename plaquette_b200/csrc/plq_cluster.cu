@@ -304,6 +304,15 @@ __global__ void __launch_bounds__(kThreads) bonds_kernel(ClusterArgs a) {
     if (row8 && s0 < n) *reinterpret_cast<uint64_t *>(a.bonds + s0) = opened;
 }
 
+// The keyed bond (s, mu) to the +mu neighbour `nb`, evaluated where it is
+// used (no bond array on the keyed stream): open iff the two sites agree and
+// the bond's keyed draw is below p (cluster_prelude.wgsl:61-80).
+template <int D>
+__device__ __forceinline__ bool keyed_bond(const ClusterArgs &a, int64_t s, int mu, int64_t nb) {
+    return a.state[s] == a.state[nb] &&
+           keyed24(a.seed32 ^ kBondKey, (uint32_t)(s * D + mu), a.sweep32) < a.kp24;
+}
+
 // ------------------------------------------------------------ 2. labels
 __device__ __forceinline__ int32_t find_root(int32_t *parent, int32_t x, int cap, Control *ctrl) {
     int32_t p = ld_relaxed32(&parent[x]);
@@ -390,7 +399,7 @@ __device__ __forceinline__ void lunite(int32_t *p, int32_t a, int32_t b, int cap
     }
 }
 
-template <int D>
+template <int D, bool KEYED>
 __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
     __shared__ int32_t p[kTileSites];
     __shared__ uint8_t bs[kTileSites];  // the tile's bond bytes
@@ -417,7 +426,22 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
         const int li = k * (int)blockDim.x + (int)threadIdx.x;
         const bool valid = li < T;
         const int xl = li & m0;
-        const uint32_t own = valid ? a.bonds[base + xl + (int64_t)(li >> sh0) * L0] : 0u;
+        uint32_t own = 0;
+        if (valid) {
+            const int64_t s = base + xl + (int64_t)(li >> sh0) * L0;
+            if (KEYED) {
+                // +x and +y bonds from the spins and the keyed draws (the bonds along
+                // dims >= 2 all leave the tile: boundary_hook_kernel evaluates them)
+                const int xg = tx * T0 + xl;
+                own = keyed_bond<D>(a, s, 0, xg + 1 < L0 ? s + 1 : s + 1 - L0) ? 1u : 0u;
+                if (D >= 2) {
+                    const int yg = ty * T1 + (li >> sh0);
+                    own |= keyed_bond<D>(a, s, 1, yg + 1 < L1 ? s + L0 : s - (int64_t)(L1 - 1) * L0) ? 2u : 0u;
+                }
+            } else {
+                own = a.bonds[s];
+            }
+        }
         if (valid) bs[li] = (uint8_t)own;
         // the bond into this site from its -x neighbour (lane - 1), inside this warp's segment
         const uint32_t from_left = __shfl_up_sync(0xffffffffu, own, 1);
@@ -461,7 +485,7 @@ __global__ void __launch_bounds__(kThreads) tile_hook_kernel(ClusterArgs a) {
 // tile's last column (when tiles split the rows), +y bonds of its last row
 // (when tiles split dim 1), and every bond along dims >= 2.  Thread t of the
 // grid takes candidate site t of each family in turn.
-template <int D>
+template <int D, bool KEYED>
 __global__ void __launch_bounds__(kThreads) boundary_hook_kernel(ClusterArgs a) {
     const int64_t n = a.g.n_sites;
     const int L0 = a.g.L[0], L1 = D >= 2 ? a.g.L[1] : 1;
@@ -486,19 +510,28 @@ __global__ void __launch_bounds__(kThreads) boundary_hook_kernel(ClusterArgs a) 
             s = (row * T1 + (T1 - 1)) * per_row + (cy - row * per_row);
             mu = 1;
         }
-        if (!((a.bonds[s] >> mu) & 1u)) continue;
+        if (!KEYED && !((a.bonds[s] >> mu) & 1u)) continue;
         int32_t x[D];
         site_coords<D>(a.g, s, x);
         // compile-time directions keep the coordinates in registers
         const int64_t nb = mu == 0 ? nbr_plus(a.g, s, x, 0) : nbr_plus(a.g, s, x, D >= 2 ? 1 : 0);
+        if (KEYED && !keyed_bond<D>(a, s, mu, nb)) continue;
         unite(a.parent, (int32_t)s, (int32_t)nb, a.cap, a.ctrl);
     }
     if (D >= 3) {
         for (int64_t s = t0; s < n; s += stride) {
-            const uint8_t b = (uint8_t)(a.bonds[s] >> 2);
-            if (!b) continue;
+            uint8_t b = 0;
             int32_t x[D];
-            site_coords<D>(a.g, s, x);
+            if (KEYED) {
+                site_coords<D>(a.g, s, x);
+#pragma unroll
+                for (int mu = 2; mu < D; ++mu)
+                    if (keyed_bond<D>(a, s, mu, nbr_plus(a.g, s, x, mu))) b |= (uint8_t)(1u << (mu - 2));
+            } else {
+                b = (uint8_t)(a.bonds[s] >> 2);
+                if (!b) continue;
+                site_coords<D>(a.g, s, x);
+            }
 #pragma unroll
             for (int mu = 2; mu < D; ++mu)
                 if ((b >> (mu - 2)) & 1u) unite(a.parent, (int32_t)s, (int32_t)nbr_plus(a.g, s, x, mu), a.cap, a.ctrl);
@@ -920,14 +953,18 @@ int sweep_d(plq_chain *c, uint64_t sweeps) {
             cd->lookback_launches++;
         };
         if (stream) {
+            // PCG stream: the bond draws sit at scanned positions, so they are made in one pass
             lookback(a);
             bonds_kernel<D, true><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
+            tile_hook_kernel<D, false><<<(unsigned)cd->n_tiles, kThreads, 0, c->stream>>>(a);
+            boundary_hook_kernel<D, false><<<gs, kThreads, 0, c->stream>>>(a);
+            c->launches += 3;
         } else {
-            bonds_kernel<D, false><<<(unsigned)cd->n_chunks, kThreads, 0, c->stream>>>(a);
+            // keyed: each bond is a closed form of its index, evaluated where it is used
+            tile_hook_kernel<D, true><<<(unsigned)cd->n_tiles, kThreads, 0, c->stream>>>(a);
+            boundary_hook_kernel<D, true><<<gs, kThreads, 0, c->stream>>>(a);
+            c->launches += 2;
         }
-        tile_hook_kernel<D><<<(unsigned)cd->n_tiles, kThreads, 0, c->stream>>>(a);
-        boundary_hook_kernel<D><<<gs, kThreads, 0, c->stream>>>(a);
-        c->launches += 3;
         if (!stream) {
             relabel_keyed_kernel<<<gs, kThreads, 0, c->stream>>>(a);
             c->launches++;
