@@ -50,6 +50,7 @@ __device__ __forceinline__ uint32_t word_dx(const uint8_t *p, uint32_t base, int
 
 struct WordPos {
     uint32_t s;       // first site of the word
+    uint32_t x0;      // its coordinate along direction 0
     int32_t op[8], om[8];  // row-aligned offsets to the +mu / -mu rows (mu >= 1)
     uint32_t left, right;  // offsets to the previous / next word of the row (wrapping)
     int b;            // byte of the first colour site
@@ -63,6 +64,7 @@ __device__ __forceinline__ WordPos word_pos(const LocalArgs &a, uint32_t w) {
     const uint32_t row = fdiv(P.s, g.dm[0], g.dl[0]);
     const uint32_t x0 = P.s - row * (uint32_t)g.L[0];
     const uint32_t L0 = (uint32_t)g.L[0];
+    P.x0 = x0;
     P.left = x0 == 0 ? L0 - 4u : (uint32_t)-4;
     P.right = x0 + 4u == L0 ? (uint32_t)(4 - (int)L0) : 4u;
     int par = 0;
@@ -80,6 +82,22 @@ __device__ __forceinline__ WordPos word_pos(const LocalArgs &a, uint32_t w) {
     }
     P.b = (a.color ^ par) & 1;
     return P;
+}
+
+// The position of word w + 1 from that of word w: within a row only the site,
+// x0 and the row-wrap offsets move (the offsets to other rows and the colour's
+// byte do not); at a row's end everything is recomputed.
+template <int D>
+__device__ __forceinline__ void word_pos_next(const LocalArgs &a, uint32_t w_next, WordPos &P) {
+    const uint32_t L0 = (uint32_t)a.g.L[0];
+    if (P.x0 + 4u < L0) {
+        P.s += 4u;
+        P.x0 += 4u;
+        P.left = (uint32_t)-4;
+        P.right = P.x0 + 4u == L0 ? (uint32_t)(4 - (int)L0) : 4u;
+    } else {
+        P = word_pos<D>(a, w_next);
+    }
 }
 
 // Decision of one colour site from its key; `k` is the draw (53-bit stream or
@@ -140,11 +158,12 @@ __device__ __forceinline__ void site_words_chunk(const LocalArgs &a, int64_t chu
     const uint8_t *S = a.state;
     const uint32_t M1 = 0x01010101u;
     const uint32_t P2 = 2u * D + 1u;  // g(2)
+    WordPos P = word_pos<D>(a, w0);
 #pragma unroll 1
     for (int i = 0; i < R; ++i) {
         const uint32_t w = w0 + i;
         if (w >= n_words) break;
-        const WordPos P = word_pos<D>(a, w);
+        if (i > 0) word_pos_next<D>(a, w, P);
         const uint32_t C = ld_word(S, P.s);
         uint32_t nb[2 * D];
         nb[0] = word_dx(S, P.s, +1, P.left, P.right);
@@ -215,11 +234,12 @@ __device__ __forceinline__ void link_words_chunk(const LocalArgs &a, int64_t chu
     u128 st{0, 0};
     if (STREAM) st = jump(a.jump, a.base, a.pass_offset + 2ull * w0);
     const uint8_t *Umu = a.state + (size_t)mu * n;
+    WordPos P = word_pos<D>(a, w0);
 #pragma unroll 1
     for (int i = 0; i < R; ++i) {
         const uint32_t w = w0 + i;
         if (w >= n_words) break;
-        const WordPos P = word_pos<D>(a, w);
+        if (i > 0) word_pos_next<D>(a, w, P);
         // displacement of +mu: along x a byte shift, else a row offset
         const int dxm = mu == 0 ? 1 : 0;
         const uint32_t om_mu = mu == 0 ? 0u : (uint32_t)P.op[mu];
