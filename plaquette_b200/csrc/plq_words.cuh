@@ -242,7 +242,11 @@ __device__ __forceinline__ void link_words_chunk(const LocalArgs &a, int64_t chu
         if (i > 0) word_pos_next<D>(a, w, P);
         // displacement of +mu: along x a byte shift, else a row offset
         const int dxm = mu == 0 ? 1 : 0;
-        const uint32_t om_mu = mu == 0 ? 0u : (uint32_t)P.op[mu];
+        // P.op[mu] by compile-time indices: a runtime index would put P in local memory
+        uint32_t om_mu = 0;
+#pragma unroll
+        for (int k = 1; k < D; ++k)
+            if (k == mu) om_mu = (uint32_t)P.op[k];
         uint32_t unsat = 0;
 #pragma unroll
         for (int nu = 0; nu < D; ++nu) {
