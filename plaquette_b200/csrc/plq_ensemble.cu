@@ -645,6 +645,13 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
     ce = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
     if (ce != cudaSuccess) return fail(ens_fail(ce, "stream"));
     E->descs.assign(descs, descs + n);
+    // 1. on the host: every member's geometry, decision tables and (PCG stream) jump table,
+    //    then one device arena for all states and one for all tables -- a few allocations
+    //    and one synchronisation for the whole ensemble rather than several per member
+    auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    std::vector<Tables> tables(n);
+    std::vector<std::vector<AffineHost>> jumps(n);
+    size_t state_bytes = 0, table_bytes = 0, stage_bytes = 0;
     for (int32_t m = 0; m < n; ++m) {
         const plq_chain_desc &d = descs[m];
         EnsMember mem;
@@ -659,7 +666,7 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
             if (i < d.d) ns *= d.shape[i];
         }
         a.g.n_sites = ns;
-    geom_init(a.g, d.d, d.shape);
+        geom_init(a.g, d.d, d.shape);
         mem.link = d.model == PLQ_GAUGE;
         mem.passes = mem.link ? 2 * d.d : 2;
         mem.n_vars = mem.link ? ns * d.d : ns;
@@ -677,79 +684,89 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         a.words = !(d.flags & PLQ_FLAG_GENERIC_PASS) &&
                   words_eligible(d.model, q, d.d, a.g.L, d.updater, d.rng) ? 1 : 0;
         mem.wpt = tuned_wpt(d);
-        // state (links: direction planes)
-        uint8_t *st = nullptr;
-        ce = cudaMalloc((void **)&st, (size_t)mem.n_vars);
-        if (ce != cudaSuccess) return fail(ens_fail(ce, "member state"));
-        E->allocs.push_back(st);
+        if (starts && starts[m] && first_state_at_least(starts[m], mem.n_vars, q) >= 0)
+            return fail(plq_fail(PLQ_EINVAL, "start state out of range"));
+        ModelParams p;
+        std::memset(&p, 0, sizeof p);
+        p.model = d.model;
+        p.q = q;
+        p.d = d.d;
+        p.beta = d.beta;
+        p.j = d.j;
+        p.h = d.h;
+        for (int k = 0; k < PLQ_MAX_Q; ++k) p.offsets[k] = d.offsets[k];
+        std::string err;
+        if (!build_tables(p, d.updater, d.rng, tables[m], err)) return fail(plq_fail(PLQ_EUNSUPPORTED, err));
+        const Tables &t = tables[m];
+        table_bytes += align(t.hb53.size() * 8) + align(t.hb24.size() * 4) + align(t.metro53.size() * 8) +
+                       align(t.metro24.size() * 4);
+        if (d.rng == PLQ_RNG_STREAM) {
+            uint64_t slo, shi, ilo, ihi;
+            pcg_seed_from_u64(d.seed, slo, shi, ilo, ihi);
+            build_jump_table(ilo, ihi, jumps[m]);
+            a.inc = u128{ilo, ihi};
+            u128 s0 = jump(reinterpret_cast<const Affine *>(jumps[m].data()), u128{slo, shi}, d.stream_offset);
+            a.base = pcg_step(s0, a.inc);
+            table_bytes += align(jumps[m].size() * sizeof(AffineHost));
+        }
+        state_bytes += align((size_t)mem.n_vars);
+        if (mem.link && starts && starts[m]) stage_bytes = std::max(stage_bytes, (size_t)mem.n_vars);
+        E->members.push_back(mem);
+        E->n_vars.push_back(mem.n_vars);
+        E->ts_of_member.push_back(-1);
+    }
+    uint8_t *state_arena = nullptr, *table_arena = nullptr, *stage = nullptr;
+    ce = cudaMalloc((void **)&state_arena, std::max<size_t>(state_bytes, 256));
+    if (ce == cudaSuccess) E->allocs.push_back(state_arena);
+    if (ce == cudaSuccess) ce = cudaMalloc((void **)&table_arena, std::max<size_t>(table_bytes, 256));
+    if (ce == cudaSuccess) E->allocs.push_back(table_arena);
+    if (ce == cudaSuccess && stage_bytes) ce = cudaMalloc((void **)&stage, stage_bytes);
+    if (ce != cudaSuccess) {
+        if (stage) cudaFree(stage);
+        return fail(ens_fail(ce, "ensemble arenas"));
+    }
+    // 2. the uploads, in stream order: starts (links through one staging buffer and the
+    //    plane conversion), tables and jump tables
+    size_t soff = 0, toff = 0;
+    auto put = [&](const void *host, size_t bytes) -> void * {
+        if (!bytes) return nullptr;
+        void *dst = table_arena + toff;
+        toff += align(bytes);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, E->stream);
+        return dst;
+    };
+    for (int32_t m = 0; m < n && ce == cudaSuccess; ++m) {
+        EnsMember &mem = E->members[m];
+        LocalArgs &a = mem.a;
+        uint8_t *st = state_arena + soff;
+        soff += align((size_t)mem.n_vars);
         a.state = st;
         if (starts && starts[m]) {
-            if (first_state_at_least(starts[m], mem.n_vars, q) >= 0)
-                return fail(plq_fail(PLQ_EINVAL, "start state out of range"));
             if (mem.link) {
-                uint8_t *tmp = nullptr;
-                ce = cudaMalloc((void **)&tmp, (size_t)mem.n_vars);
-                if (ce == cudaSuccess)
-                    ce = cudaMemcpyAsync(tmp, starts[m], (size_t)mem.n_vars, cudaMemcpyHostToDevice, E->stream);
-                if (ce == cudaSuccess) ce = launch_links_to_planes(tmp, st, ns, d.d, E->stream);
-                if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
-                if (tmp) cudaFree(tmp);
+                ce = cudaMemcpyAsync(stage, starts[m], (size_t)mem.n_vars, cudaMemcpyHostToDevice, E->stream);
+                if (ce == cudaSuccess) ce = launch_links_to_planes(stage, st, a.g.n_sites, a.g.d, E->stream);
             } else {
                 ce = cudaMemcpyAsync(st, starts[m], (size_t)mem.n_vars, cudaMemcpyHostToDevice, E->stream);
             }
         } else {
             ce = cudaMemsetAsync(st, 0, (size_t)mem.n_vars, E->stream);
         }
-        if (ce != cudaSuccess) return fail(ens_fail(ce, "member start"));
-        if (d.rng == PLQ_RNG_STREAM) {
-            uint64_t slo, shi, ilo, ihi;
-            pcg_seed_from_u64(d.seed, slo, shi, ilo, ihi);
-            std::vector<AffineHost> tab;
-            build_jump_table(ilo, ihi, tab);
-            a.inc = u128{ilo, ihi};
-            u128 s = jump(reinterpret_cast<const Affine *>(tab.data()), u128{slo, shi}, d.stream_offset);
-            a.base = pcg_step(s, a.inc);
-            AffineHost *dj = nullptr;
-            ce = dev_upload(E, tab.data(), tab.size(), &dj);
-            if (ce != cudaSuccess) return fail(ens_fail(ce, "jump table"));
-            a.jump = reinterpret_cast<const Affine *>(dj);
-        }
-        E->members.push_back(mem);
-        E->n_vars.push_back(mem.n_vars);
-        E->ts_of_member.push_back(-1);
-    }
-    // one table set per member at its own beta
-    for (int32_t m = 0; m < n; ++m) {
-        const plq_chain_desc &d = descs[m];
-        ModelParams p;
-        std::memset(&p, 0, sizeof p);
-        p.model = d.model;
-        p.q = d.model == PLQ_POTTS ? d.q : 2;
-        p.d = d.d;
-        p.beta = d.beta;
-        p.j = d.j;
-        p.h = d.h;
-        for (int a = 0; a < PLQ_MAX_Q; ++a) p.offsets[a] = d.offsets[a];
-        Tables t;
-        std::string err;
-        if (!build_tables(p, d.updater, d.rng, t, err)) return fail(plq_fail(PLQ_EUNSUPPORTED, err));
+        if (!jumps[m].empty()) a.jump = reinterpret_cast<const Affine *>(put(jumps[m].data(),
+                                                                             jumps[m].size() * sizeof(AffineHost)));
+        const Tables &t = tables[m];
         TableSet ts;
         std::memset(&ts, 0, sizeof ts);
-        ts.beta = d.beta;
-        uint64_t *a53 = nullptr, *b53 = nullptr;
-        uint32_t *a24 = nullptr, *b24 = nullptr;
-        ce = dev_upload(E, t.hb53.data(), t.hb53.size(), &a53);
-        if (ce == cudaSuccess) ce = dev_upload(E, t.hb24.data(), t.hb24.size(), &a24);
-        if (ce == cudaSuccess) ce = dev_upload(E, t.metro53.data(), t.metro53.size(), &b53);
-        if (ce == cudaSuccess) ce = dev_upload(E, t.metro24.data(), t.metro24.size(), &b24);
-        if (ce != cudaSuccess) return fail(ens_fail(ce, "tables"));
-        ts.hb53 = a53;
-        ts.hb24 = a24;
-        ts.metro53 = b53;
-        ts.metro24 = b24;
+        ts.beta = descs[m].beta;
+        ts.hb53 = (const uint64_t *)put(t.hb53.data(), t.hb53.size() * 8);
+        ts.hb24 = (const uint32_t *)put(t.hb24.data(), t.hb24.size() * 4);
+        ts.metro53 = (const uint64_t *)put(t.metro53.data(), t.metro53.size() * 8);
+        ts.metro24 = (const uint32_t *)put(t.metro24.data(), t.metro24.size() * 4);
         E->ts_of_member[m] = (int32_t)E->tsets.size();
         E->tsets.push_back(ts);
     }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
+    if (stage) cudaFree(stage);
+    if (ce != cudaSuccess) return fail(ens_fail(ce, "member set-up"));
     std::vector<unsigned long long> pos(n, 0);
     std::vector<long long> zeros(n, 0);
     LaunchState ls;
