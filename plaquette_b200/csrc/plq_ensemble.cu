@@ -144,6 +144,7 @@ struct EnsArgs {
     int pt_every;
     LaunchState *ls;
     Control *ctrl;
+    unsigned long long *done;  // per member: work items completed in this launch (zero between launches)
     uint64_t sweeps;
     int ranks;  // ranks per thread of a work item
 };
@@ -352,24 +353,70 @@ __device__ void swap_phase(const EnsArgs &e, unsigned long long att) {
 
 static_assert(sizeof(LocalArgs) % 4 == 0, "work items copy LocalArgs as 32-bit words");
 
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Work items per colour pass of member m (as append_items cuts them).
+__device__ __forceinline__ unsigned long long member_chunks(const EnsArgs &e, int m) {
+    const EnsMember &mem = e.members[m];
+    const long long units = mem.a.words ? mem.a.g.n_sites / 4 : mem.a.g.n_sites / 2;
+    const long long chunk = (long long)kEnsThreads * (mem.a.words ? mem.wpt : e.ranks);
+    return (unsigned long long)((units + chunk - 1) / chunk);
+}
+
+// Thread 0: wait (bounded) until every work item of member m's passes before
+// pass p of sweep t (in this launch) is complete.  The acquire makes the
+// stores of those items -- run by any CTA -- visible to this CTA's threads
+// after the next __syncthreads.
+__device__ void wait_member(const EnsArgs &e, int m, unsigned long long t, int p) {
+    const unsigned long long need = (t * (unsigned long long)e.members[m].passes + (unsigned long long)p) *
+                                    member_chunks(e, m);
+    int spins = 0;
+    while (ld_acquire_u64(&e.done[m]) < need) {
+        if (++spins > kBarrierSpin) {
+            atomicOr(&e.ctrl->status, kStatusLookbackTimeout);
+            break;
+        }
+        __nanosleep(64);
+    }
+}
+
+// The persistent launch.  A CTA takes a contiguous block of each super-phase's
+// work items (neighbouring items mostly share a member, whose arguments then
+// stay in shared memory).  There is no grid barrier between super-phases:
+// before a run of items of member m's pass p the CTA waits until the member's
+// previous passes are complete (per-member counters, released by the CTAs
+// that ran them), so a pass of one member overlaps the tails of every other
+// member's passes.  Every wait is on items of an earlier super-phase and all
+// CTAs are resident (cooperative launch), so the waits always end.  Grid
+// barriers remain around the tempering phase and at the end of the launch.
 template <int R, bool WORDS_ONLY>
 __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
     for (unsigned long long t = 0; t < e.sweeps; ++t) {
         for (int sp = 0; sp < e.n_sp; ++sp) {
-            // a contiguous block of the super-phase's items per CTA: neighbouring items
-            // mostly share a member, so its arguments stay in shared memory
             const int64_t b0 = e.sp_begin[sp], b1 = e.sp_begin[sp + 1];
             const int64_t per = (b1 - b0 + gridDim.x - 1) / gridDim.x;
             const int64_t lo = b0 + (int64_t)blockIdx.x * per;
             const int64_t hi = lo + per < b1 ? lo + per : b1;
             int last_m = -1;  // the arguments in shared memory (a member has one pass per super-phase)
+            unsigned long long run = 0;  // items of member last_m done in this run
             for (int64_t i = lo; i < hi; ++i) {
                 int m = e.item_member[i];
                 if (m != last_m) {
-                    // the member's arguments into shared memory, one 32-bit word per thread, then
-                    // the pass-specific fields
-                    __syncthreads();  // every thread is done with the previous member's arguments
+                    __syncthreads();  // every thread is done with the previous run's items and arguments
+                    if (threadIdx.x == 0) {
+                        if (last_m >= 0) {  // release them
+                            __threadfence();
+                            atomicAdd(&e.done[last_m], run);
+                        }
+                        wait_member(e, m, t, e.item_pass[i]);
+                    }
+                    // the member's arguments into shared memory, one 32-bit word per thread,
+                    // then the pass-specific fields
                     const uint32_t *src = reinterpret_cast<const uint32_t *>(&e.members[m].a);
                     uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
                     for (int k = threadIdx.x; k < (int)(sizeof(LocalArgs) / 4); k += blockDim.x) dst[k] = src[k];
@@ -377,19 +424,29 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
                     if (threadIdx.x == 0) item_pass_fields(e, m, e.item_pass[i], t, sa);
                     __syncthreads();
                     last_m = m;
+                    run = 0;
                 }
                 run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i], e.members[m].wpt);
+                ++run;
             }
-            grid_barrier(e);
+            if (last_m >= 0) {
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    __threadfence();
+                    atomicAdd(&e.done[last_m], run);
+                }
+            }
         }
-        const unsigned long long done = e.ls->sweep + t + 1;
-        if (e.n_ladders && e.pt_every > 0 && done % (unsigned long long)e.pt_every == 0) {
-            if (blockIdx.x == 0)
-                for (int m = threadIdx.x; m < e.n_members; m += blockDim.x) e.energy[m] = 0;
-            grid_barrier(e);
+        const unsigned long long swept = e.ls->sweep + t + 1;
+        if (e.n_ladders && e.pt_every > 0 && swept % (unsigned long long)e.pt_every == 0) {
+            grid_barrier(e);  // every member's sweeps complete
             energy_phase(e);
             grid_barrier(e);
-            if (blockIdx.x == 0) swap_phase(e, e.ls->pt_attempts + done / (unsigned long long)e.pt_every - 1);
+            if (blockIdx.x == 0) {
+                swap_phase(e, e.ls->pt_attempts + swept / (unsigned long long)e.pt_every - 1);
+                __syncthreads();
+                for (int m = threadIdx.x; m < e.n_members; m += blockDim.x) e.energy[m] = 0;  // for the next phase
+            }
             grid_barrier(e);
         }
     }
@@ -399,6 +456,7 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
         for (int m = threadIdx.x; m < e.n_members; m += blockDim.x) {
             if (e.members[m].a.jump) e.pos[m] += e.sweeps * (unsigned long long)e.members[m].n_vars;
             if (e.msweep) e.msweep[m] += e.sweeps;
+            e.done[m] = 0;
         }
         __syncthreads();
         if (threadIdx.x == 0) e.ls->sweep += e.sweeps;
@@ -437,6 +495,7 @@ struct plq_ensemble {
     TableSet *d_tsets = nullptr;
     int32_t *d_ts = nullptr;
     unsigned long long *d_pos = nullptr;
+    unsigned long long *d_done = nullptr;  // per-member work-item counters of the persistent launch
     long long *d_energy = nullptr;
     LadderDev *d_ladders = nullptr;
     LaunchState *d_ls = nullptr;
@@ -569,6 +628,7 @@ EnsArgs ens_args(plq_ensemble *E, uint64_t sweeps) {
     a.tsets = E->d_tsets;
     a.ts_of_member = E->d_ts;
     a.pos = E->d_pos;
+    a.done = E->d_done;
     a.item_member = E->d_item_member;
     a.item_chunk = E->d_item_chunk;
     a.item_pass = E->d_item_pass;
@@ -779,6 +839,7 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
     if (ce == cudaSuccess) ce = dev_upload(E, E->tsets.data(), E->tsets.size(), &E->d_tsets);
     if (ce == cudaSuccess) ce = dev_upload(E, E->ts_of_member.data(), E->ts_of_member.size(), &E->d_ts);
     if (ce == cudaSuccess) ce = dev_upload(E, pos.data(), pos.size(), &E->d_pos);
+    if (ce == cudaSuccess) ce = dev_upload(E, pos.data(), pos.size(), &E->d_done);  // zeros
     if (ce == cudaSuccess) ce = dev_upload(E, zeros.data(), zeros.size(), &E->d_energy);
     if (ce == cudaSuccess) ce = dev_upload(E, &ls, 1, &E->d_ls);
     if (ce == cudaSuccess) ce = dev_upload(E, &ctrl, 1, &E->d_ctrl);
@@ -990,6 +1051,8 @@ extern "C" int plq_ensemble_advance_unbatched(plq_ensemble *E, uint64_t sweeps) 
                 }
             swap_kernel<<<1, kEnsThreads, 0, E->stream>>>(ea, ls.pt_attempts + done / E->pt_every - 1);
             E->launches++;
+            // energies start every phase at zero (the persistent launch relies on it too)
+            cudaMemsetAsync(E->d_energy, 0, sizeof(long long) * E->members.size(), E->stream);
             e = cudaMemcpyAsync(ts.data(), E->d_ts, ts.size() * sizeof(ts[0]), cudaMemcpyDeviceToHost, E->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
             if (e != cudaSuccess) return ens_fail(e, "unbatched swaps");
@@ -1570,7 +1633,7 @@ struct TickBuffers {
     EnsMember *members = nullptr;
     TableSet *tsets = nullptr;
     int32_t *ts = nullptr;
-    unsigned long long *pos = nullptr, *msweep = nullptr;
+    unsigned long long *pos = nullptr, *msweep = nullptr, *done = nullptr;
     int32_t *im = nullptr, *ic = nullptr;
     int8_t *ip = nullptr;
     int64_t *spb = nullptr;
@@ -1578,7 +1641,7 @@ struct TickBuffers {
     Control *ctrl = nullptr;
     size_t cap_members = 0, cap_items = 0;
     void release() {
-        void *ps[] = {members, tsets, ts, pos, msweep, im, ic, ip, spb, ls, ctrl};
+        void *ps[] = {members, tsets, ts, pos, msweep, done, im, ic, ip, spb, ls, ctrl};
         for (void *p : ps)
             if (p) cudaFree(p);
         *this = TickBuffers();
@@ -1631,12 +1694,15 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         cudaFree(B.ts);
         cudaFree(B.pos);
         cudaFree(B.msweep);
+        cudaFree(B.done);
         size_t c = std::max<size_t>(n, 2 * B.cap_members);
         e = cudaMalloc((void **)&B.members, c * sizeof(EnsMember));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B.tsets, c * sizeof(TableSet));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B.ts, c * sizeof(int32_t));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B.pos, c * sizeof(unsigned long long));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B.msweep, c * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B.done, c * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemsetAsync(B.done, 0, c * sizeof(unsigned long long), stream);
         B.cap_members = c;
     }
     if (e == cudaSuccess && B.cap_items < im.size() + 1) {
@@ -1676,6 +1742,7 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         a.ts_of_member = B.ts + lo;
         a.pos = B.pos + lo;
         a.msweep = B.msweep + lo;
+        a.done = B.done + lo;
         a.item_member = B.im;
         a.item_chunk = B.ic;
         a.item_pass = B.ip;

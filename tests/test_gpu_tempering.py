@@ -122,17 +122,19 @@ def test_tempering_equals_host_replay(gpu, oracle, batched):
 
 
 def test_a_favourable_swap_is_always_taken(gpu, oracle):
-    """A cold lattice at the low beta and a random one at the high beta:
-    (b_0 - b_1)(E_0 - E_1) > 0, so the first attempt must swap them (a sign
-    error in the rule would keep them, exp of a large negative number)."""
-    specs = [(plq.ISING, (16, 16, 16), plq.METROPOLIS, 0.1, 61, 1.0),
-             (plq.ISING, (16, 16, 16), plq.METROPOLIS, 0.5, 62, 1.0)]
-    ladders = [([0, 1], [0.1, 0.5], 5)]
+    """Both betas in the ordered phase: after one sweep the cold lattice at
+    the lower beta (0.3) still has by far the lower energy (bond sum ~ 10900
+    of 12288 against ~ 4300 for the random one at 0.4), so
+    (b_0 - b_1)(E_0 - E_1) ~ +600 > 0 and the first attempt must swap them
+    (a sign error in the rule would keep them: exp(-600) is 0)."""
+    specs = [(plq.ISING, (16, 16, 16), plq.METROPOLIS, 0.3, 61, 1.0),
+             (plq.ISING, (16, 16, 16), plq.METROPOLIS, 0.4, 62, 1.0)]
+    ladders = [([0, 1], [0.3, 0.4], 5)]
     descs, starts, replay = _build(gpu, oracle, specs, ladders, cold=(0,))
     ens = Ensemble(gpu, descs, starts)
-    ens.add_ladder([0, 1], [0.1, 0.5], 1, seed=5)
+    ens.add_ladder([0, 1], [0.3, 0.4], 1, seed=5)
     ens.advance(1)
     replay.advance(1, 1)
     assert replay.accepted == 1
-    assert list(ens.betas()) == [0.5, 0.1]
+    assert list(ens.betas()) == [0.4, 0.3]
     assert np.array_equal(ens.betas(), replay.beta)
