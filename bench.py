@@ -698,7 +698,9 @@ def measure_cluster(name, steps, warmup, ctx, e2e=True):
     launches0 = chain.launches
     t_wall0 = time.time()
     ev0.record(stream)
+    nvtx_push("timed")
     chain.advance(steps * per_step)
+    nvtx_pop()
     ev1.record(stream)
     ev1.synchronize()
     t_wall1 = time.time()
