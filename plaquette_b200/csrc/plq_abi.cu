@@ -237,7 +237,7 @@ void chain_free(plq_chain *c) {
     cluster_free(c);
     void *ptrs[] = {c->d_state, c->d_state_alt, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
                     c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs, c->d_loop_bits,
-                    c->d_meas, c->d_pairs, c->d_hb53_fused, c->d_h1};
+                    c->d_meas, c->d_pairs, c->d_hb53_fused};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -413,14 +413,6 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
             c->fused_tz = fused3d_default_tz(c->g.L[2]);
             e = cudaMalloc((void **)&c->d_state_alt, (size_t)c->n_vars);
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(state_alt)"));
-            if (desc->rng == PLQ_RNG_KEYED) {
-                // the first of keyed_uniform's two hashes depends on the site alone: computed
-                // once here, each draw of a sweep then costs one hash and a 4-byte read
-                e = cudaMalloc((void **)&c->d_h1, sizeof(uint32_t) * (size_t)n);
-                if (e == cudaSuccess) e = launch_fused3d_h1(c->d_h1, c->seed32, c->g.L[0], c->g.L[1], c->g.L[2], c->stream);
-                if (e != cudaSuccess) return fail(cuda_fail(e, "first keyed hashes"));
-                c->launches++;
-            }
             for (int k = 0; k < 2; ++k) {
                 c->fused_map_buf[k] = k ? c->d_state_alt : c->d_state;
                 e = fused3d_make_maps(c->fused_map_buf[k], c->g.L[0], c->g.L[1], c->g.L[2], &c->fused_maps[k]);
@@ -509,7 +501,6 @@ static int fused_sweep(plq_chain *c) {
     }
     f.seed32 = c->seed32;
     f.sweep32 = (uint32_t)c->sweeps_done;
-    f.h1 = c->d_h1;
     if (stream) {
         f.jump = c->d_jump;
         f.base = c->base;

@@ -58,7 +58,6 @@ struct plq_chain {
     uint8_t *d_io = nullptr;     // host-order staging on the device
     uint64_t *d_hb53 = nullptr, *d_metro53 = nullptr;
     uint64_t *d_hb53_fused = nullptr;  // stream heat-bath cut points << 11 (the fused sweep's table)
-    uint32_t *d_h1 = nullptr;  // keyed fused sweep: every site's first keyed hash (colour-major)
     uint32_t *d_hb24 = nullptr, *d_metro24 = nullptr;
     int32_t pw[64];
     plq::Affine *d_jump = nullptr;

@@ -139,11 +139,10 @@ __device__ __forceinline__ uint32_t decide(const uint8_t *tab, uint32_t key, uin
 
 // Updates the colour-c sites (byte offsets b, b+2) of one 32-bit word in place:
 // the word and its keys are shifted by b bytes once, so both sites sit at fixed
-// byte offsets 0 and 2.  PRE: h0, h1 are the two sites' precomputed first hashes
-// (keyed_uniform = lowbias32(first ^ sweep * golden) >> 8).
-template <int Q, bool STREAM, bool HB, bool PRE>
+// byte offsets 0 and 2.
+template <int Q, bool STREAM, bool HB>
 __device__ __forceinline__ uint32_t update_word(const FusedArgs &a, const uint8_t *tab, uint32_t C, uint32_t K,
-                                                int b, uint32_t var0, u128 &st, uint32_t h0 = 0, uint32_t h1 = 0) {
+                                                int b, uint32_t var0, u128 &st) {
     const uint32_t sh = 8u * (uint32_t)b;
     const uint32_t Cs = C >> sh, Ks = K >> sh;
     uint32_t delta = 0;
@@ -155,8 +154,6 @@ __device__ __forceinline__ uint32_t update_word(const FusedArgs &a, const uint8_
         if (STREAM) {
             k = xsl_rr(st);  // all 64 bits: the table holds the 53-bit cut points << 11
             st = pcg_step(st, a.inc);
-        } else if (PRE) {
-            k = lowbias32((i ? h1 : h0) ^ (a.sweep32 * 0x9e3779b9u)) >> 8;
         } else {
             k = keyed24(a.seed32, var0 + (uint32_t)(b + 2 * i), a.sweep32);
         }
@@ -167,17 +164,11 @@ __device__ __forceinline__ uint32_t update_word(const FusedArgs &a, const uint8_
 }
 
 // A run of 16 bytes at x offset xr of smem row `row` (plane c, neighbours in
-// planes m and p); rows are L0 bytes, x wraps.  PRE: hp points at the first
-// hashes of the run's 8 sites of the pass's colour (32-byte aligned).
-template <int Q, bool STREAM, bool HB, bool PRE>
+// planes m and p); rows are L0 bytes, x wraps.
+template <int Q, bool STREAM, bool HB>
 __device__ __forceinline__ uint4 update_run(const FusedArgs &a, const uint8_t *tab, const uint8_t *pc,
                                             const uint8_t *pm, const uint8_t *pp, int row, int xr, int L0,
-                                            int b, uint32_t var0, u128 &st, const uint32_t *hp = nullptr) {
-    uint4 H0 = make_uint4(0, 0, 0, 0), H1 = make_uint4(0, 0, 0, 0);
-    if (PRE) {
-        H0 = __ldg(reinterpret_cast<const uint4 *>(hp));
-        H1 = __ldg(reinterpret_cast<const uint4 *>(hp) + 1);
-    }
+                                            int b, uint32_t var0, u128 &st) {
     const int off = row * L0 + xr;
     uint4 C = *reinterpret_cast<const uint4 *>(pc + off);
     uint4 U = *reinterpret_cast<const uint4 *>(pc + off - L0);
@@ -191,14 +182,14 @@ __device__ __forceinline__ uint4 update_run(const FusedArgs &a, const uint8_t *t
     uint32_t K2 = key_word<Q>(C.z, __funnelshift_l(C.y, C.z, 8), __funnelshift_r(C.z, C.w, 8), U.z, D.z, M.z, P.z);
     uint32_t K3 = key_word<Q>(C.w, __funnelshift_l(C.z, C.w, 8), __funnelshift_r(C.w, Rw, 8), U.w, D.w, M.w, P.w);
     uint4 O;
-    O.x = update_word<Q, STREAM, HB, PRE>(a, tab, C.x, K0, b, var0, st, H0.x, H0.y);
-    O.y = update_word<Q, STREAM, HB, PRE>(a, tab, C.y, K1, b, var0 + 4, st, H0.z, H0.w);
-    O.z = update_word<Q, STREAM, HB, PRE>(a, tab, C.z, K2, b, var0 + 8, st, H1.x, H1.y);
-    O.w = update_word<Q, STREAM, HB, PRE>(a, tab, C.w, K3, b, var0 + 12, st, H1.z, H1.w);
+    O.x = update_word<Q, STREAM, HB>(a, tab, C.x, K0, b, var0, st);
+    O.y = update_word<Q, STREAM, HB>(a, tab, C.y, K1, b, var0 + 4, st);
+    O.z = update_word<Q, STREAM, HB>(a, tab, C.z, K2, b, var0 + 8, st);
+    O.w = update_word<Q, STREAM, HB>(a, tab, C.w, K3, b, var0 + 12, st);
     return O;
 }
 
-template <int Q, bool STREAM, bool HB, bool PRE>
+template <int Q, bool STREAM, bool HB>
 __global__ void __launch_bounds__(FTHREADS, FusedCfg<Q, STREAM>::ctas)
     fused3d_kernel(const FusedArgs a, const __grid_constant__ CUtensorMap tm_rows,
                    const __grid_constant__ CUtensorMap tm_halo) {
@@ -306,9 +297,8 @@ __global__ void __launch_bounds__(FTHREADS, FusedCfg<Q, STREAM>::ctas)
 #pragma unroll
         for (int k = 0; k < FRUNS_PER_THREAD; ++k) {
             u128 st = st0[k];
-            const size_t site0 = zoff1 + (size_t)rgy[k] * L0 + rx[k];
-            out0[k] = update_run<Q, STREAM, HB, PRE>(a, tab, sC, sM, sP, rrow[k], rx[k], L0, (rgy[k] + gz1) & 1,
-                                                     (uint32_t)site0, st, PRE ? a.h1 + (site0 >> 1) : nullptr);
+            out0[k] = update_run<Q, STREAM, HB>(a, tab, sC, sM, sP, rrow[k], rx[k], L0, (rgy[k] + gz1) & 1,
+                                                (uint32_t)(zoff1 + (size_t)rgy[k] * L0 + rx[k]), st);
         }
         uint32_t outR = 0;
         if (has_ring) {
@@ -322,11 +312,8 @@ __global__ void __launch_bounds__(FTHREADS, FusedCfg<Q, STREAM>::ctas)
                                      *reinterpret_cast<const uint32_t *>(sM + off),
                                      *reinterpret_cast<const uint32_t *>(sP + off));
             u128 st = stR;
-            const size_t site0 = zoff1 + (size_t)ring_gy * L0 + ring_x;
-            uint2 HR = make_uint2(0, 0);
-            if (PRE) HR = __ldg(reinterpret_cast<const uint2 *>(a.h1 + (site0 >> 1)));
-            outR = update_word<Q, STREAM, HB, PRE>(a, tab, C, K, (ring_gy + gz1) & 1, (uint32_t)site0, st, HR.x,
-                                                   HR.y);
+            outR = update_word<Q, STREAM, HB>(a, tab, C, K, (ring_gy + gz1) & 1,
+                                              (uint32_t)(zoff1 + (size_t)ring_gy * L0 + ring_x), st);
         }
         __syncthreads();  // all colour-0 inputs read; publish
 #pragma unroll
@@ -349,11 +336,8 @@ __global__ void __launch_bounds__(FTHREADS, FusedCfg<Q, STREAM>::ctas)
                                  ? jump(a.jump, a.base, a.off1 + ((zoff0 + (size_t)rgy[k] * L0 + rx[k]) >> 1))
                                  : apply(a.plane, st1[k]);
                 u128 st = st1[k];
-                const size_t site0 = zoff0 + (size_t)rgy[k] * L0 + rx[k];
-                out1[k] = update_run<Q, STREAM, HB, PRE>(a, tab, sM, zM, sC, rrow[k], rx[k], L0,
-                                                         (rgy[k] + gz0 + 1) & 1, (uint32_t)site0, st,
-                                                         PRE ? a.h1 + plane_sites * (size_t)L2 / 2 + (site0 >> 1)
-                                                             : nullptr);
+                out1[k] = update_run<Q, STREAM, HB>(a, tab, sM, zM, sC, rrow[k], rx[k], L0, (rgy[k] + gz0 + 1) & 1,
+                                                    (uint32_t)(zoff0 + (size_t)rgy[k] * L0 + rx[k]), st);
             }
 #pragma unroll
             for (int k = 0; k < FRUNS_PER_THREAD; ++k)
@@ -420,9 +404,9 @@ cudaError_t fused3d_make_maps(const uint8_t *buf, int L0, int L1, int L2, FusedM
     return cudaSuccess;
 }
 
-template <int Q, bool STREAM, bool HB, bool PRE>
+template <int Q, bool STREAM, bool HB>
 static cudaError_t launch_t(FusedArgs a, const FusedMaps &m, cudaStream_t s) {
-    auto kern = fused3d_kernel<Q, STREAM, HB, PRE>;
+    auto kern = fused3d_kernel<Q, STREAM, HB>;
     size_t smem = fused3d_smem_bytes(a.L0, FusedCfg<Q, STREAM>::slots);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -433,42 +417,12 @@ static cudaError_t launch_t(FusedArgs a, const FusedMaps &m, cudaStream_t s) {
 }
 
 cudaError_t launch_fused3d(const FusedArgs &a, const FusedMaps &m, int q, bool stream, bool hb, cudaStream_t s) {
-    const bool pre = !stream && a.h1 != nullptr;
     if (q == 2) {
-        if (hb) {
-            if (stream) return launch_t<2, true, true, false>(a, m, s);
-            return pre ? launch_t<2, false, true, true>(a, m, s) : launch_t<2, false, true, false>(a, m, s);
-        }
-        return pre ? launch_t<2, false, false, true>(a, m, s) : launch_t<2, false, false, false>(a, m, s);
+        if (hb) return stream ? launch_t<2, true, true>(a, m, s) : launch_t<2, false, true>(a, m, s);
+        return launch_t<2, false, false>(a, m, s);
     }
-    if (q == 3 && hb) {
-        if (stream) return launch_t<3, true, true, false>(a, m, s);
-        return pre ? launch_t<3, false, true, true>(a, m, s) : launch_t<3, false, true, false>(a, m, s);
-    }
+    if (q == 3 && hb) return stream ? launch_t<3, true, true>(a, m, s) : launch_t<3, false, true>(a, m, s);
     return cudaErrorInvalidValue;
-}
-
-// h1[parity(s) * n/2 + s/2] = lowbias32(seed32 ^ s): one thread per 4 sites of a row.
-__global__ void fused_h1_kernel(uint32_t *h1, uint32_t seed32, int L0, int L1, uint32_t n) {
-    const uint32_t half = n / 2;
-    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < n / 4; w += gridDim.x * blockDim.x) {
-        const uint32_t s0 = 4u * w;
-        const uint32_t row = s0 / (uint32_t)L0;  // (z * L1 + y); x0 = s0 - row * L0
-        const uint32_t y = row % (uint32_t)L1, z = row / (uint32_t)L1;
-        const uint32_t x0 = s0 - row * (uint32_t)L0;
-#pragma unroll
-        for (uint32_t i = 0; i < 4; ++i) {
-            const uint32_t s = s0 + i;
-            const uint32_t par = (x0 + i + y + z) & 1u;
-            h1[par * half + (s >> 1)] = lowbias32(seed32 ^ s);
-        }
-    }
-}
-
-cudaError_t launch_fused3d_h1(uint32_t *h1, uint32_t seed32, int L0, int L1, int L2, cudaStream_t s) {
-    const uint32_t n = (uint32_t)L0 * (uint32_t)L1 * (uint32_t)L2;
-    fused_h1_kernel<<<148 * 8, 256, 0, s>>>(h1, seed32, L0, L1, n);
-    return cudaGetLastError();
 }
 
 }  // namespace plq

@@ -15,10 +15,6 @@ struct FusedArgs {
     const void *table;   // decision table in global memory (copied to smem)
     int table_words;     // its size in 32-bit words
     uint32_t seed32, sweep32;
-    // keyed stream: lowbias32(seed32 ^ site) of every site, the sweep-independent first
-    // hash of keyed_uniform, colour-major: site s at [parity(s) * n/2 + s/2]; null to
-    // compute both hashes per draw
-    const uint32_t *h1;
     const Affine *jump;  // PCG stream (null on the keyed stream)
     u128 base, inc;
     uint64_t off0, off1; // stream positions of rank 0 of colours 0 and 1
@@ -41,7 +37,5 @@ size_t fused3d_smem_bytes(int L0, int slots);
 int fused3d_table_limit_bytes();
 cudaError_t fused3d_make_maps(const uint8_t *buf, int L0, int L1, int L2, FusedMaps *out);
 cudaError_t launch_fused3d(const FusedArgs &a, const FusedMaps &maps, int q, bool stream, bool hb, cudaStream_t s);
-// Fills the first-hash array of a keyed fused chain (FusedArgs::h1).
-cudaError_t launch_fused3d_h1(uint32_t *h1, uint32_t seed32, int L0, int L1, int L2, cudaStream_t s);
 
 }  // namespace plq
