@@ -67,7 +67,7 @@ struct EnsMember {
     int64_t n_vars;
     int wpt;           // four-site body: words per thread of a work item (the tuned shape)
     int pad_;
-    int64_t reserved_;
+    uint32_t *pk;      // packed Z2 links (one 32-bit row of L0 links per word, d planes), or null
     double j;
     int ladder;
 };
@@ -233,6 +233,143 @@ __device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk, int
     }
 }
 
+// ---- Z2 gauge members with L0 <= 32 on the keyed stream: links bit-packed by rows.
+// Inside a persistent launch such a member's links live in pk: word dir * rows + r
+// holds bit x = U_dir(x, r) for row r (the site index over directions >= 1).  A
+// work item takes rows of one (direction mu, parity) pass: the six staples of
+// every link of a row come out of XORs of whole row words (a shift along
+// direction 0 is a rotation of the row, along the others another row), their
+// count of unsatisfied staples out of a bit-sliced counter, and each link of
+// the pass's parity then decides exactly as the byte body does -- the same key
+// cur + 4(d-1) - 2 * unsatisfied, the same keyed draw of variable site * d + mu,
+// the same table -- so results are bit-identical.  The launch packs the bytes
+// first and unpacks them at its end (pack_links_kernel).
+
+__device__ __forceinline__ uint32_t row_xp(uint32_t w, uint32_t L0, uint32_t full) {  // bit x <- bit x+1
+    return ((w >> 1) | (w << (L0 - 1))) & full;
+}
+__device__ __forceinline__ uint32_t row_xm(uint32_t w, uint32_t L0, uint32_t full) {  // bit x <- bit x-1
+    return ((w << 1) | (w >> (L0 - 1))) & full;
+}
+// bit-sliced counter (c2 c1 c0) += v, per bit position (counts stay below 8)
+__device__ __forceinline__ void count_add(uint32_t &c0, uint32_t &c1, uint32_t &c2, uint32_t v) {
+    const uint32_t k0 = c0 & v;
+    c0 ^= v;
+    c2 |= c1 & k0;
+    c1 ^= k0;
+}
+
+template <int D>
+__device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk, int R) {
+    const uint32_t L0 = (uint32_t)a.g.L[0];
+    const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
+    const int mu = a.dir;
+    const uint32_t full = L0 == 32 ? 0xFFFFFFFFu : ((1u << L0) - 1u);
+    const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
+    const bool hb = a.kernel == PLQ_HEATBATH;
+    const uint32_t sweep_mix = a.sweep32 * 0x9e3779b9u;
+#pragma unroll 1
+    for (int i = 0; i < R; ++i) {
+        const uint32_t r = r0 + (uint32_t)i;
+        if (r >= rows) break;
+        int32_t op[4] = {0, 0, 0, 0}, om[4] = {0, 0, 0, 0};
+        uint32_t rr = r;
+        int par = 0;
+#pragma unroll
+        for (int k = 1; k < D; ++k) {
+            const uint32_t q = fdiv(rr, a.g.dm[k], a.g.dl[k]);
+            const int32_t c = (int32_t)(rr - q * (uint32_t)a.g.L[k]);
+            rr = q;
+            par += c;
+            const int32_t rs = (int32_t)(a.g.stride[k] / (int64_t)L0);
+            op[k] = c + 1 < a.g.L[k] ? rs : -(a.g.L[k] - 1) * rs;
+            om[k] = c > 0 ? -rs : (a.g.L[k] - 1) * rs;
+        }
+        int32_t op_mu = 0;
+#pragma unroll
+        for (int k = 1; k < D; ++k)
+            if (k == mu) op_mu = op[k];
+        const uint32_t Umu = pk[(uint32_t)mu * rows + r];
+        uint32_t c0 = 0, c1 = 0, c2 = 0;  // unsatisfied staples per link
+#pragma unroll
+        for (int nu = 0; nu < D; ++nu) {
+            if (nu == mu) continue;
+            const uint32_t *Pnu = pk + (uint32_t)nu * rows;
+            const uint32_t *Pmu = pk + (uint32_t)mu * rows;
+            // forward: U_nu(s+mu) U_mu(s+nu) U_nu(s)
+            const uint32_t nu_s = Pnu[r];
+            const uint32_t nu_smu = mu == 0 ? row_xp(nu_s, L0, full) : Pnu[r + (uint32_t)op_mu];
+            const uint32_t mu_snu = nu == 0 ? row_xp(Umu, L0, full) : Pmu[r + (uint32_t)op[nu]];
+            count_add(c0, c1, c2, nu_smu ^ mu_snu ^ nu_s);
+            // backward: U_nu(s+mu-nu) U_mu(s-nu) U_nu(s-nu)
+            uint32_t nu_smn, mu_smn, nu_smumn;
+            if (nu == 0) {
+                nu_smn = row_xm(nu_s, L0, full);
+                mu_smn = row_xm(Umu, L0, full);
+                nu_smumn = row_xm(nu_smu, L0, full);
+            } else {
+                nu_smn = Pnu[r + (uint32_t)om[nu]];
+                mu_smn = Pmu[r + (uint32_t)om[nu]];
+                nu_smumn = mu == 0 ? row_xp(nu_smn, L0, full) : Pnu[r + (uint32_t)op_mu + (uint32_t)om[nu]];
+            }
+            count_add(c0, c1, c2, nu_smumn ^ mu_smn ^ nu_smn);
+        }
+        // the links of the pass's parity: x with (x + par) % 2 == colour
+        const uint32_t x0 = (uint32_t)((a.color ^ par) & 1);
+        uint32_t flip = 0;
+        const uint32_t var_row = r * L0 * (uint32_t)D + (uint32_t)mu;
+#pragma unroll 1
+        for (uint32_t x = x0; x < L0; x += 2) {
+            const uint32_t cur = (Umu >> x) & 1u;
+            const uint32_t uns = ((c0 >> x) & 1u) | (((c1 >> x) & 1u) << 1) | (((c2 >> x) & 1u) << 2);
+            const uint32_t key = cur + 4u * (uint32_t)(D - 1) - 2u * uns;
+            const uint32_t k = lowbias32(lowbias32(a.seed32 ^ (var_row + x * (uint32_t)D)) ^ sweep_mix) >> 8;
+            uint32_t nv;
+            if (hb) {
+                nv = a.hb24[key] <= k ? 1u : 0u;
+            } else {
+                const uint32_t e = a.metro24[key];
+                nv = (e == 0xFFFFFFFFu || k < e) ? 1u - cur : cur;
+            }
+            flip |= (nv ^ cur) << x;
+        }
+        pk[(uint32_t)mu * rows + r] = Umu ^ flip;
+    }
+}
+
+// Packing entry of one member: its rows of all d directions occupy
+// [first, first + d * rows) of the launch's packing index space.
+struct PackEntry {
+    uint8_t *state;   // byte planes (dir * n_sites + site)
+    uint32_t *pk;
+    uint32_t first;   // first index of this member
+    uint32_t L0;
+};
+
+// Bytes to bits (unpack = false) or back (unpack = true) for every packed
+// member of the launch: one thread per row of one direction.
+__global__ void pack_links_kernel(const PackEntry *tab, int n_tab, uint32_t total, bool unpack) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_tab - 1;
+        while (lo < hi) {  // the entry holding g
+            const int mid = (lo + hi + 1) / 2;
+            if (tab[mid].first <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const PackEntry &t = tab[lo];
+        const uint32_t idx = g - t.first;  // dir * rows + row: its bytes start at idx * L0
+        uint8_t *bytes = t.state + (size_t)idx * t.L0;
+        if (!unpack) {
+            uint32_t w = 0;
+            for (uint32_t x = 0; x < t.L0; ++x) w |= (uint32_t)(bytes[x] & 1u) << x;
+            t.pk[idx] = w;
+        } else {
+            const uint32_t w = t.pk[idx];
+            for (uint32_t x = 0; x < t.L0; ++x) bytes[x] = (uint8_t)((w >> x) & 1u);
+        }
+    }
+}
+
 // The pass-specific fields of member m's arguments (already copied into sa)
 // for colour pass `sp` of sweep index `sweep`.
 __device__ void item_pass_fields(const EnsArgs &e, int m, int sp, unsigned long long sweep_in_launch, LocalArgs &sa) {
@@ -362,8 +499,9 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 // Work items per colour pass of member m (as append_items cuts them).
 __device__ __forceinline__ unsigned long long member_chunks(const EnsArgs &e, int m) {
     const EnsMember &mem = e.members[m];
-    const long long units = mem.a.words ? mem.a.g.n_sites / 4 : mem.a.g.n_sites / 2;
-    const long long chunk = (long long)kEnsThreads * (mem.a.words ? mem.wpt : e.ranks);
+    const long long units = mem.pk ? mem.a.g.n_sites / mem.a.g.L[0]
+                                   : (mem.a.words ? mem.a.g.n_sites / 4 : mem.a.g.n_sites / 2);
+    const long long chunk = (long long)kEnsThreads * (mem.pk || mem.a.words ? mem.wpt : e.ranks);
     return (unsigned long long)((units + chunk - 1) / chunk);
 }
 
@@ -426,7 +564,16 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
                     last_m = m;
                     run = 0;
                 }
-                run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i], e.members[m].wpt);
+                if (e.members[m].pk) {
+                    switch (sa.g.d) {
+                        case 2: packed_link_item<2>(sa, e.members[m].pk, e.item_chunk[i], e.members[m].wpt); break;
+                        case 3: packed_link_item<3>(sa, e.members[m].pk, e.item_chunk[i], e.members[m].wpt); break;
+                        case 4: packed_link_item<4>(sa, e.members[m].pk, e.item_chunk[i], e.members[m].wpt); break;
+                        default: break;
+                    }
+                } else {
+                    run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i], e.members[m].wpt);
+                }
                 ++run;
             }
             if (last_m >= 0) {
@@ -517,6 +664,10 @@ struct plq_ensemble {
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_sweeps = 0;
     int graph_ranks = 0, graph_ctas = 0;
+    // packed Z2 members: their packing table (device) and its index space
+    PackEntry *d_pack = nullptr;
+    int n_pack = 0;
+    uint32_t pack_total = 0;
     // every member's primaries: one device buffer, the launches captured once
     long long *d_prims_all = nullptr;
     std::vector<int64_t> prims_offset;  // member m's first entry
@@ -565,8 +716,10 @@ int append_items(const EnsMember *mems, const std::vector<size_t> &ids, size_t l
         for (size_t m : ids) {
             const int P = mems[m].passes;
             const LocalArgs &ma = mems[m].a;
-            const int64_t chunk = (int64_t)kEnsThreads * (ma.words ? mems[m].wpt : ranks);
-            const int64_t units = ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2;
+            // work per item: 256 * ranks colour ranks, or 256 * wpt four-site words or packed rows
+            const bool shaped = ma.words || mems[m].pk;
+            const int64_t chunk = (int64_t)kEnsThreads * (shaped ? mems[m].wpt : ranks);
+            const int64_t units = mems[m].pk ? ma.g.n_sites / ma.g.L[0] : (ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2);
             const int64_t nc = (units + chunk - 1) / chunk;
             for (int p = 0; p < P; ++p) {
                 const int p0 = p * S / P, p1 = (p + 1) * S / P;
@@ -667,12 +820,63 @@ int max_ctas_per_sm(int ranks, bool words_only) {
     return n;
 }
 
-cudaError_t launch_persistent(plq_ensemble *E, uint64_t sweeps) {
-    EnsArgs a = ens_args(E, sweeps);
+// One persistent launch with arguments `a`: packed Z2 members are packed before
+// and unpacked after it, so outside a launch every member is in byte planes.
+cudaError_t launch_ensemble(plq_ensemble *E, EnsArgs &a) {
+    const unsigned pack_blocks = (unsigned)std::min<uint32_t>((E->pack_total + 255) / 256, 148u * 8u);
+    cudaError_t e = cudaSuccess;
+    if (E->n_pack) {
+        pack_links_kernel<<<pack_blocks, 256, 0, E->stream>>>(E->d_pack, E->n_pack, E->pack_total, false);
+        e = cudaGetLastError();
+    }
     void *params[] = {&a};
     dim3 grid((unsigned)(E->ctx->sm_count * E->ctas_per_sm));
-    return cudaLaunchCooperativeKernel(kernel_ptr(E->ranks, E->words_only), grid, dim3(kEnsThreads), params, 0,
-                                       E->stream);
+    if (e == cudaSuccess)
+        e = cudaLaunchCooperativeKernel(kernel_ptr(E->ranks, E->words_only), grid, dim3(kEnsThreads), params, 0,
+                                        E->stream);
+    if (e == cudaSuccess && E->n_pack) {
+        pack_links_kernel<<<pack_blocks, 256, 0, E->stream>>>(E->d_pack, E->n_pack, E->pack_total, true);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t launch_persistent(plq_ensemble *E, uint64_t sweeps) {
+    EnsArgs a = ens_args(E, sweeps);
+    return launch_ensemble(E, a);
+}
+
+// Members that run packed: Z2 gauge on the keyed stream, 2 <= d <= 4, rows of
+// at most 32 links, outside tempering ladders (whose energies the kernel
+// reads from the byte planes).
+bool packed_eligible(const plq_chain_desc &d) {
+    return d.model == PLQ_GAUGE && d.rng == PLQ_RNG_KEYED && d.d >= 2 && d.d <= 4 && d.shape[0] <= 32 &&
+           (d.updater == PLQ_HEATBATH || d.updater == PLQ_METROPOLIS) && !(d.flags & PLQ_FLAG_GENERIC_PASS);
+}
+
+// The device packing table of the members with pk set.
+cudaError_t build_pack_table(plq_ensemble *E) {
+    std::vector<PackEntry> tab;
+    uint32_t total = 0;
+    for (auto &mem : E->members) {
+        if (!mem.pk) continue;
+        PackEntry t;
+        t.state = mem.a.state;
+        t.pk = mem.pk;
+        t.first = total;
+        t.L0 = (uint32_t)mem.a.g.L[0];
+        total += (uint32_t)mem.a.g.d * (uint32_t)(mem.a.g.n_sites / mem.a.g.L[0]);
+        tab.push_back(t);
+    }
+    if (E->d_pack) {
+        cudaFree(E->d_pack);
+        E->allocs.erase(std::remove(E->allocs.begin(), E->allocs.end(), (void *)E->d_pack), E->allocs.end());
+        E->d_pack = nullptr;
+    }
+    E->n_pack = (int)tab.size();
+    E->pack_total = total;
+    if (tab.empty()) return cudaSuccess;
+    return dev_upload(E, tab.data(), tab.size(), &E->d_pack);
 }
 
 }  // namespace
@@ -770,6 +974,7 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
             table_bytes += align(jumps[m].size() * sizeof(AffineHost));
         }
         state_bytes += align((size_t)mem.n_vars);
+        if (packed_eligible(d)) state_bytes += align(sizeof(uint32_t) * (size_t)mem.n_vars / (size_t)d.shape[0]);
         if (mem.link && starts && starts[m]) stage_bytes = std::max(stage_bytes, (size_t)mem.n_vars);
         E->members.push_back(mem);
         E->n_vars.push_back(mem.n_vars);
@@ -801,6 +1006,10 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         uint8_t *st = state_arena + soff;
         soff += align((size_t)mem.n_vars);
         a.state = st;
+        if (packed_eligible(descs[m])) {
+            mem.pk = reinterpret_cast<uint32_t *>(state_arena + soff);
+            soff += align(sizeof(uint32_t) * (size_t)mem.n_vars / (size_t)descs[m].shape[0]);
+        }
         if (starts && starts[m]) {
             if (mem.link) {
                 ce = cudaMemcpyAsync(stage, starts[m], (size_t)mem.n_vars, cudaMemcpyHostToDevice, E->stream);
@@ -827,6 +1036,8 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
     if (stage) cudaFree(stage);
     if (ce != cudaSuccess) return fail(ens_fail(ce, "member set-up"));
+    ce = build_pack_table(E);
+    if (ce != cudaSuccess) return fail(ens_fail(ce, "packing table"));
     std::vector<unsigned long long> pos(n, 0);
     std::vector<long long> zeros(n, 0);
     LaunchState ls;
@@ -930,10 +1141,13 @@ extern "C" int plq_ensemble_add_ladder(plq_ensemble *E, int32_t k, const int32_t
         const int rc = rebuild_tables(E, m, betas[i]);
         if (rc != PLQ_OK) return rc;
         E->members[m].ladder = (int)E->ladders.size();
+        E->members[m].pk = nullptr;  // the energy phase reads ladder members' byte planes
     }
     int32_t *d_slots = nullptr;
     cudaError_t ce = dev_upload(E, ids.data(), ids.size(), &d_slots);
     if (ce != cudaSuccess) return ens_fail(ce, "ladder slots");
+    cudaError_t pe = build_pack_table(E);
+    if (pe != cudaSuccess) return ens_fail(pe, "packing table");
     LadderDev L;
     L.k = k;
     L.every = every;
@@ -1139,7 +1353,7 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
     //    after a one-sweep warm-up, each from the snapshot); the fastest is kept
     std::map<ShapeKey, std::vector<size_t>> groups;
     for (size_t m = 0; m < E->members.size(); ++m)
-        if (E->members[m].a.words) groups[shape_key(E->descs[m])].push_back(m);
+        if (E->members[m].a.words || E->members[m].pk) groups[shape_key(E->descs[m])].push_back(m);
     for (auto &kv : groups) {
         const std::vector<size_t> &ids = kv.second;
         int best_w = E->members[ids[0]].wpt;
@@ -1180,11 +1394,8 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
                 a.n_sp = n_sp;
                 a.n_ladders = 0;
                 a.pt_every = 0;
-                void *params[] = {&a};
-                dim3 grid((unsigned)(E->ctx->sm_count * E->ctas_per_sm));
                 cudaEventRecord(t0, E->stream);
-                e = cudaLaunchCooperativeKernel(kernel_ptr(E->ranks, E->words_only), grid, dim3(kEnsThreads), params,
-                                                0, E->stream);
+                e = launch_ensemble(E, a);
                 cudaEventRecord(t1, E->stream);
                 if (e == cudaSuccess) e = cudaEventSynchronize(t1);
                 if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
