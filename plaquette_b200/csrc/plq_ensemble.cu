@@ -1070,7 +1070,7 @@ namespace {
 // Member m's current table set (the host copy) rebuilt at `beta`, in place:
 // the table sizes depend on the model and shape only, so the device buffers
 // (and every captured launch that reads them) stay.
-int rebuild_tables(plq_ensemble *E, int32_t m, double beta) {
+int rebuild_tables(plq_ensemble *E, int32_t m, double beta, bool sync = true) {
     const plq_chain_desc &d = E->descs[m];
     ModelParams p;
     std::memset(&p, 0, sizeof p);
@@ -1098,7 +1098,9 @@ int rebuild_tables(plq_ensemble *E, int32_t m, double beta) {
         ce = cudaMemcpyAsync((void *)ts.metro24, t.metro24.data(), m24, cudaMemcpyHostToDevice, E->stream);
     if (ce == cudaSuccess && E->d_tsets)
         ce = cudaMemcpyAsync(E->d_tsets + E->ts_of_member[m], &ts, sizeof ts, cudaMemcpyHostToDevice, E->stream);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
+    // the host tables are pageable: each copy is staged before cudaMemcpyAsync returns, so
+    // they may go out of scope unsynchronised
+    if (ce == cudaSuccess && sync) ce = cudaStreamSynchronize(E->stream);
     if (ce != cudaSuccess) return ens_fail(ce, "member tables");
     return PLQ_OK;
 }
@@ -1138,7 +1140,7 @@ extern "C" int plq_ensemble_add_ladder(plq_ensemble *E, int32_t k, const int32_t
     // slot i of the ladder runs at betas[i]: rebuild member i's table set at that beta
     for (int32_t i = 0; i < k; ++i) {
         const int32_t m = ids[i];
-        const int rc = rebuild_tables(E, m, betas[i]);
+        const int rc = rebuild_tables(E, m, betas[i], false);
         if (rc != PLQ_OK) return rc;
         E->members[m].ladder = (int)E->ladders.size();
         E->members[m].pk = nullptr;  // the energy phase reads ladder members' byte planes
