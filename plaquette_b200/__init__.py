@@ -263,6 +263,8 @@ class GpuChain:
         if start is not None:
             start = np.ascontiguousarray(start, dtype=np.uint8)
             ptr = start.ctypes.data
+        # bound now: at interpreter exit the module's globals may already be gone
+        self._destroy = lib().plq_chain_destroy
         check(lib().plq_chain_create(gpu._h, C.byref(desc), ptr, C.byref(self._h)))
         self.n_vars = int(lib().plq_chain_n_vars(self._h))
         self.n_primaries = {ISING: 2, POTTS: 1 + desc.q, GAUGE: 1}[desc.model]
@@ -270,7 +272,7 @@ class GpuChain:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().plq_chain_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     __del__ = close

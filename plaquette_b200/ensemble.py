@@ -56,12 +56,14 @@ class Ensemble:
                     self._keep.append(s)
                     ptrs[i] = s.ctypes.data
         self._h = C.c_void_p()
+        # bound now: at interpreter exit the module's globals may already be gone
+        self._destroy = lib().plq_ensemble_destroy
         check(lib().plq_ensemble_create(gpu._h, n, arr, ptrs, C.byref(self._h)))
         self.n = n
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().plq_ensemble_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     __del__ = close

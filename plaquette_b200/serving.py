@@ -46,12 +46,14 @@ class Server:
     def __init__(self, gpu: Gpu, budget_bytes: int = 0, max_slots: int = 64, tick_ms: float = 10.0):
         self.gpu = gpu
         self._h = C.c_void_p()
+        # bound now: at interpreter exit the module's globals may already be gone
+        self._destroy = lib().plq_server_destroy
         check(lib().plq_server_create(gpu._h, budget_bytes, max_slots, tick_ms, C.byref(self._h)))
         self._jobs = {}
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().plq_server_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     __del__ = close
