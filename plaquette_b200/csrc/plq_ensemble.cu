@@ -65,9 +65,9 @@ struct EnsMember {
     int link;          // variables on links
     int passes;        // colour passes per sweep
     int64_t n_vars;
-    int wpt;           // four-site body: words per thread of a work item (the tuned shape)
-    int pad_;
-    uint32_t *pk;      // packed Z2 links (one 32-bit row of L0 links per word, d planes), or null
+    int wpt;           // four-site or packed body: words (rows) per thread of a work item (the tuned shape)
+    int pk_wide;       // packed rows are 64-bit words (sites with 32 < L0 <= 64)
+    void *pk;          // packed variables: one row of L0 bits per word (links: d planes), or null
     double j;
     int ladder;
 };
@@ -245,22 +245,136 @@ __device__ void run_item(const LocalArgs &a, int d, int link, int64_t chunk, int
 // the same table -- so results are bit-identical.  The launch packs the bytes
 // first and unpacks them at its end (pack_links_kernel).
 
-__device__ __forceinline__ uint32_t row_xp(uint32_t w, uint32_t L0, uint32_t full) {  // bit x <- bit x+1
+template <class W>
+__device__ __forceinline__ W row_xp(W w, uint32_t L0, W full) {  // bit x <- bit x+1
     return ((w >> 1) | (w << (L0 - 1))) & full;
 }
-__device__ __forceinline__ uint32_t row_xm(uint32_t w, uint32_t L0, uint32_t full) {  // bit x <- bit x-1
+template <class W>
+__device__ __forceinline__ W row_xm(W w, uint32_t L0, W full) {  // bit x <- bit x-1
     return ((w << 1) | (w >> (L0 - 1))) & full;
 }
 // bit-sliced counter (c2 c1 c0) += v, per bit position (counts stay below 8)
-__device__ __forceinline__ void count_add(uint32_t &c0, uint32_t &c1, uint32_t &c2, uint32_t v) {
-    const uint32_t k0 = c0 & v;
+template <class W>
+__device__ __forceinline__ void count_add(W &c0, W &c1, W &c2, W v) {
+    const W k0 = c0 & v;
     c0 ^= v;
     c2 |= c1 & k0;
     c1 ^= k0;
 }
+__device__ __forceinline__ int popc_w(uint32_t v) { return __popc(v); }
+__device__ __forceinline__ int popc_w(uint64_t v) { return __popcll(v); }
+
+// Row r's coordinates along directions 1..D-1: their parity and the row
+// offsets to the +k / -k neighbour rows (periodic).
+template <int D>
+__device__ __forceinline__ int row_geometry(const Geom &g, uint32_t r, uint32_t L0, int32_t *op, int32_t *om) {
+    uint32_t rr = r;
+    int par = 0;
+#pragma unroll
+    for (int k = 1; k < D; ++k) {
+        const uint32_t q = fdiv(rr, g.dm[k], g.dl[k]);
+        const int32_t c = (int32_t)(rr - q * (uint32_t)g.L[k]);
+        rr = q;
+        par += c;
+        const int32_t rs = (int32_t)(g.stride[k] / (int64_t)L0);
+        op[k] = c + 1 < g.L[k] ? rs : -(g.L[k] - 1) * rs;
+        om[k] = c > 0 ? -rs : (g.L[k] - 1) * rs;
+    }
+    return par;
+}
+
+// q = 2 sites (Ising, or Potts at q = 2) packed by rows: the per-site count of
+// neighbours in state 1 comes out of the bit-sliced counter over the 2d
+// neighbour rows (d <= 3: at most 6), key cur + 2 * count as the byte body's.
+template <int D, class W>
+__device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R) {
+    const uint32_t L0 = (uint32_t)a.g.L[0];
+    const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
+    const W full = L0 == 8 * sizeof(W) ? ~(W)0 : (((W)1 << L0) - 1);
+    const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
+    const bool hb = a.kernel == PLQ_HEATBATH;
+    const uint32_t sweep_mix = a.sweep32 * 0x9e3779b9u;
+#pragma unroll 1
+    for (int i = 0; i < R; ++i) {
+        const uint32_t r = r0 + (uint32_t)i;
+        if (r >= rows) break;
+        int32_t op[4] = {0, 0, 0, 0}, om[4] = {0, 0, 0, 0};
+        const int par = row_geometry<D>(a.g, r, L0, op, om);
+        const W C = pk[r];
+        W c0 = 0, c1 = 0, c2 = 0;
+        count_add(c0, c1, c2, row_xp(C, L0, full));
+        count_add(c0, c1, c2, row_xm(C, L0, full));
+#pragma unroll
+        for (int k = 1; k < D; ++k) {
+            count_add(c0, c1, c2, pk[r + (uint32_t)op[k]]);
+            count_add(c0, c1, c2, pk[r + (uint32_t)om[k]]);
+        }
+        const uint32_t x0 = (uint32_t)((a.color ^ par) & 1);
+        W flip = 0;
+        const uint32_t site_row = r * L0;
+#pragma unroll 1
+        for (uint32_t x = x0; x < L0; x += 2) {
+            const uint32_t cur = (uint32_t)(C >> x) & 1u;
+            const uint32_t cnt = ((uint32_t)(c0 >> x) & 1u) | (((uint32_t)(c1 >> x) & 1u) << 1) |
+                                 (((uint32_t)(c2 >> x) & 1u) << 2);
+            const uint32_t key = cur + 2u * cnt;
+            const uint32_t k = lowbias32(lowbias32(a.seed32 ^ (site_row + x)) ^ sweep_mix) >> 8;
+            uint32_t nv;
+            if (hb) {
+                nv = a.hb24[key] <= k ? 1u : 0u;
+            } else {
+                const uint32_t e = a.metro24[key];
+                nv = (e == 0xFFFFFFFFu || k < e) ? 1u - cur : cur;
+            }
+            flip |= (W)(nv ^ cur) << x;
+        }
+        pk[r] = C ^ flip;
+    }
+}
+
+// Energy integer of packed rows [c * blockDim, (c + 1) * blockDim), one row per
+// thread: sites -- the bond sum (Ising) or agreement count (Potts) over the
+// +mu bonds; links -- the plaquette sum over mu < nu (as energy_chunk).
+template <int D, class W>
+__device__ long long packed_energy_rows(const LocalArgs &a, const W *pk, int link, int64_t c) {
+    const uint32_t L0 = (uint32_t)a.g.L[0];
+    const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
+    const W full = L0 == 8 * sizeof(W) ? ~(W)0 : (((W)1 << L0) - 1);
+    const uint32_t r = (uint32_t)(c * (int64_t)blockDim.x) + threadIdx.x;
+    if (r >= rows) return 0;
+    int32_t op[4] = {0, 0, 0, 0}, om[4] = {0, 0, 0, 0};
+    row_geometry<D>(a.g, r, L0, op, om);
+    long long acc = 0;
+    if (!link) {
+        const W C = pk[r];
+        int diff = popc_w((C ^ row_xp(C, L0, full)) & full);
+        long long pairs = L0;
+#pragma unroll
+        for (int k = 1; k < D; ++k) {
+            diff += popc_w(C ^ pk[r + (uint32_t)op[k]]);
+            pairs += L0;
+        }
+        acc = a.model == PLQ_ISING ? pairs - 2ll * diff : pairs - diff;
+    } else {
+#pragma unroll
+        for (int mu = 0; mu < D; ++mu) {
+#pragma unroll
+            for (int nu = mu + 1; nu < D; ++nu) {
+                const W *Pmu = pk + (uint32_t)mu * rows, *Pnu = pk + (uint32_t)nu * rows;
+                const W umu = Pmu[r], unu = Pnu[r];
+                // U_nu(s + mu): mu = 0 a rotation of the row, else the +mu row
+                const W nu_smu = mu == 0 ? row_xp(unu, L0, full) : Pnu[r + (uint32_t)op[mu]];
+                const W mu_snu = Pmu[r + (uint32_t)op[nu]];  // nu >= 1
+                acc += (long long)L0 - 2ll * popc_w(umu ^ nu_smu ^ mu_snu ^ unu);
+            }
+        }
+    }
+    return acc;
+}
 
 template <int D>
 __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk, int R) {
+    // (rows of at most 32 links)
     const uint32_t L0 = (uint32_t)a.g.L[0];
     const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
     const int mu = a.dir;
@@ -337,13 +451,15 @@ __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk
     }
 }
 
-// Packing entry of one member: its rows of all d directions occupy
-// [first, first + d * rows) of the launch's packing index space.
+// Packing entry of one member: its rows (of all d directions, for links)
+// occupy [first, first + planes * rows) of the launch's packing index space.
 struct PackEntry {
     uint8_t *state;   // byte planes (dir * n_sites + site)
-    uint32_t *pk;
+    void *pk;
     uint32_t first;   // first index of this member
     uint32_t L0;
+    int wide;         // 64-bit rows
+    int pad;
 };
 
 // Bytes to bits (unpack = false) or back (unpack = true) for every packed
@@ -360,11 +476,12 @@ __global__ void pack_links_kernel(const PackEntry *tab, int n_tab, uint32_t tota
         const uint32_t idx = g - t.first;  // dir * rows + row: its bytes start at idx * L0
         uint8_t *bytes = t.state + (size_t)idx * t.L0;
         if (!unpack) {
-            uint32_t w = 0;
-            for (uint32_t x = 0; x < t.L0; ++x) w |= (uint32_t)(bytes[x] & 1u) << x;
-            t.pk[idx] = w;
+            uint64_t w = 0;
+            for (uint32_t x = 0; x < t.L0; ++x) w |= (uint64_t)(bytes[x] & 1u) << x;
+            if (t.wide) static_cast<uint64_t *>(t.pk)[idx] = w;
+            else static_cast<uint32_t *>(t.pk)[idx] = (uint32_t)w;
         } else {
-            const uint32_t w = t.pk[idx];
+            const uint64_t w = t.wide ? static_cast<const uint64_t *>(t.pk)[idx] : static_cast<const uint32_t *>(t.pk)[idx];
             for (uint32_t x = 0; x < t.L0; ++x) bytes[x] = (uint8_t)((w >> x) & 1u);
         }
     }
@@ -457,7 +574,23 @@ __device__ void energy_phase(const EnsArgs &e) {
         int m = e.e_item_member[i];
         if (threadIdx.x == 0) sa = e.members[m].a;
         __syncthreads();
-        long long part = energy_item(sa, sa.g.d, e.members[m].link, e.e_item_chunk[i]);
+        const EnsMember &mem = e.members[m];
+        long long part = 0;
+        if (!mem.pk) {
+            part = energy_item(sa, sa.g.d, mem.link, e.e_item_chunk[i]);
+        } else if (mem.pk_wide) {
+            const uint64_t *pk = static_cast<const uint64_t *>(mem.pk);
+            part = sa.g.d == 2 ? packed_energy_rows<2, uint64_t>(sa, pk, mem.link, e.e_item_chunk[i])
+                               : packed_energy_rows<3, uint64_t>(sa, pk, mem.link, e.e_item_chunk[i]);
+        } else {
+            const uint32_t *pk = static_cast<const uint32_t *>(mem.pk);
+            switch (sa.g.d) {
+                case 2: part = packed_energy_rows<2, uint32_t>(sa, pk, mem.link, e.e_item_chunk[i]); break;
+                case 3: part = packed_energy_rows<3, uint32_t>(sa, pk, mem.link, e.e_item_chunk[i]); break;
+                case 4: part = packed_energy_rows<4, uint32_t>(sa, pk, mem.link, e.e_item_chunk[i]); break;
+                default: break;
+            }
+        }
         long long tot = block_sum(part);
         if (threadIdx.x == 0 && tot) atomicAdd((unsigned long long *)&e.energy[m], (unsigned long long)tot);
         __syncthreads();
@@ -564,12 +697,24 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
                     last_m = m;
                     run = 0;
                 }
-                if (e.members[m].pk) {
+                const EnsMember &mem = e.members[m];
+                if (mem.pk && mem.link) {
+                    uint32_t *pk = static_cast<uint32_t *>(mem.pk);
                     switch (sa.g.d) {
-                        case 2: packed_link_item<2>(sa, e.members[m].pk, e.item_chunk[i], e.members[m].wpt); break;
-                        case 3: packed_link_item<3>(sa, e.members[m].pk, e.item_chunk[i], e.members[m].wpt); break;
-                        case 4: packed_link_item<4>(sa, e.members[m].pk, e.item_chunk[i], e.members[m].wpt); break;
+                        case 2: packed_link_item<2>(sa, pk, e.item_chunk[i], mem.wpt); break;
+                        case 3: packed_link_item<3>(sa, pk, e.item_chunk[i], mem.wpt); break;
+                        case 4: packed_link_item<4>(sa, pk, e.item_chunk[i], mem.wpt); break;
                         default: break;
+                    }
+                } else if (mem.pk) {
+                    if (mem.pk_wide) {
+                        uint64_t *pk = static_cast<uint64_t *>(mem.pk);
+                        if (sa.g.d == 2) packed_site_item<2, uint64_t>(sa, pk, e.item_chunk[i], mem.wpt);
+                        else packed_site_item<3, uint64_t>(sa, pk, e.item_chunk[i], mem.wpt);
+                    } else {
+                        uint32_t *pk = static_cast<uint32_t *>(mem.pk);
+                        if (sa.g.d == 2) packed_site_item<2, uint32_t>(sa, pk, e.item_chunk[i], mem.wpt);
+                        else packed_site_item<3, uint32_t>(sa, pk, e.item_chunk[i], mem.wpt);
                     }
                 } else {
                     run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i], e.members[m].wpt);
@@ -747,7 +892,10 @@ int build_items(plq_ensemble *E) {
     std::vector<int32_t> em, ec;
     for (auto &l : E->ladders)
         for (int32_t m : l) {
-            int64_t nc = (E->members[m].a.g.n_sites + kEnergyChunk - 1) / kEnergyChunk;
+            const EnsMember &mem = E->members[m];
+            // packed members: one row per thread; bytes: kEnergyChunk sites per item
+            const int64_t nc = mem.pk ? (mem.a.g.n_sites / mem.a.g.L[0] + kEnsThreads - 1) / kEnsThreads
+                                      : (mem.a.g.n_sites + kEnergyChunk - 1) / kEnergyChunk;
             for (int64_t c = 0; c < nc; ++c) {
                 em.push_back(m);
                 ec.push_back((int32_t)c);
@@ -846,12 +994,23 @@ cudaError_t launch_persistent(plq_ensemble *E, uint64_t sweeps) {
     return launch_ensemble(E, a);
 }
 
-// Members that run packed: Z2 gauge on the keyed stream, 2 <= d <= 4, rows of
-// at most 32 links, outside tempering ladders (whose energies the kernel
-// reads from the byte planes).
+// Members that run packed, on the keyed stream with Metropolis or heat bath:
+// Z2 gauge links with 2 <= d <= 4 and rows of at most 32 links; q = 2 sites
+// (Ising, Potts at q = 2) with 2 <= d <= 3 (at most 6 neighbours for the
+// counter) and rows of at most 64 sites.
 bool packed_eligible(const plq_chain_desc &d) {
-    return d.model == PLQ_GAUGE && d.rng == PLQ_RNG_KEYED && d.d >= 2 && d.d <= 4 && d.shape[0] <= 32 &&
-           (d.updater == PLQ_HEATBATH || d.updater == PLQ_METROPOLIS) && !(d.flags & PLQ_FLAG_GENERIC_PASS);
+    if (d.rng != PLQ_RNG_KEYED || (d.updater != PLQ_HEATBATH && d.updater != PLQ_METROPOLIS) ||
+        (d.flags & PLQ_FLAG_GENERIC_PASS))
+        return false;
+    if (d.model == PLQ_GAUGE) return d.d >= 2 && d.d <= 4 && d.shape[0] <= 32;
+    const int q = d.model == PLQ_POTTS ? d.q : 2;
+    return q == 2 && d.d >= 2 && d.d <= 3 && d.shape[0] <= 64;
+}
+
+// Bytes of a packed member's rows (every direction of a link member).
+size_t packed_bytes(const plq_chain_desc &d, int64_t n_vars) {
+    const size_t rows = (size_t)n_vars / (size_t)d.shape[0];  // links: d planes of rows
+    return rows * (d.model != PLQ_GAUGE && d.shape[0] > 32 ? 8 : 4);
 }
 
 // The device packing table of the members with pk set.
@@ -861,11 +1020,14 @@ cudaError_t build_pack_table(plq_ensemble *E) {
     for (auto &mem : E->members) {
         if (!mem.pk) continue;
         PackEntry t;
+        std::memset(&t, 0, sizeof t);
         t.state = mem.a.state;
         t.pk = mem.pk;
         t.first = total;
         t.L0 = (uint32_t)mem.a.g.L[0];
-        total += (uint32_t)mem.a.g.d * (uint32_t)(mem.a.g.n_sites / mem.a.g.L[0]);
+        t.wide = mem.pk_wide;
+        const uint32_t planes = mem.link ? (uint32_t)mem.a.g.d : 1u;
+        total += planes * (uint32_t)(mem.a.g.n_sites / mem.a.g.L[0]);
         tab.push_back(t);
     }
     if (E->d_pack) {
@@ -974,7 +1136,7 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
             table_bytes += align(jumps[m].size() * sizeof(AffineHost));
         }
         state_bytes += align((size_t)mem.n_vars);
-        if (packed_eligible(d)) state_bytes += align(sizeof(uint32_t) * (size_t)mem.n_vars / (size_t)d.shape[0]);
+        if (packed_eligible(d)) state_bytes += align(packed_bytes(d, mem.n_vars));
         if (mem.link && starts && starts[m]) stage_bytes = std::max(stage_bytes, (size_t)mem.n_vars);
         E->members.push_back(mem);
         E->n_vars.push_back(mem.n_vars);
@@ -1007,8 +1169,9 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         soff += align((size_t)mem.n_vars);
         a.state = st;
         if (packed_eligible(descs[m])) {
-            mem.pk = reinterpret_cast<uint32_t *>(state_arena + soff);
-            soff += align(sizeof(uint32_t) * (size_t)mem.n_vars / (size_t)descs[m].shape[0]);
+            mem.pk = state_arena + soff;
+            mem.pk_wide = descs[m].model != PLQ_GAUGE && descs[m].shape[0] > 32 ? 1 : 0;
+            soff += align(packed_bytes(descs[m], mem.n_vars));
         }
         if (starts && starts[m]) {
             if (mem.link) {
@@ -1143,7 +1306,6 @@ extern "C" int plq_ensemble_add_ladder(plq_ensemble *E, int32_t k, const int32_t
         const int rc = rebuild_tables(E, m, betas[i], false);
         if (rc != PLQ_OK) return rc;
         E->members[m].ladder = (int)E->ladders.size();
-        E->members[m].pk = nullptr;  // the energy phase reads ladder members' byte planes
     }
     int32_t *d_slots = nullptr;
     cudaError_t ce = dev_upload(E, ids.data(), ids.size(), &d_slots);

@@ -188,3 +188,42 @@ def test_tuner_chooses_a_shape_per_member_shape(gpu):
         c.advance(5)
         assert np.array_equal(ens.read(m), c.read()), m
         assert np.array_equal(later.read(m), c.read()), m
+
+
+@pytest.mark.parametrize("spec", [
+    (plq.ISING, 2, (48, 16, 8), plq.METROPOLIS, 0.2216544),   # 64-bit rows
+    (plq.ISING, 2, (64, 64), plq.HEATBATH, 0.44),             # 64-bit rows, 2D
+    (plq.POTTS, 2, (40, 12, 6), plq.HEATBATH, 0.9),           # Potts at q = 2: agreement energy
+    (plq.ISING, 2, (2, 6, 4), plq.METROPOLIS, 0.5),           # rows of two sites
+    (plq.GAUGE, 2, (2, 4, 2, 4), plq.HEATBATH, 0.6),          # rows of two links
+    (plq.GAUGE, 2, (32, 4, 4), plq.METROPOLIS, 0.8),          # full 32-bit rows
+], ids=lambda s: f"{s[0]}-{'x'.join(map(str, s[2]))}")
+def test_packed_members_match_their_own_chains(gpu, spec):
+    """Keyed q = 2 sites and Z2 links run as packed rows inside the persistent
+    launch (the per-member chain runs the byte passes): identical
+    configurations and primaries, and the same under a tempering ladder,
+    whose energies the launch reads from the packed rows."""
+    kind, q, shape, upd, beta = spec
+    n = int(np.prod(shape)) * (len(shape) if kind == plq.GAUGE else 1)
+    descs, starts = [], []
+    for k in range(3):
+        starts.append(plq.hot_start(90 + k, q, n)[0])
+        descs.append(plq.make_desc(kind, q, shape, upd, beta=beta * (1 + 0.05 * k), seed=90 + k, rng=plq.RNG_KEYED,
+                                   batch=1))
+    ens = Ensemble(gpu, descs, starts)
+    chains = [plq.GpuChain(gpu, d, s) for d, s in zip(descs, starts)]
+    ens.advance(7)
+    for m, c in enumerate(chains):
+        c.advance(7)
+        assert np.array_equal(ens.read(m), c.read()), m
+        assert list(ens.primaries(m)) == list(c.primaries()), m
+    # a ladder over the same members: batched (packed, energies from packed rows) == per-lattice (bytes)
+    a = Ensemble(gpu, descs, starts)
+    b = Ensemble(gpu, descs, starts)
+    for e in (a, b):
+        e.add_ladder([0, 1, 2], [beta, beta * 1.05, beta * 1.1], 2, seed=3)
+    a.advance(12)
+    b.advance_unbatched(12)
+    assert np.array_equal(a.betas(), b.betas())
+    for m in range(3):
+        assert np.array_equal(a.read(m), b.read(m)), m
