@@ -475,14 +475,30 @@ __global__ void pack_links_kernel(const PackEntry *tab, int n_tab, uint32_t tota
         const PackEntry &t = tab[lo];
         const uint32_t idx = g - t.first;  // dir * rows + row: its bytes start at idx * L0
         uint8_t *bytes = t.state + (size_t)idx * t.L0;
+        const bool quads = (t.L0 & 3u) == 0;  // the row's bytes come as aligned 32-bit words
         if (!unpack) {
             uint64_t w = 0;
-            for (uint32_t x = 0; x < t.L0; ++x) w |= (uint64_t)(bytes[x] & 1u) << x;
+            if (quads) {
+                // four 0/1 bytes to four bits: b_i * 2^(8i) times 2^24 + 2^17 + 2^10 + 2^3 lands
+                // b_i on bit 24 + i, every other product below bit 24 or beyond bit 31
+                const uint32_t *q4 = reinterpret_cast<const uint32_t *>(bytes);
+                for (uint32_t k = 0; k < t.L0 / 4; ++k)
+                    w |= (uint64_t)((((q4[k] & 0x01010101u) * 0x01020408u) >> 24) & 0xFu) << (4 * k);
+            } else {
+                for (uint32_t x = 0; x < t.L0; ++x) w |= (uint64_t)(bytes[x] & 1u) << x;
+            }
             if (t.wide) static_cast<uint64_t *>(t.pk)[idx] = w;
             else static_cast<uint32_t *>(t.pk)[idx] = (uint32_t)w;
         } else {
             const uint64_t w = t.wide ? static_cast<const uint64_t *>(t.pk)[idx] : static_cast<const uint32_t *>(t.pk)[idx];
-            for (uint32_t x = 0; x < t.L0; ++x) bytes[x] = (uint8_t)((w >> x) & 1u);
+            if (quads) {
+                // four bits to four bytes: bit i times 2^0 + 2^7 + 2^14 + 2^21 has a copy on bit 8i
+                uint32_t *q4 = reinterpret_cast<uint32_t *>(bytes);
+                for (uint32_t k = 0; k < t.L0 / 4; ++k)
+                    q4[k] = ((uint32_t)((w >> (4 * k)) & 0xFu) * 0x00204081u) & 0x01010101u;
+            } else {
+                for (uint32_t x = 0; x < t.L0; ++x) bytes[x] = (uint8_t)((w >> x) & 1u);
+            }
         }
     }
 }
@@ -968,13 +984,20 @@ int max_ctas_per_sm(int ranks, bool words_only) {
     return n;
 }
 
-// One persistent launch with arguments `a`: packed Z2 members are packed before
+// One persistent launch with arguments `a`: packed members are packed before
 // and unpacked after it, so outside a launch every member is in byte planes.
-cudaError_t launch_ensemble(plq_ensemble *E, EnsArgs &a) {
-    const unsigned pack_blocks = (unsigned)std::min<uint32_t>((E->pack_total + 255) / 256, 148u * 8u);
+// `tab` (n entries, `total` rows) is the packing table: the ensemble's by default.
+cudaError_t launch_ensemble(plq_ensemble *E, EnsArgs &a, const PackEntry *tab = nullptr, int n = -1,
+                            uint32_t total = 0) {
+    if (n < 0) {
+        tab = E->d_pack;
+        n = E->n_pack;
+        total = E->pack_total;
+    }
+    const unsigned pack_blocks = (unsigned)std::min<uint32_t>((total + 255) / 256, 148u * 8u);
     cudaError_t e = cudaSuccess;
-    if (E->n_pack) {
-        pack_links_kernel<<<pack_blocks, 256, 0, E->stream>>>(E->d_pack, E->n_pack, E->pack_total, false);
+    if (n) {
+        pack_links_kernel<<<pack_blocks, 256, 0, E->stream>>>(tab, n, total, false);
         e = cudaGetLastError();
     }
     void *params[] = {&a};
@@ -982,8 +1005,8 @@ cudaError_t launch_ensemble(plq_ensemble *E, EnsArgs &a) {
     if (e == cudaSuccess)
         e = cudaLaunchCooperativeKernel(kernel_ptr(E->ranks, E->words_only), grid, dim3(kEnsThreads), params, 0,
                                         E->stream);
-    if (e == cudaSuccess && E->n_pack) {
-        pack_links_kernel<<<pack_blocks, 256, 0, E->stream>>>(E->d_pack, E->n_pack, E->pack_total, true);
+    if (e == cudaSuccess && n) {
+        pack_links_kernel<<<pack_blocks, 256, 0, E->stream>>>(tab, n, total, true);
         e = cudaGetLastError();
     }
     return e;
@@ -1013,11 +1036,12 @@ size_t packed_bytes(const plq_chain_desc &d, int64_t n_vars) {
     return rows * (d.model != PLQ_GAUGE && d.shape[0] > 32 ? 8 : 4);
 }
 
-// The device packing table of the members with pk set.
-cudaError_t build_pack_table(plq_ensemble *E) {
+// The packing table of members `ids` (those with pk set) on the host.
+std::vector<PackEntry> pack_entries(const plq_ensemble *E, const std::vector<size_t> &ids, uint32_t &total) {
     std::vector<PackEntry> tab;
-    uint32_t total = 0;
-    for (auto &mem : E->members) {
+    total = 0;
+    for (size_t m : ids) {
+        const EnsMember &mem = E->members[m];
         if (!mem.pk) continue;
         PackEntry t;
         std::memset(&t, 0, sizeof t);
@@ -1030,6 +1054,15 @@ cudaError_t build_pack_table(plq_ensemble *E) {
         total += planes * (uint32_t)(mem.a.g.n_sites / mem.a.g.L[0]);
         tab.push_back(t);
     }
+    return tab;
+}
+
+// The device packing table of every member with pk set.
+cudaError_t build_pack_table(plq_ensemble *E) {
+    std::vector<size_t> all(E->members.size());
+    for (size_t m = 0; m < all.size(); ++m) all[m] = m;
+    uint32_t total = 0;
+    std::vector<PackEntry> tab = pack_entries(E, all, total);
     if (E->d_pack) {
         cudaFree(E->d_pack);
         E->allocs.erase(std::remove(E->allocs.begin(), E->allocs.end(), (void *)E->d_pack), E->allocs.end());
@@ -1528,10 +1561,20 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
             std::vector<int8_t> ip;
             std::vector<int64_t> spb;
             const int n_sp = append_items(E->members.data(), ids, 0, E->ranks, im, ic, ip, spb);
+            uint32_t g_total = 0;
+            const std::vector<PackEntry> g_tab = pack_entries(E, ids, g_total);
+            PackEntry *d_gtab = nullptr;
             int32_t *d_im = nullptr, *d_ic = nullptr;
             int8_t *d_ip = nullptr;
             int64_t *d_spb = nullptr;
-            e = cudaMalloc((void **)&d_im, im.size() * sizeof(int32_t));
+            e = cudaSuccess;
+            if (!g_tab.empty()) {
+                e = cudaMalloc((void **)&d_gtab, g_tab.size() * sizeof(PackEntry));
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(d_gtab, g_tab.data(), g_tab.size() * sizeof(PackEntry), cudaMemcpyHostToDevice,
+                                        E->stream);
+            }
+            if (e == cudaSuccess) e = cudaMalloc((void **)&d_im, im.size() * sizeof(int32_t));
             if (e == cudaSuccess) e = cudaMalloc((void **)&d_ic, ic.size() * sizeof(int32_t));
             if (e == cudaSuccess) e = cudaMalloc((void **)&d_ip, ip.size() * sizeof(int8_t));
             if (e == cudaSuccess) e = cudaMalloc((void **)&d_spb, spb.size() * sizeof(int64_t));
@@ -1559,7 +1602,7 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
                 a.n_ladders = 0;
                 a.pt_every = 0;
                 cudaEventRecord(t0, E->stream);
-                e = launch_ensemble(E, a);
+                e = launch_ensemble(E, a, d_gtab, (int)g_tab.size(), g_total);
                 cudaEventRecord(t1, E->stream);
                 if (e == cudaSuccess) e = cudaEventSynchronize(t1);
                 if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
@@ -1568,6 +1611,7 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
             cudaFree(d_ic);
             cudaFree(d_ip);
             cudaFree(d_spb);
+            if (d_gtab) cudaFree(d_gtab);
             if (e != cudaSuccess) break;
             if (ms < best_g) {
                 best_g = ms;
