@@ -121,6 +121,7 @@ struct LaunchState {
     unsigned long long pt_attempts; // per-ensemble attempt counter
     unsigned int bar_count;
     unsigned int bar_gen;
+    unsigned long long ticket;      // next work-item ticket of the running launch (zero between launches)
 };
 
 struct EnsArgs {
@@ -671,91 +672,93 @@ __device__ void wait_member(const EnsArgs &e, int m, unsigned long long t, int p
     }
 }
 
-// The persistent launch.  A CTA takes a contiguous block of each super-phase's
-// work items (neighbouring items mostly share a member, whose arguments then
-// stay in shared memory).  There is no grid barrier between super-phases:
-// before a run of items of member m's pass p the CTA waits until the member's
+// The persistent launch.  Work items are dealt out dynamically: ticket k is
+// item k mod n_items of sweep k / n_items, and a CTA takes its next ticket
+// (one atomic add) while it runs the current item, so the CTAs stay evenly
+// loaded although items differ several-fold in work (each super-phase lists
+// its items largest first).  There is no grid barrier between super-phases:
+// before an item of member m's pass p the CTA waits until the member's
 // previous passes are complete (per-member counters, released by the CTAs
 // that ran them), so a pass of one member overlaps the tails of every other
-// member's passes.  Every wait is on items of an earlier super-phase and all
-// CTAs are resident (cooperative launch), so the waits always end.  Grid
-// barriers remain around the tempering phase and at the end of the launch.
+// member's passes.  Tickets are taken in order and every wait is on items of
+// lower tickets, all taken by resident CTAs (cooperative launch) that wait
+// only on still lower ones, so the waits always end.  A CTA whose ticket lies
+// past the end of a sweep with a tempering phase joins that phase's grid
+// barriers (all its items of the sweep are done by then); every CTA crosses
+// every sweep end, in order, so all take the same barriers.
 template <int R, bool WORDS_ONLY>
 __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
-    for (unsigned long long t = 0; t < e.sweeps; ++t) {
-        for (int sp = 0; sp < e.n_sp; ++sp) {
-            const int64_t b0 = e.sp_begin[sp], b1 = e.sp_begin[sp + 1];
-            const int64_t per = (b1 - b0 + gridDim.x - 1) / gridDim.x;
-            const int64_t lo = b0 + (int64_t)blockIdx.x * per;
-            const int64_t hi = lo + per < b1 ? lo + per : b1;
-            int last_m = -1;  // the arguments in shared memory (a member has one pass per super-phase)
-            unsigned long long run = 0;  // items of member last_m done in this run
-            for (int64_t i = lo; i < hi; ++i) {
-                int m = e.item_member[i];
-                if (m != last_m) {
-                    __syncthreads();  // every thread is done with the previous run's items and arguments
-                    if (threadIdx.x == 0) {
-                        if (last_m >= 0) {  // release them
-                            __threadfence();
-                            atomicAdd(&e.done[last_m], run);
-                        }
-                        wait_member(e, m, t, e.item_pass[i]);
-                    }
-                    // the member's arguments into shared memory, one 32-bit word per thread,
-                    // then the pass-specific fields
-                    const uint32_t *src = reinterpret_cast<const uint32_t *>(&e.members[m].a);
-                    uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
-                    for (int k = threadIdx.x; k < (int)(sizeof(LocalArgs) / 4); k += blockDim.x) dst[k] = src[k];
+    __shared__ unsigned long long s_ticket;
+    const unsigned long long n_items = (unsigned long long)e.sp_begin[e.n_sp];
+    const unsigned long long total = n_items * e.sweeps;
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&e.ls->ticket, 1ull);
+    __syncthreads();
+    unsigned long long tk = s_ticket;
+    unsigned long long round = 0;  // sweeps whose end this CTA has crossed
+    int last_m = -1;               // the member whose arguments are in sa
+    for (;;) {
+        const unsigned long long r = tk < total ? tk / n_items : e.sweeps;
+        for (; round < r; ++round) {  // this CTA is past the end of sweep `round`: its tempering phase
+            const unsigned long long swept = e.ls->sweep + round + 1;
+            if (e.n_ladders && e.pt_every > 0 && swept % (unsigned long long)e.pt_every == 0) {
+                grid_barrier(e);  // every member's sweeps complete
+                energy_phase(e);
+                grid_barrier(e);
+                if (blockIdx.x == 0) {
+                    swap_phase(e, e.ls->pt_attempts + swept / (unsigned long long)e.pt_every - 1);
                     __syncthreads();
-                    if (threadIdx.x == 0) item_pass_fields(e, m, e.item_pass[i], t, sa);
-                    __syncthreads();
-                    last_m = m;
-                    run = 0;
+                    for (int m = threadIdx.x; m < e.n_members; m += blockDim.x) e.energy[m] = 0;  // for the next phase
                 }
-                const EnsMember &mem = e.members[m];
-                if (mem.pk && mem.link) {
-                    uint32_t *pk = static_cast<uint32_t *>(mem.pk);
-                    switch (sa.g.d) {
-                        case 2: packed_link_item<2>(sa, pk, e.item_chunk[i], mem.wpt); break;
-                        case 3: packed_link_item<3>(sa, pk, e.item_chunk[i], mem.wpt); break;
-                        case 4: packed_link_item<4>(sa, pk, e.item_chunk[i], mem.wpt); break;
-                        default: break;
-                    }
-                } else if (mem.pk) {
-                    if (mem.pk_wide) {
-                        uint64_t *pk = static_cast<uint64_t *>(mem.pk);
-                        if (sa.g.d == 2) packed_site_item<2, uint64_t>(sa, pk, e.item_chunk[i], mem.wpt);
-                        else packed_site_item<3, uint64_t>(sa, pk, e.item_chunk[i], mem.wpt);
-                    } else {
-                        uint32_t *pk = static_cast<uint32_t *>(mem.pk);
-                        if (sa.g.d == 2) packed_site_item<2, uint32_t>(sa, pk, e.item_chunk[i], mem.wpt);
-                        else packed_site_item<3, uint32_t>(sa, pk, e.item_chunk[i], mem.wpt);
-                    }
-                } else {
-                    run_item<R, WORDS_ONLY>(sa, sa.g.d, e.members[m].link, e.item_chunk[i], e.members[m].wpt);
-                }
-                ++run;
-            }
-            if (last_m >= 0) {
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    __threadfence();
-                    atomicAdd(&e.done[last_m], run);
-                }
+                grid_barrier(e);
             }
         }
-        const unsigned long long swept = e.ls->sweep + t + 1;
-        if (e.n_ladders && e.pt_every > 0 && swept % (unsigned long long)e.pt_every == 0) {
-            grid_barrier(e);  // every member's sweeps complete
-            energy_phase(e);
-            grid_barrier(e);
-            if (blockIdx.x == 0) {
-                swap_phase(e, e.ls->pt_attempts + swept / (unsigned long long)e.pt_every - 1);
-                __syncthreads();
-                for (int m = threadIdx.x; m < e.n_members; m += blockDim.x) e.energy[m] = 0;  // for the next phase
+        if (tk >= total) break;
+        const int64_t i = (int64_t)(tk - r * n_items);
+        const int m = e.item_member[i];
+        const int p = e.item_pass[i];
+        if (threadIdx.x == 0) {
+            const unsigned long long next = atomicAdd(&e.ls->ticket, 1ull);  // used after this item
+            wait_member(e, m, r, p);
+            s_ticket = next;
+        }
+        if (m != last_m) {  // the member's arguments into shared memory, one 32-bit word per thread
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(&e.members[m].a);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
+            for (int k = threadIdx.x; k < (int)(sizeof(LocalArgs) / 4); k += blockDim.x) dst[k] = src[k];
+            last_m = m;
+        }
+        __syncthreads();  // the wait is over and the arguments are loaded
+        if (threadIdx.x == 0) item_pass_fields(e, m, p, r, sa);
+        tk = s_ticket;
+        __syncthreads();
+        const EnsMember &mem = e.members[m];
+        const int64_t chunk = e.item_chunk[i];
+        if (mem.pk && mem.link) {
+            uint32_t *pk = static_cast<uint32_t *>(mem.pk);
+            switch (sa.g.d) {
+                case 2: packed_link_item<2>(sa, pk, chunk, mem.wpt); break;
+                case 3: packed_link_item<3>(sa, pk, chunk, mem.wpt); break;
+                case 4: packed_link_item<4>(sa, pk, chunk, mem.wpt); break;
+                default: break;
             }
-            grid_barrier(e);
+        } else if (mem.pk) {
+            if (mem.pk_wide) {
+                uint64_t *pk = static_cast<uint64_t *>(mem.pk);
+                if (sa.g.d == 2) packed_site_item<2, uint64_t>(sa, pk, chunk, mem.wpt);
+                else packed_site_item<3, uint64_t>(sa, pk, chunk, mem.wpt);
+            } else {
+                uint32_t *pk = static_cast<uint32_t *>(mem.pk);
+                if (sa.g.d == 2) packed_site_item<2, uint32_t>(sa, pk, chunk, mem.wpt);
+                else packed_site_item<3, uint32_t>(sa, pk, chunk, mem.wpt);
+            }
+        } else {
+            run_item<R, WORDS_ONLY>(sa, sa.g.d, mem.link, chunk, mem.wpt);
+        }
+        __syncthreads();  // every thread's stores of the item are done: release it
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&e.done[m], 1ull);
         }
     }
     // advance the device-resident launch state (block 0, after every CTA left the loop)
@@ -767,7 +770,10 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
             e.done[m] = 0;
         }
         __syncthreads();
-        if (threadIdx.x == 0) e.ls->sweep += e.sweeps;
+        if (threadIdx.x == 0) {
+            e.ls->sweep += e.sweeps;
+            e.ls->ticket = 0;
+        }
     }
 }
 
@@ -857,6 +863,29 @@ void drop_graph(plq_ensemble *E) {
     E->graph = nullptr;
 }
 
+// Estimated time of work item `c` of a member (arbitrary units: only the
+// order of items matters): the units of its busiest thread -- packed rows,
+// four-site words or colour ranks -- times their cost in instructions.
+int64_t item_cost(const EnsMember &mem, int64_t c, int ranks) {
+    const LocalArgs &a = mem.a;
+    const bool shaped = a.words || mem.pk;
+    const int64_t per_thread = shaped ? mem.wpt : ranks;
+    const int64_t chunk = (int64_t)kEnsThreads * per_thread;
+    const int64_t units = mem.pk ? a.g.n_sites / a.g.L[0] : (a.words ? a.g.n_sites / 4 : a.g.n_sites / 2);
+    const int64_t in_item = std::min(chunk, units - c * chunk);
+    const int64_t busiest = std::min(per_thread, (in_item + kEnsThreads - 1) / kEnsThreads);
+    int64_t unit_cost;
+    if (mem.pk) {  // a row: its staples or neighbour counts, then L0 / 2 updates
+        const int64_t upd = a.g.L[0] / 2;
+        unit_cost = mem.link ? 40 * upd + 35 * (a.g.d - 1) : 35 * upd + 12 * a.g.d;
+    } else if (a.words) {
+        unit_cost = 400;  // four sites of one colour in bytes
+    } else {
+        unit_cost = 150;  // one colour rank, generic body
+    }
+    return busiest * unit_cost;
+}
+
 // Work items of one sweep of members `ids`, by super-phase; member indices
 // are relative to lo, and super-phase bounds are appended to spb (the last
 // one too).  With S super-phases (the most colour passes of any member),
@@ -865,15 +894,18 @@ void drop_graph(plq_ensemble *E) {
 // colours each spread over half the super-phases, a 4D gauge lattice's eight
 // passes one per super-phase, so every super-phase holds a similar share of
 // the sweep and each pass still ends (at a grid barrier) before the member's
-// next pass begins.  A member's items hold 256 * wpt four-site words (256 *
-// ranks colour ranks in the generic body).  Returns S.
+// next pass begins.  A member's items hold 256 * wpt four-site words or
+// packed rows (256 * ranks colour ranks in the generic body).  Each
+// super-phase lists its items largest first (item_cost), as the kernel deals
+// them out in list order.  Returns S.
 int append_items(const EnsMember *mems, const std::vector<size_t> &ids, size_t lo, int ranks,
                  std::vector<int32_t> &im, std::vector<int32_t> &ic, std::vector<int8_t> &ip,
                  std::vector<int64_t> &spb) {
     int S = 0;
     for (size_t m : ids) S = std::max(S, mems[m].passes);
     for (int sp = 0; sp < S; ++sp) {
-        spb.push_back((int64_t)im.size());
+        const size_t first = im.size();
+        spb.push_back((int64_t)first);
         for (size_t m : ids) {
             const int P = mems[m].passes;
             const LocalArgs &ma = mems[m].a;
@@ -893,6 +925,25 @@ int append_items(const EnsMember *mems, const std::vector<size_t> &ids, size_t l
                 }
             }
         }
+        // largest first; equal costs keep member order
+        const size_t n = im.size() - first;
+        std::vector<int64_t> cost(n);
+        std::vector<size_t> ord(n);
+        for (size_t k = 0; k < n; ++k) {
+            cost[k] = item_cost(mems[im[first + k] + lo], ic[first + k], ranks);
+            ord[k] = k;
+        }
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
+        std::vector<int32_t> tm(n), tc(n);
+        std::vector<int8_t> tp(n);
+        for (size_t k = 0; k < n; ++k) {
+            tm[k] = im[first + ord[k]];
+            tc[k] = ic[first + ord[k]];
+            tp[k] = ip[first + ord[k]];
+        }
+        std::copy(tm.begin(), tm.end(), im.begin() + first);
+        std::copy(tc.begin(), tc.end(), ic.begin() + first);
+        std::copy(tp.begin(), tp.end(), ip.begin() + first);
     }
     spb.push_back((int64_t)im.size());
     return S;
