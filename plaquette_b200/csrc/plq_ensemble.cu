@@ -504,21 +504,46 @@ __global__ void pack_links_kernel(const PackEntry *tab, int n_tab, uint32_t tota
     }
 }
 
-// The pass-specific fields of member m's arguments (already copied into sa)
-// for colour pass `sp` of sweep index `sweep`.
-__device__ void item_pass_fields(const EnsArgs &e, int m, int sp, unsigned long long sweep_in_launch, LocalArgs &sa) {
+// The pass-specific fields of member m's arguments for colour pass `sp` of
+// sweep `sweep_in_launch`: loaded into registers (pass_fields), then written
+// over the member's arguments in shared memory (apply).
+struct PassFields {
+    const uint64_t *hb53;
+    const uint32_t *hb24;
+    const uint64_t *metro53;
+    const uint32_t *metro24;
+    uint64_t pass_offset;
+    uint32_t sweep32;
+    int dir, color;
+};
+
+__device__ __forceinline__ PassFields pass_fields(const EnsArgs &e, int m, int sp,
+                                                  unsigned long long sweep_in_launch) {
     const EnsMember &mem = e.members[m];
     const TableSet &ts = e.tsets[e.ts_of_member[m]];
-    sa.hb53 = ts.hb53;
-    sa.hb24 = ts.hb24;
-    sa.metro53 = ts.metro53;
-    sa.metro24 = ts.metro24;
-    sa.dir = mem.link ? sp >> 1 : 0;
-    sa.color = sp & 1;
-    sa.sweep32 = (uint32_t)((e.msweep ? e.msweep[m] : e.ls->sweep) + sweep_in_launch);
-    if (sa.jump)
-        sa.pass_offset = e.pos[m] + sweep_in_launch * (unsigned long long)mem.n_vars +
-                         (unsigned long long)sp * (unsigned long long)(mem.a.g.n_sites / 2);
+    PassFields f;
+    f.hb53 = ts.hb53;
+    f.hb24 = ts.hb24;
+    f.metro53 = ts.metro53;
+    f.metro24 = ts.metro24;
+    f.dir = mem.link ? sp >> 1 : 0;
+    f.color = sp & 1;
+    f.sweep32 = (uint32_t)((e.msweep ? e.msweep[m] : e.ls->sweep) + sweep_in_launch);
+    f.pass_offset = mem.a.jump ? e.pos[m] + sweep_in_launch * (unsigned long long)mem.n_vars +
+                                     (unsigned long long)sp * (unsigned long long)(mem.a.g.n_sites / 2)
+                               : 0;
+    return f;
+}
+
+__device__ __forceinline__ void apply(const PassFields &f, LocalArgs &sa) {
+    sa.hb53 = f.hb53;
+    sa.hb24 = f.hb24;
+    sa.metro53 = f.metro53;
+    sa.metro24 = f.metro24;
+    sa.dir = f.dir;
+    sa.color = f.color;
+    sa.sweep32 = f.sweep32;
+    if (sa.jump) sa.pass_offset = f.pass_offset;
 }
 
 // int64 energy integer of a member chunk: Ising bond sum, Potts agreement,
@@ -674,7 +699,7 @@ __device__ void wait_member(const EnsArgs &e, int m, unsigned long long t, int p
 
 // The persistent launch.  Work items are dealt out dynamically: ticket k is
 // item k mod n_items of sweep k / n_items, and a CTA takes its next ticket
-// (one atomic add) while it runs the current item, so the CTAs stay evenly
+// (one atomic add) at the start of the current item, so the CTAs stay evenly
 // loaded although items differ several-fold in work (each super-phase lists
 // its items largest first).  There is no grid barrier between super-phases:
 // before an item of member m's pass p the CTA waits until the member's
@@ -684,10 +709,15 @@ __device__ void wait_member(const EnsArgs &e, int m, unsigned long long t, int p
 // lower tickets, all taken by resident CTAs (cooperative launch) that wait
 // only on still lower ones, so the waits always end.  A CTA whose ticket lies
 // past the end of a sweep with a tempering phase joins that phase's grid
-// barriers (all its items of the sweep are done by then); every CTA crosses
-// every sweep end, in order, so all take the same barriers.
+// barriers (all its items of the sweep are done and released by then); every
+// CTA crosses every sweep end, in order, so all take the same barriers.
+//
+// Between two items three threads work side by side: thread 0 takes the next
+// ticket and waits for the member, thread 32 loads the pass fields, thread 64
+// releases the previous item; the item's index entries are loaded while the
+// item before it runs.
 template <int R, bool WORDS_ONLY>
-__global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
+__global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
     __shared__ unsigned long long s_ticket;
     const unsigned long long n_items = (unsigned long long)e.sp_begin[e.n_sp];
@@ -695,32 +725,55 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
     if (threadIdx.x == 0) s_ticket = atomicAdd(&e.ls->ticket, 1ull);
     __syncthreads();
     unsigned long long tk = s_ticket;
+    unsigned long long r = 0;  // the ticket's sweep
+    int m = -1, p = 0;         // the ticket's item: member, pass, chunk
+    int64_t chunk = 0;
+    if (tk < total) {
+        r = tk / n_items;
+        const int64_t i = (int64_t)(tk - r * n_items);
+        m = e.item_member[i];
+        p = e.item_pass[i];
+        chunk = e.item_chunk[i];
+    }
     unsigned long long round = 0;  // sweeps whose end this CTA has crossed
     int last_m = -1;               // the member whose arguments are in sa
+    int pending = -1;              // member of the last item run, not yet released
     for (;;) {
-        const unsigned long long r = tk < total ? tk / n_items : e.sweeps;
-        for (; round < r; ++round) {  // this CTA is past the end of sweep `round`: its tempering phase
-            const unsigned long long swept = e.ls->sweep + round + 1;
-            if (e.n_ladders && e.pt_every > 0 && swept % (unsigned long long)e.pt_every == 0) {
-                grid_barrier(e);  // every member's sweeps complete
-                energy_phase(e);
-                grid_barrier(e);
-                if (blockIdx.x == 0) {
-                    swap_phase(e, e.ls->pt_attempts + swept / (unsigned long long)e.pt_every - 1);
-                    __syncthreads();
-                    for (int m = threadIdx.x; m < e.n_members; m += blockDim.x) e.energy[m] = 0;  // for the next phase
+        const unsigned long long r_at = tk < total ? r : e.sweeps;
+        if (round < r_at) {
+            if (pending >= 0) {  // release it before any tempering barrier
+                if (threadIdx.x == 0) {
+                    __threadfence();
+                    atomicAdd(&e.done[pending], 1ull);
                 }
-                grid_barrier(e);
+                pending = -1;
+            }
+            for (; round < r_at; ++round) {  // past the end of sweep `round`: its tempering phase
+                const unsigned long long swept = e.ls->sweep + round + 1;
+                if (e.n_ladders && e.pt_every > 0 && swept % (unsigned long long)e.pt_every == 0) {
+                    grid_barrier(e);  // every member's sweeps complete
+                    energy_phase(e);
+                    grid_barrier(e);
+                    if (blockIdx.x == 0) {
+                        swap_phase(e, e.ls->pt_attempts + swept / (unsigned long long)e.pt_every - 1);
+                        __syncthreads();
+                        for (int k = threadIdx.x; k < e.n_members; k += blockDim.x) e.energy[k] = 0;  // next phase
+                    }
+                    grid_barrier(e);
+                }
             }
         }
         if (tk >= total) break;
-        const int64_t i = (int64_t)(tk - r * n_items);
-        const int m = e.item_member[i];
-        const int p = e.item_pass[i];
+        PassFields pf;
         if (threadIdx.x == 0) {
             const unsigned long long next = atomicAdd(&e.ls->ticket, 1ull);  // used after this item
             wait_member(e, m, r, p);
             s_ticket = next;
+        } else if (threadIdx.x == 32) {
+            pf = pass_fields(e, m, p, r);
+        } else if (threadIdx.x == 64 && pending >= 0) {
+            __threadfence();
+            atomicAdd(&e.done[pending], 1ull);
         }
         if (m != last_m) {  // the member's arguments into shared memory, one 32-bit word per thread
             const uint32_t *src = reinterpret_cast<const uint32_t *>(&e.members[m].a);
@@ -728,12 +781,22 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
             for (int k = threadIdx.x; k < (int)(sizeof(LocalArgs) / 4); k += blockDim.x) dst[k] = src[k];
             last_m = m;
         }
-        __syncthreads();  // the wait is over and the arguments are loaded
-        if (threadIdx.x == 0) item_pass_fields(e, m, p, r, sa);
-        tk = s_ticket;
+        __syncthreads();  // the wait is over, the previous item released, the arguments loaded
+        if (threadIdx.x == 32) apply(pf, sa);
+        // the next item's index entries, loaded while this one runs
+        const unsigned long long tk_next = s_ticket;
+        unsigned long long r_next = 0;
+        int m_next = -1, p_next = 0;
+        int64_t chunk_next = 0;
+        if (tk_next < total) {
+            r_next = tk_next / n_items;
+            const int64_t i = (int64_t)(tk_next - r_next * n_items);
+            m_next = e.item_member[i];
+            p_next = e.item_pass[i];
+            chunk_next = e.item_chunk[i];
+        }
         __syncthreads();
         const EnsMember &mem = e.members[m];
-        const int64_t chunk = e.item_chunk[i];
         if (mem.pk && mem.link) {
             uint32_t *pk = static_cast<uint32_t *>(mem.pk);
             switch (sa.g.d) {
@@ -755,11 +818,17 @@ __global__ void __launch_bounds__(kEnsThreads) ensemble_kernel(EnsArgs e) {
         } else {
             run_item<R, WORDS_ONLY>(sa, sa.g.d, mem.link, chunk, mem.wpt);
         }
-        __syncthreads();  // every thread's stores of the item are done: release it
-        if (threadIdx.x == 0) {
-            __threadfence();
-            atomicAdd(&e.done[m], 1ull);
-        }
+        __syncthreads();  // every thread's stores of the item are done (released by the next step)
+        pending = m;
+        tk = tk_next;
+        r = r_next;
+        m = m_next;
+        p = p_next;
+        chunk = chunk_next;
+    }
+    if (pending >= 0 && threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&e.done[pending], 1ull);
     }
     // advance the device-resident launch state (block 0, after every CTA left the loop)
     grid_barrier(e);
