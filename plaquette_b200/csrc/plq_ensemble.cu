@@ -284,11 +284,60 @@ __device__ __forceinline__ int row_geometry(const Geom &g, uint32_t r, uint32_t 
     return par;
 }
 
+// Decide the n = L0 / 2 variables of one row that a pass updates.  Cs, c0s,
+// c1s, c2s: the row's state bits and the bits of each variable's count
+// (c2 c1 c0 in binary: neighbours in state 1, or satisfied staples), all
+// shifted so variable j of the pass sits at bit 2j.  Its table key is
+// cur + 2 * count, a nibble: eight variables' keys are gathered into one word
+// (pairs (cur, c0) and (c1, c2) interleaved at two-bit granularity, Hacker's
+// Delight's outer perfect shuffle without its last stage), and the key times
+// four is the byte offset of its entry in the shared-memory table tab.  The
+// draw of variable j is the keyed stream's at index v0 + j * DV.  Returns the
+// bits to flip, at 2j: Metropolis accepts when the draw is below the entry;
+// heat bath sets the new state to (entry <= draw).
+template <class W, int DV, bool HB>
+__device__ __forceinline__ W decide_row(W Cs, W c0s, W c1s, W c2s, int n, uint32_t v0, uint32_t seed32,
+                                        uint32_t sweep_mix, const uint32_t *tab) {
+    const W M = (W)0x5555555555555555ull;
+    const W P = (Cs & M) | ((c0s << 1) & ~M);
+    const W Q = (c1s & M) | ((c2s << 1) & ~M);
+    const char *tb = reinterpret_cast<const char *>(tab);
+    W out = 0;
+#pragma unroll 1
+    for (int c = 0; 8 * c < n; ++c) {
+        uint32_t x = __byte_perm((uint32_t)(P >> (16 * c)), (uint32_t)(Q >> (16 * c)), 0x5410);
+        x = __byte_perm(x, 0, 0x3120);
+        uint32_t t = (x ^ (x >> 4)) & 0x00F000F0u;
+        x ^= t ^ (t << 4);
+        t = (x ^ (x >> 2)) & 0x0C0C0C0Cu;
+        x ^= t ^ (t << 2);
+        const int m = n - 8 * c;
+        const uint32_t vc = v0 + (uint32_t)(8 * c * DV);
+        uint32_t o = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (i < m) {
+                const uint32_t key4 = i == 0 ? (x << 2) & 0x3Cu : (x >> (4 * i - 2)) & 0x3Cu;
+                const uint32_t e = *reinterpret_cast<const uint32_t *>(tb + key4);
+                const uint32_t k = lowbias32(lowbias32(seed32 ^ (vc + (uint32_t)(i * DV))) ^ sweep_mix) >> 8;
+                const bool b = HB ? e <= k : k < e;
+                o |= (uint32_t)b << (2 * i);
+            }
+        }
+        out |= (W)o << (16 * c);
+    }
+    if (HB) {  // new states -> flips, over the n variables
+        const W valid = 2 * n >= (int)(8 * sizeof(W)) ? ~(W)0 : (((W)1 << (2 * n)) - 1);
+        out ^= P & M & valid;
+    }
+    return out;
+}
+
 // q = 2 sites (Ising, or Potts at q = 2) packed by rows: the per-site count of
 // neighbours in state 1 comes out of the bit-sliced counter over the 2d
 // neighbour rows (d <= 3: at most 6), key cur + 2 * count as the byte body's.
 template <int D, class W>
-__device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R) {
+__device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R, const uint32_t *tab) {
     const uint32_t L0 = (uint32_t)a.g.L[0];
     const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
     const W full = L0 == 8 * sizeof(W) ? ~(W)0 : (((W)1 << L0) - 1);
@@ -311,25 +360,11 @@ __device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R
             count_add(c0, c1, c2, pk[r + (uint32_t)om[k]]);
         }
         const uint32_t x0 = (uint32_t)((a.color ^ par) & 1);
-        W flip = 0;
-        const uint32_t site_row = r * L0;
-#pragma unroll 4  // four independent draw chains in flight (unroll 2: +13 %, unroll 4: +4 % more)
-        for (uint32_t x = x0; x < L0; x += 2) {
-            const uint32_t cur = (uint32_t)(C >> x) & 1u;
-            const uint32_t cnt = ((uint32_t)(c0 >> x) & 1u) | (((uint32_t)(c1 >> x) & 1u) << 1) |
-                                 (((uint32_t)(c2 >> x) & 1u) << 2);
-            const uint32_t key = cur + 2u * cnt;
-            const uint32_t k = lowbias32(lowbias32(a.seed32 ^ (site_row + x)) ^ sweep_mix) >> 8;
-            uint32_t nv;
-            if (hb) {
-                nv = a.hb24[key] <= k ? 1u : 0u;
-            } else {
-                const uint32_t e = a.metro24[key];
-                nv = (e == 0xFFFFFFFFu || k < e) ? 1u - cur : cur;
-            }
-            flip |= (W)(nv ^ cur) << x;
-        }
-        pk[r] = C ^ flip;
+        const int n = (int)(L0 / 2);
+        const uint32_t v0 = r * L0 + x0;  // the keyed stream's index of the row's first variable
+        const W flip = hb ? decide_row<W, 2, true>(C >> x0, c0 >> x0, c1 >> x0, c2 >> x0, n, v0, a.seed32, sweep_mix, tab)
+                          : decide_row<W, 2, false>(C >> x0, c0 >> x0, c1 >> x0, c2 >> x0, n, v0, a.seed32, sweep_mix, tab);
+        pk[r] = C ^ (flip << x0);
     }
 }
 
@@ -374,7 +409,7 @@ __device__ long long packed_energy_rows(const LocalArgs &a, const W *pk, int lin
 }
 
 template <int D>
-__device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk, int R) {
+__device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk, int R, const uint32_t *tab) {
     // (rows of at most 32 links)
     const uint32_t L0 = (uint32_t)a.g.L[0];
     const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
@@ -405,7 +440,7 @@ __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk
         for (int k = 1; k < D; ++k)
             if (k == mu) op_mu = op[k];
         const uint32_t Umu = pk[(uint32_t)mu * rows + r];
-        uint32_t c0 = 0, c1 = 0, c2 = 0;  // unsatisfied staples per link
+        uint32_t c0 = 0, c1 = 0, c2 = 0;  // satisfied staples per link
 #pragma unroll
         for (int nu = 0; nu < D; ++nu) {
             if (nu == mu) continue;
@@ -415,7 +450,7 @@ __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk
             const uint32_t nu_s = Pnu[r];
             const uint32_t nu_smu = mu == 0 ? row_xp(nu_s, L0, full) : Pnu[r + (uint32_t)op_mu];
             const uint32_t mu_snu = nu == 0 ? row_xp(Umu, L0, full) : Pmu[r + (uint32_t)op[nu]];
-            count_add(c0, c1, c2, nu_smu ^ mu_snu ^ nu_s);
+            count_add(c0, c1, c2, ~(nu_smu ^ mu_snu ^ nu_s));
             // backward: U_nu(s+mu-nu) U_mu(s-nu) U_nu(s-nu)
             uint32_t nu_smn, mu_smn, nu_smumn;
             if (nu == 0) {
@@ -427,28 +462,18 @@ __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk
                 mu_smn = Pmu[r + (uint32_t)om[nu]];
                 nu_smumn = mu == 0 ? row_xp(nu_smn, L0, full) : Pnu[r + (uint32_t)op_mu + (uint32_t)om[nu]];
             }
-            count_add(c0, c1, c2, nu_smumn ^ mu_smn ^ nu_smn);
+            count_add(c0, c1, c2, ~(nu_smumn ^ mu_smn ^ nu_smn));
         }
-        // the links of the pass's parity: x with (x + par) % 2 == colour
+        // the links of the pass's parity: x with (x + par) % 2 == colour; the byte body's key
+        // cur + 4(d-1) - 2 * unsatisfied is cur + 2 * satisfied
         const uint32_t x0 = (uint32_t)((a.color ^ par) & 1);
-        uint32_t flip = 0;
-        const uint32_t var_row = r * L0 * (uint32_t)D + (uint32_t)mu;
-#pragma unroll 4  // four independent draw chains in flight (unroll 2: +13 %, unroll 4: +4 % more)
-        for (uint32_t x = x0; x < L0; x += 2) {
-            const uint32_t cur = (Umu >> x) & 1u;
-            const uint32_t uns = ((c0 >> x) & 1u) | (((c1 >> x) & 1u) << 1) | (((c2 >> x) & 1u) << 2);
-            const uint32_t key = cur + 4u * (uint32_t)(D - 1) - 2u * uns;
-            const uint32_t k = lowbias32(lowbias32(a.seed32 ^ (var_row + x * (uint32_t)D)) ^ sweep_mix) >> 8;
-            uint32_t nv;
-            if (hb) {
-                nv = a.hb24[key] <= k ? 1u : 0u;
-            } else {
-                const uint32_t e = a.metro24[key];
-                nv = (e == 0xFFFFFFFFu || k < e) ? 1u - cur : cur;
-            }
-            flip |= (nv ^ cur) << x;
-        }
-        pk[(uint32_t)mu * rows + r] = Umu ^ flip;
+        const int n = (int)(L0 / 2);
+        const uint32_t v0 = (r * L0 + x0) * (uint32_t)D + (uint32_t)mu;  // keyed index of link (x0, r, mu)
+        const uint32_t flip = hb ? decide_row<uint32_t, 2 * D, true>(Umu >> x0, c0 >> x0, c1 >> x0, c2 >> x0, n, v0,
+                                                                     a.seed32, sweep_mix, tab)
+                                 : decide_row<uint32_t, 2 * D, false>(Umu >> x0, c0 >> x0, c1 >> x0, c2 >> x0, n, v0,
+                                                                      a.seed32, sweep_mix, tab);
+        pk[(uint32_t)mu * rows + r] = Umu ^ (flip << x0);
     }
 }
 
@@ -712,14 +737,15 @@ __device__ void wait_member(const EnsArgs &e, int m, unsigned long long t, int p
 // barriers (all its items of the sweep are done and released by then); every
 // CTA crosses every sweep end, in order, so all take the same barriers.
 //
-// Between two items three threads work side by side: thread 0 takes the next
-// ticket and waits for the member, thread 32 loads the pass fields, thread 64
-// releases the previous item; the item's index entries are loaded while the
-// item before it runs.
+// Between two items three warps work side by side: thread 0 takes the next
+// ticket and waits for the member, threads 32-47 load the pass fields and (a
+// packed member's) decision table, thread 64 releases the previous item; the
+// item's index entries are loaded while the item before it runs.
 template <int R, bool WORDS_ONLY>
 __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
     __shared__ unsigned long long s_ticket;
+    __shared__ uint32_t s_tab[16];  // a packed member's decision table (keys cur + 2 * count < 16)
     const unsigned long long n_items = (unsigned long long)e.sp_begin[e.n_sp];
     const unsigned long long total = n_items * e.sweeps;
     if (threadIdx.x == 0) s_ticket = atomicAdd(&e.ls->ticket, 1ull);
@@ -765,12 +791,17 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
         }
         if (tk >= total) break;
         PassFields pf;
+        uint32_t tv = 0;
+        const EnsMember &mem = e.members[m];
         if (threadIdx.x == 0) {
             const unsigned long long next = atomicAdd(&e.ls->ticket, 1ull);  // used after this item
             wait_member(e, m, r, p);
             s_ticket = next;
-        } else if (threadIdx.x == 32) {
+        } else if (threadIdx.x >= 32 && threadIdx.x < 48) {
             pf = pass_fields(e, m, p, r);
+            const int k = (int)threadIdx.x - 32;
+            const int nk = 2 + 4 * (mem.link ? mem.a.g.d - 1 : mem.a.g.d);  // keys of a q = 2 table
+            if (mem.pk && k < nk) tv = (mem.a.kernel == PLQ_HEATBATH ? pf.hb24 : pf.metro24)[k];
         } else if (threadIdx.x == 64 && pending >= 0) {
             __threadfence();
             atomicAdd(&e.done[pending], 1ull);
@@ -783,6 +814,7 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
         }
         __syncthreads();  // the wait is over, the previous item released, the arguments loaded
         if (threadIdx.x == 32) apply(pf, sa);
+        if (threadIdx.x >= 32 && threadIdx.x < 48) s_tab[threadIdx.x - 32] = tv;
         // the next item's index entries, loaded while this one runs
         const unsigned long long tk_next = s_ticket;
         unsigned long long r_next = 0;
@@ -796,24 +828,23 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
             chunk_next = e.item_chunk[i];
         }
         __syncthreads();
-        const EnsMember &mem = e.members[m];
         if (mem.pk && mem.link) {
             uint32_t *pk = static_cast<uint32_t *>(mem.pk);
             switch (sa.g.d) {
-                case 2: packed_link_item<2>(sa, pk, chunk, mem.wpt); break;
-                case 3: packed_link_item<3>(sa, pk, chunk, mem.wpt); break;
-                case 4: packed_link_item<4>(sa, pk, chunk, mem.wpt); break;
+                case 2: packed_link_item<2>(sa, pk, chunk, mem.wpt, s_tab); break;
+                case 3: packed_link_item<3>(sa, pk, chunk, mem.wpt, s_tab); break;
+                case 4: packed_link_item<4>(sa, pk, chunk, mem.wpt, s_tab); break;
                 default: break;
             }
         } else if (mem.pk) {
             if (mem.pk_wide) {
                 uint64_t *pk = static_cast<uint64_t *>(mem.pk);
-                if (sa.g.d == 2) packed_site_item<2, uint64_t>(sa, pk, chunk, mem.wpt);
-                else packed_site_item<3, uint64_t>(sa, pk, chunk, mem.wpt);
+                if (sa.g.d == 2) packed_site_item<2, uint64_t>(sa, pk, chunk, mem.wpt, s_tab);
+                else packed_site_item<3, uint64_t>(sa, pk, chunk, mem.wpt, s_tab);
             } else {
                 uint32_t *pk = static_cast<uint32_t *>(mem.pk);
-                if (sa.g.d == 2) packed_site_item<2, uint32_t>(sa, pk, chunk, mem.wpt);
-                else packed_site_item<3, uint32_t>(sa, pk, chunk, mem.wpt);
+                if (sa.g.d == 2) packed_site_item<2, uint32_t>(sa, pk, chunk, mem.wpt, s_tab);
+                else packed_site_item<3, uint32_t>(sa, pk, chunk, mem.wpt, s_tab);
             }
         } else {
             run_item<R, WORDS_ONLY>(sa, sa.g.d, mem.link, chunk, mem.wpt);
