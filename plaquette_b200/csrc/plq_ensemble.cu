@@ -265,21 +265,32 @@ __device__ __forceinline__ void count_add(W &c0, W &c1, W &c2, W v) {
 __device__ __forceinline__ int popc_w(uint32_t v) { return __popc(v); }
 __device__ __forceinline__ int popc_w(uint64_t v) { return __popcll(v); }
 
+// Rows of a lattice (sites over directions >= 1): L1 * L2 * ... (extents past
+// d are 1), by multiplication.
+__host__ __device__ __forceinline__ uint32_t row_count(const Geom &g) {
+    uint32_t n = 1;
+#pragma unroll
+    for (int k = 1; k < kMaxD; ++k) n *= (uint32_t)g.L[k];
+    return n;
+}
+
 // Row r's coordinates along directions 1..D-1: their parity and the row
-// offsets to the +k / -k neighbour rows (periodic).
+// offsets to the +k / -k neighbour rows (periodic).  The row stride of
+// direction k is L1 * ... * L(k-1).
 template <int D>
-__device__ __forceinline__ int row_geometry(const Geom &g, uint32_t r, uint32_t L0, int32_t *op, int32_t *om) {
+__device__ __forceinline__ int row_geometry(const Geom &g, uint32_t r, int32_t *op, int32_t *om) {
     uint32_t rr = r;
     int par = 0;
+    int32_t rs = 1;
 #pragma unroll
     for (int k = 1; k < D; ++k) {
         const uint32_t q = fdiv(rr, g.dm[k], g.dl[k]);
         const int32_t c = (int32_t)(rr - q * (uint32_t)g.L[k]);
         rr = q;
         par += c;
-        const int32_t rs = (int32_t)(g.stride[k] / (int64_t)L0);
         op[k] = c + 1 < g.L[k] ? rs : -(g.L[k] - 1) * rs;
         om[k] = c > 0 ? -rs : (g.L[k] - 1) * rs;
+        rs *= g.L[k];
     }
     return par;
 }
@@ -339,7 +350,7 @@ __device__ __forceinline__ W decide_row(W Cs, W c0s, W c1s, W c2s, int n, uint32
 template <int D, class W>
 __device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R, const uint32_t *tab) {
     const uint32_t L0 = (uint32_t)a.g.L[0];
-    const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
+    const uint32_t rows = row_count(a.g);
     const W full = L0 == 8 * sizeof(W) ? ~(W)0 : (((W)1 << L0) - 1);
     const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
     const bool hb = a.kernel == PLQ_HEATBATH;
@@ -349,7 +360,7 @@ __device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R
         const uint32_t r = r0 + (uint32_t)i;
         if (r >= rows) break;
         int32_t op[4] = {0, 0, 0, 0}, om[4] = {0, 0, 0, 0};
-        const int par = row_geometry<D>(a.g, r, L0, op, om);
+        const int par = row_geometry<D>(a.g, r, op, om);
         const W C = pk[r];
         W c0 = 0, c1 = 0, c2 = 0;
         count_add(c0, c1, c2, row_xp(C, L0, full));
@@ -374,12 +385,12 @@ __device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R
 template <int D, class W>
 __device__ long long packed_energy_rows(const LocalArgs &a, const W *pk, int link, int64_t c) {
     const uint32_t L0 = (uint32_t)a.g.L[0];
-    const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
+    const uint32_t rows = row_count(a.g);
     const W full = L0 == 8 * sizeof(W) ? ~(W)0 : (((W)1 << L0) - 1);
     const uint32_t r = (uint32_t)(c * (int64_t)blockDim.x) + threadIdx.x;
     if (r >= rows) return 0;
     int32_t op[4] = {0, 0, 0, 0}, om[4] = {0, 0, 0, 0};
-    row_geometry<D>(a.g, r, L0, op, om);
+    row_geometry<D>(a.g, r, op, om);
     long long acc = 0;
     if (!link) {
         const W C = pk[r];
@@ -412,7 +423,7 @@ template <int D>
 __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk, int R, const uint32_t *tab) {
     // (rows of at most 32 links)
     const uint32_t L0 = (uint32_t)a.g.L[0];
-    const uint32_t rows = (uint32_t)(a.g.n_sites / L0);
+    const uint32_t rows = row_count(a.g);
     const int mu = a.dir;
     const uint32_t full = L0 == 32 ? 0xFFFFFFFFu : ((1u << L0) - 1u);
     const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
@@ -423,18 +434,7 @@ __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk
         const uint32_t r = r0 + (uint32_t)i;
         if (r >= rows) break;
         int32_t op[4] = {0, 0, 0, 0}, om[4] = {0, 0, 0, 0};
-        uint32_t rr = r;
-        int par = 0;
-#pragma unroll
-        for (int k = 1; k < D; ++k) {
-            const uint32_t q = fdiv(rr, a.g.dm[k], a.g.dl[k]);
-            const int32_t c = (int32_t)(rr - q * (uint32_t)a.g.L[k]);
-            rr = q;
-            par += c;
-            const int32_t rs = (int32_t)(a.g.stride[k] / (int64_t)L0);
-            op[k] = c + 1 < a.g.L[k] ? rs : -(a.g.L[k] - 1) * rs;
-            om[k] = c > 0 ? -rs : (a.g.L[k] - 1) * rs;
-        }
+        const int par = row_geometry<D>(a.g, r, op, om);
         int32_t op_mu = 0;
 #pragma unroll
         for (int k = 1; k < D; ++k)
@@ -699,7 +699,7 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 // Work items per colour pass of member m (as append_items cuts them).
 __device__ __forceinline__ unsigned long long member_chunks(const EnsArgs &e, int m) {
     const EnsMember &mem = e.members[m];
-    const long long units = mem.pk ? mem.a.g.n_sites / mem.a.g.L[0]
+    const long long units = mem.pk ? (long long)row_count(mem.a.g)
                                    : (mem.a.words ? mem.a.g.n_sites / 4 : mem.a.g.n_sites / 2);
     const long long chunk = (long long)kEnsThreads * (mem.pk || mem.a.words ? mem.wpt : e.ranks);
     return (unsigned long long)((units + chunk - 1) / chunk);
