@@ -306,6 +306,38 @@ __device__ __forceinline__ int row_geometry(const Geom &g, uint32_t r, int32_t *
 // draw of variable j is the keyed stream's at index v0 + j * DV.  Returns the
 // bits to flip, at 2j: Metropolis accepts when the draw is below the entry;
 // heat bath sets the new state to (entry <= draw).
+// Eight (or, TAIL, the first m < 8) variables of a row from their key word x
+// (nibble i: variable i's key): the flip or new-state bits at 2i.
+template <int DV, bool HB, bool TAIL>
+__device__ __forceinline__ uint32_t decide8(uint32_t x, int m, uint32_t vc, uint32_t seed32, uint32_t sweep_mix,
+                                            const char *tb) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!TAIL || i < m) {
+            const uint32_t key4 = i == 0 ? (x << 2) & 0x3Cu : (x >> (4 * i - 2)) & 0x3Cu;
+            const uint32_t e = *reinterpret_cast<const uint32_t *>(tb + key4);
+            const uint32_t k = lowbias32(lowbias32(seed32 ^ (vc + (uint32_t)(i * DV))) ^ sweep_mix) >> 8;
+            const bool b = HB ? e <= k : k < e;
+            o |= (uint32_t)b << (2 * i);
+        }
+    }
+    return o;
+}
+
+// The key word of variables 8c .. 8c + 7: pairs (cur, c0) of P and (c1, c2)
+// of Q interleaved at two-bit granularity.
+template <class W>
+__device__ __forceinline__ uint32_t key_word(W P, W Q, int c) {
+    uint32_t x = __byte_perm((uint32_t)(P >> (16 * c)), (uint32_t)(Q >> (16 * c)), 0x5410);
+    x = __byte_perm(x, 0, 0x3120);
+    uint32_t t = (x ^ (x >> 4)) & 0x00F000F0u;
+    x ^= t ^ (t << 4);
+    t = (x ^ (x >> 2)) & 0x0C0C0C0Cu;
+    x ^= t ^ (t << 2);
+    return x;
+}
+
 template <class W, int DV, bool HB>
 __device__ __forceinline__ W decide_row(W Cs, W c0s, W c1s, W c2s, int n, uint32_t v0, uint32_t seed32,
                                         uint32_t sweep_mix, const uint32_t *tab) {
@@ -314,29 +346,15 @@ __device__ __forceinline__ W decide_row(W Cs, W c0s, W c1s, W c2s, int n, uint32
     const W Q = (c1s & M) | ((c2s << 1) & ~M);
     const char *tb = reinterpret_cast<const char *>(tab);
     W out = 0;
+    const int full = n >> 3;
 #pragma unroll 1
-    for (int c = 0; 8 * c < n; ++c) {
-        uint32_t x = __byte_perm((uint32_t)(P >> (16 * c)), (uint32_t)(Q >> (16 * c)), 0x5410);
-        x = __byte_perm(x, 0, 0x3120);
-        uint32_t t = (x ^ (x >> 4)) & 0x00F000F0u;
-        x ^= t ^ (t << 4);
-        t = (x ^ (x >> 2)) & 0x0C0C0C0Cu;
-        x ^= t ^ (t << 2);
-        const int m = n - 8 * c;
-        const uint32_t vc = v0 + (uint32_t)(8 * c * DV);
-        uint32_t o = 0;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (i < m) {
-                const uint32_t key4 = i == 0 ? (x << 2) & 0x3Cu : (x >> (4 * i - 2)) & 0x3Cu;
-                const uint32_t e = *reinterpret_cast<const uint32_t *>(tb + key4);
-                const uint32_t k = lowbias32(lowbias32(seed32 ^ (vc + (uint32_t)(i * DV))) ^ sweep_mix) >> 8;
-                const bool b = HB ? e <= k : k < e;
-                o |= (uint32_t)b << (2 * i);
-            }
-        }
-        out |= (W)o << (16 * c);
-    }
+    for (int c = 0; c < full; ++c)
+        out |= (W)decide8<DV, HB, false>(key_word(P, Q, c), 8, v0 + (uint32_t)(8 * c * DV), seed32, sweep_mix, tb)
+               << (16 * c);
+    if (n & 7)
+        out |= (W)decide8<DV, HB, true>(key_word(P, Q, full), n & 7, v0 + (uint32_t)(8 * full * DV), seed32,
+                                        sweep_mix, tb)
+               << (16 * full);
     if (HB) {  // new states -> flips, over the n variables
         const W valid = 2 * n >= (int)(8 * sizeof(W)) ? ~(W)0 : (((W)1 << (2 * n)) - 1);
         out ^= P & M & valid;
@@ -699,9 +717,10 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 // Work items per colour pass of member m (as append_items cuts them).
 __device__ __forceinline__ unsigned long long member_chunks(const EnsArgs &e, int m) {
     const EnsMember &mem = e.members[m];
-    const long long units = mem.pk ? (long long)row_count(mem.a.g)
-                                   : (mem.a.words ? mem.a.g.n_sites / 4 : mem.a.g.n_sites / 2);
-    const long long chunk = (long long)kEnsThreads * (mem.pk || mem.a.words ? mem.wpt : e.ranks);
+    // (32-bit: variables < 2^31, a chunk < 2^16)
+    const uint32_t units = mem.pk ? row_count(mem.a.g)
+                                  : (uint32_t)(mem.a.words ? mem.a.g.n_sites / 4 : mem.a.g.n_sites / 2);
+    const uint32_t chunk = (uint32_t)kEnsThreads * (uint32_t)(mem.pk || mem.a.words ? mem.wpt : e.ranks);
     return (unsigned long long)((units + chunk - 1) / chunk);
 }
 
