@@ -124,6 +124,16 @@ struct LaunchState {
     unsigned long long ticket;      // next work-item ticket of the running launch (zero between launches)
 };
 
+// One work item: `count` consecutive chunks, from `chunk`, of one colour pass
+// of one member (index relative to the launch's member array).  16 bytes:
+// the kernel fetches it with one load.
+struct alignas(16) WorkItem {
+    int32_t member;
+    int32_t chunk;
+    int32_t count;
+    int32_t pass;  // colour pass (link members: 2 * direction + parity)
+};
+
 struct EnsArgs {
     EnsMember *members;
     int n_members;
@@ -131,11 +141,8 @@ struct EnsArgs {
     int32_t *ts_of_member;
     unsigned long long *pos;  // stream heat bath: per-member stream position (relative)
     unsigned long long *msweep;  // per-member sweep counters (serving), or null: all share ls->sweep
-    const int32_t *item_member;
-    const int32_t *item_chunk;
-    const int8_t *item_pass;   // colour pass of the item (link members: 2 * direction + parity)
-    const int64_t *sp_begin;
-    int n_sp;
+    const WorkItem *items;     // one sweep's items, super-phase by super-phase
+    int64_t n_items;
     const int32_t *e_item_member;
     const int32_t *e_item_chunk;
     int64_t n_e_items;
@@ -759,37 +766,37 @@ __device__ void wait_member(const EnsArgs &e, int m, unsigned long long t, int p
 // Between two items three warps work side by side: thread 0 takes the next
 // ticket and waits for the member, threads 32-47 load the pass fields and (a
 // packed member's) decision table, thread 64 releases the previous item; the
-// item's index entries are loaded while the item before it runs.
+// next item's entry is loaded while this one runs.  An item is a run of
+// chunks of one pass (more than one where a super-phase holds far more chunks
+// than the grid has CTAs); the CTA runs them back to back and releases them
+// together.
 template <int R, bool WORDS_ONLY>
 __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kernel(EnsArgs e) {
     __shared__ LocalArgs sa;
     __shared__ unsigned long long s_ticket;
     __shared__ uint32_t s_tab[16];  // a packed member's decision table (keys cur + 2 * count < 16)
-    const unsigned long long n_items = (unsigned long long)e.sp_begin[e.n_sp];
+    const unsigned long long n_items = (unsigned long long)e.n_items;
     const unsigned long long total = n_items * e.sweeps;
     if (threadIdx.x == 0) s_ticket = atomicAdd(&e.ls->ticket, 1ull);
     __syncthreads();
     unsigned long long tk = s_ticket;
     unsigned long long r = 0;  // the ticket's sweep
-    int m = -1, p = 0;         // the ticket's item: member, pass, chunk
-    int64_t chunk = 0;
+    WorkItem it{0, 0, 0, 0};  // ... and item
     if (tk < total) {
         r = tk / n_items;
-        const int64_t i = (int64_t)(tk - r * n_items);
-        m = e.item_member[i];
-        p = e.item_pass[i];
-        chunk = e.item_chunk[i];
+        it = e.items[tk - r * n_items];
     }
     unsigned long long round = 0;  // sweeps whose end this CTA has crossed
     int last_m = -1;               // the member whose arguments are in sa
     int pending = -1;              // member of the last item run, not yet released
+    int pending_n = 0;             // ... and its chunks
     for (;;) {
         const unsigned long long r_at = tk < total ? r : e.sweeps;
         if (round < r_at) {
             if (pending >= 0) {  // release it before any tempering barrier
                 if (threadIdx.x == 0) {
                     __threadfence();
-                    atomicAdd(&e.done[pending], 1ull);
+                    atomicAdd(&e.done[pending], (unsigned long long)pending_n);
                 }
                 pending = -1;
             }
@@ -809,6 +816,7 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
             }
         }
         if (tk >= total) break;
+        const int m = it.member, p = it.pass;
         PassFields pf;
         uint32_t tv = 0;
         const EnsMember &mem = e.members[m];
@@ -823,7 +831,7 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
             if (mem.pk && k < nk) tv = (mem.a.kernel == PLQ_HEATBATH ? pf.hb24 : pf.metro24)[k];
         } else if (threadIdx.x == 64 && pending >= 0) {
             __threadfence();
-            atomicAdd(&e.done[pending], 1ull);
+            atomicAdd(&e.done[pending], (unsigned long long)pending_n);
         }
         if (m != last_m) {  // the member's arguments into shared memory, one 32-bit word per thread
             const uint32_t *src = reinterpret_cast<const uint32_t *>(&e.members[m].a);
@@ -834,51 +842,49 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
         __syncthreads();  // the wait is over, the previous item released, the arguments loaded
         if (threadIdx.x == 32) apply(pf, sa);
         if (threadIdx.x >= 32 && threadIdx.x < 48) s_tab[threadIdx.x - 32] = tv;
-        // the next item's index entries, loaded while this one runs
+        // the next item's entry, loaded while this one runs
         const unsigned long long tk_next = s_ticket;
         unsigned long long r_next = 0;
-        int m_next = -1, p_next = 0;
-        int64_t chunk_next = 0;
+        WorkItem it_next{0, 0, 0, 0};
         if (tk_next < total) {
             r_next = tk_next / n_items;
-            const int64_t i = (int64_t)(tk_next - r_next * n_items);
-            m_next = e.item_member[i];
-            p_next = e.item_pass[i];
-            chunk_next = e.item_chunk[i];
+            it_next = e.items[tk_next - r_next * n_items];
         }
         __syncthreads();
-        if (mem.pk && mem.link) {
-            uint32_t *pk = static_cast<uint32_t *>(mem.pk);
-            switch (sa.g.d) {
-                case 2: packed_link_item<2>(sa, pk, chunk, mem.wpt, s_tab); break;
-                case 3: packed_link_item<3>(sa, pk, chunk, mem.wpt, s_tab); break;
-                case 4: packed_link_item<4>(sa, pk, chunk, mem.wpt, s_tab); break;
-                default: break;
-            }
-        } else if (mem.pk) {
-            if (mem.pk_wide) {
-                uint64_t *pk = static_cast<uint64_t *>(mem.pk);
-                if (sa.g.d == 2) packed_site_item<2, uint64_t>(sa, pk, chunk, mem.wpt, s_tab);
-                else packed_site_item<3, uint64_t>(sa, pk, chunk, mem.wpt, s_tab);
-            } else {
+        for (int q = 0; q < it.count; ++q) {
+            const int64_t chunk = (int64_t)it.chunk + q;
+            if (mem.pk && mem.link) {
                 uint32_t *pk = static_cast<uint32_t *>(mem.pk);
-                if (sa.g.d == 2) packed_site_item<2, uint32_t>(sa, pk, chunk, mem.wpt, s_tab);
-                else packed_site_item<3, uint32_t>(sa, pk, chunk, mem.wpt, s_tab);
+                switch (sa.g.d) {
+                    case 2: packed_link_item<2>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 3: packed_link_item<3>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 4: packed_link_item<4>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    default: break;
+                }
+            } else if (mem.pk) {
+                if (mem.pk_wide) {
+                    uint64_t *pk = static_cast<uint64_t *>(mem.pk);
+                    if (sa.g.d == 2) packed_site_item<2, uint64_t>(sa, pk, chunk, mem.wpt, s_tab);
+                    else packed_site_item<3, uint64_t>(sa, pk, chunk, mem.wpt, s_tab);
+                } else {
+                    uint32_t *pk = static_cast<uint32_t *>(mem.pk);
+                    if (sa.g.d == 2) packed_site_item<2, uint32_t>(sa, pk, chunk, mem.wpt, s_tab);
+                    else packed_site_item<3, uint32_t>(sa, pk, chunk, mem.wpt, s_tab);
+                }
+            } else {
+                run_item<R, WORDS_ONLY>(sa, sa.g.d, mem.link, chunk, mem.wpt);
             }
-        } else {
-            run_item<R, WORDS_ONLY>(sa, sa.g.d, mem.link, chunk, mem.wpt);
         }
         __syncthreads();  // every thread's stores of the item are done (released by the next step)
         pending = m;
+        pending_n = it.count;
         tk = tk_next;
         r = r_next;
-        m = m_next;
-        p = p_next;
-        chunk = chunk_next;
+        it = it_next;
     }
     if (pending >= 0 && threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(&e.done[pending], 1ull);
+        atomicAdd(&e.done[pending], (unsigned long long)pending_n);
     }
     // advance the device-resident launch state (block 0, after every CTA left the loop)
     grid_barrier(e);
@@ -937,10 +943,8 @@ struct plq_ensemble {
     int ranks = 4;
     int ctas_per_sm = 2;
     bool words_only = false;  // every member runs four sites at a time
-    int32_t *d_item_member = nullptr, *d_item_chunk = nullptr;
-    int8_t *d_item_pass = nullptr;
-    int64_t *d_sp_begin = nullptr;
-    int n_sp = 0;
+    WorkItem *d_items = nullptr;
+    int64_t n_items = 0;
     int32_t *d_e_member = nullptr, *d_e_chunk = nullptr;
     int64_t n_e_items = 0;
     uint64_t launches = 0;
@@ -1006,75 +1010,85 @@ int64_t item_cost(const EnsMember &mem, int64_t c, int ranks) {
 }
 
 // Work items of one sweep of members `ids`, by super-phase; member indices
-// are relative to lo, and super-phase bounds are appended to spb (the last
-// one too).  With S super-phases (the most colour passes of any member),
-// pass p of a member with P passes runs in super-phases [p S / P,
+// are relative to lo.  With S super-phases (the most colour passes of any
+// member), pass p of a member with P passes runs in super-phases [p S / P,
 // (p + 1) S / P), its chunks split evenly over them: a site lattice's two
 // colours each spread over half the super-phases, a 4D gauge lattice's eight
 // passes one per super-phase, so every super-phase holds a similar share of
-// the sweep and each pass still ends (at a grid barrier) before the member's
-// next pass begins.  A member's items hold 256 * wpt four-site words or
-// packed rows (256 * ranks colour ranks in the generic body).  Each
-// super-phase lists its items largest first (item_cost), as the kernel deals
-// them out in list order.  Returns S.
-int append_items(const EnsMember *mems, const std::vector<size_t> &ids, size_t lo, int ranks,
-                 std::vector<int32_t> &im, std::vector<int32_t> &ic, std::vector<int8_t> &ip,
-                 std::vector<int64_t> &spb) {
+// the sweep.  A chunk is 256 * wpt four-site words or packed rows (256 *
+// ranks colour ranks in the generic body).  Where a super-phase holds more
+// than 2 * min_items chunks, an item takes a run of g of a pass's consecutive
+// chunks (g = chunks / min_items) to keep the per-item overhead small; else
+// one.  Each super-phase lists its items largest first (item_cost times
+// count), as the kernel deals them out in list order.  Returns S.
+int append_items(const EnsMember *mems, const std::vector<size_t> &ids, size_t lo, int ranks, int64_t min_items,
+                 std::vector<WorkItem> &items) {
     int S = 0;
     for (size_t m : ids) S = std::max(S, mems[m].passes);
+    struct Span {
+        size_t m;
+        int p;
+        int64_t c0, c1;
+    };
     for (int sp = 0; sp < S; ++sp) {
-        const size_t first = im.size();
-        spb.push_back((int64_t)first);
+        std::vector<Span> spans;
+        int64_t chunks = 0;
         for (size_t m : ids) {
             const int P = mems[m].passes;
             const LocalArgs &ma = mems[m].a;
-            // work per item: 256 * ranks colour ranks, or 256 * wpt four-site words or packed rows
             const bool shaped = ma.words || mems[m].pk;
             const int64_t chunk = (int64_t)kEnsThreads * (shaped ? mems[m].wpt : ranks);
-            const int64_t units = mems[m].pk ? ma.g.n_sites / ma.g.L[0] : (ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2);
+            const int64_t units = mems[m].pk ? (int64_t)row_count(ma.g) : (ma.words ? ma.g.n_sites / 4 : ma.g.n_sites / 2);
             const int64_t nc = (units + chunk - 1) / chunk;
             for (int p = 0; p < P; ++p) {
                 const int p0 = p * S / P, p1 = (p + 1) * S / P;
                 if (sp < p0 || sp >= p1) continue;
                 const int64_t c0 = (int64_t)(sp - p0) * nc / (p1 - p0), c1 = (int64_t)(sp - p0 + 1) * nc / (p1 - p0);
-                for (int64_t c = c0; c < c1; ++c) {
-                    im.push_back((int32_t)(m - lo));
-                    ic.push_back((int32_t)c);
-                    ip.push_back((int8_t)p);
-                }
+                if (c1 > c0) spans.push_back(Span{m, p, c0, c1});
+                chunks += c1 - c0;
             }
         }
+        const int64_t g = min_items > 0 && chunks > 2 * min_items ? chunks / min_items : 1;
+        const size_t first = items.size();
+        for (const Span &sn : spans)
+            for (int64_t c = sn.c0; c < sn.c1; c += g)
+                items.push_back(WorkItem{(int32_t)(sn.m - lo), (int32_t)c, (int32_t)std::min(g, sn.c1 - c), sn.p});
         // largest first; equal costs keep member order
-        const size_t n = im.size() - first;
+        const size_t n = items.size() - first;
         std::vector<int64_t> cost(n);
+        for (size_t k = 0; k < n; ++k) {
+            const WorkItem &w = items[first + k];
+            cost[k] = item_cost(mems[(size_t)w.member + lo], w.chunk, ranks) * w.count;
+        }
         std::vector<size_t> ord(n);
-        for (size_t k = 0; k < n; ++k) {
-            cost[k] = item_cost(mems[im[first + k] + lo], ic[first + k], ranks);
-            ord[k] = k;
-        }
+        for (size_t k = 0; k < n; ++k) ord[k] = k;
         std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
-        std::vector<int32_t> tm(n), tc(n);
-        std::vector<int8_t> tp(n);
-        for (size_t k = 0; k < n; ++k) {
-            tm[k] = im[first + ord[k]];
-            tc[k] = ic[first + ord[k]];
-            tp[k] = ip[first + ord[k]];
-        }
-        std::copy(tm.begin(), tm.end(), im.begin() + first);
-        std::copy(tc.begin(), tc.end(), ic.begin() + first);
-        std::copy(tp.begin(), tp.end(), ip.begin() + first);
+        std::vector<WorkItem> sorted(n);
+        for (size_t k = 0; k < n; ++k) sorted[k] = items[first + ord[k]];
+        std::copy(sorted.begin(), sorted.end(), items.begin() + first);
     }
-    spb.push_back((int64_t)im.size());
     return S;
 }
 
+// Items per super-phase below which chunks are not grouped into runs, per SM
+// (about four per CTA at four CTAs per SM).
+constexpr int64_t kItemsPerSm = 16;
+
+// The launch's item list must name only its own members (the kernel indexes
+// the member array with it unchecked).
+bool items_in_range(const WorkItem *items, size_t n, size_t n_members) {
+    for (size_t k = 0; k < n; ++k)
+        if (items[k].member < 0 || (size_t)items[k].member >= n_members || items[k].count <= 0) return false;
+    return true;
+}
+
 int build_items(plq_ensemble *E) {
-    std::vector<int32_t> im, ic;
-    std::vector<int8_t> ip;
-    std::vector<int64_t> spb;
+    std::vector<WorkItem> items;
     std::vector<size_t> all(E->members.size());
     for (size_t m = 0; m < all.size(); ++m) all[m] = m;
-    const int max_passes = append_items(E->members.data(), all, 0, E->ranks, im, ic, ip, spb);
+    append_items(E->members.data(), all, 0, E->ranks, kItemsPerSm * E->ctx->sm_count, items);
+    if (!items_in_range(items.data(), items.size(), E->members.size()))
+        return plq_fail(PLQ_EINVAL, "ensemble work items name a member out of range");
     std::vector<int32_t> em, ec;
     for (auto &l : E->ladders)
         for (int32_t m : l) {
@@ -1087,21 +1101,18 @@ int build_items(plq_ensemble *E) {
                 ec.push_back((int32_t)c);
             }
         }
-    void *old[] = {E->d_item_member, E->d_item_chunk, E->d_item_pass, E->d_sp_begin, E->d_e_member, E->d_e_chunk};
+    void *old[] = {E->d_items, E->d_e_member, E->d_e_chunk};
     for (void *p : old)
         if (p) {
             cudaFree(p);
             E->allocs.erase(std::remove(E->allocs.begin(), E->allocs.end(), p), E->allocs.end());
         }
-    cudaError_t e = dev_upload(E, im.data(), im.size(), &E->d_item_member);
-    if (e == cudaSuccess) e = dev_upload(E, ic.data(), ic.size(), &E->d_item_chunk);
-    if (e == cudaSuccess) e = dev_upload(E, ip.data(), ip.size(), &E->d_item_pass);
-    if (e == cudaSuccess) e = dev_upload(E, spb.data(), spb.size(), &E->d_sp_begin);
+    cudaError_t e = dev_upload(E, items.data(), items.size(), &E->d_items);
     if (e == cudaSuccess) e = dev_upload(E, em.data(), em.size(), &E->d_e_member);
     if (e == cudaSuccess) e = dev_upload(E, ec.data(), ec.size(), &E->d_e_chunk);
     if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
     if (e != cudaSuccess) return ens_fail(e, "ensemble work items");
-    E->n_sp = max_passes;
+    E->n_items = (int64_t)items.size();
     E->n_e_items = (int64_t)em.size();
     drop_graph(E);
     return PLQ_OK;
@@ -1116,11 +1127,8 @@ EnsArgs ens_args(plq_ensemble *E, uint64_t sweeps) {
     a.ts_of_member = E->d_ts;
     a.pos = E->d_pos;
     a.done = E->d_done;
-    a.item_member = E->d_item_member;
-    a.item_chunk = E->d_item_chunk;
-    a.item_pass = E->d_item_pass;
-    a.sp_begin = E->d_sp_begin;
-    a.n_sp = E->n_sp;
+    a.items = E->d_items;
+    a.n_items = E->n_items;
     a.e_item_member = E->d_e_member;
     a.e_item_chunk = E->d_e_chunk;
     a.n_e_items = E->n_e_items;
@@ -1727,48 +1735,32 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
         double best_g = 1e300;
         for (int wpt : {1, 2, 4, 8}) {
             for (size_t m : ids) E->members[m].wpt = wpt;
-            std::vector<int32_t> im, ic;
-            std::vector<int8_t> ip;
-            std::vector<int64_t> spb;
-            const int n_sp = append_items(E->members.data(), ids, 0, E->ranks, im, ic, ip, spb);
+            std::vector<WorkItem> items;
+            append_items(E->members.data(), ids, 0, E->ranks, kItemsPerSm * E->ctx->sm_count, items);
             uint32_t g_total = 0;
             const std::vector<PackEntry> g_tab = pack_entries(E, ids, g_total);
             PackEntry *d_gtab = nullptr;
-            int32_t *d_im = nullptr, *d_ic = nullptr;
-            int8_t *d_ip = nullptr;
-            int64_t *d_spb = nullptr;
-            e = cudaSuccess;
-            if (!g_tab.empty()) {
+            WorkItem *d_items = nullptr;
+            e = items_in_range(items.data(), items.size(), E->members.size()) ? cudaSuccess : cudaErrorInvalidValue;
+            if (e == cudaSuccess && !g_tab.empty()) {
                 e = cudaMalloc((void **)&d_gtab, g_tab.size() * sizeof(PackEntry));
                 if (e == cudaSuccess)
                     e = cudaMemcpyAsync(d_gtab, g_tab.data(), g_tab.size() * sizeof(PackEntry), cudaMemcpyHostToDevice,
                                         E->stream);
             }
-            if (e == cudaSuccess) e = cudaMalloc((void **)&d_im, im.size() * sizeof(int32_t));
-            if (e == cudaSuccess) e = cudaMalloc((void **)&d_ic, ic.size() * sizeof(int32_t));
-            if (e == cudaSuccess) e = cudaMalloc((void **)&d_ip, ip.size() * sizeof(int8_t));
-            if (e == cudaSuccess) e = cudaMalloc((void **)&d_spb, spb.size() * sizeof(int64_t));
+            if (e == cudaSuccess) e = cudaMalloc((void **)&d_items, items.size() * sizeof(WorkItem));
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(E->d_members, E->members.data(), E->members.size() * sizeof(EnsMember),
                                     cudaMemcpyHostToDevice, E->stream);
             if (e == cudaSuccess)
-                e = cudaMemcpyAsync(d_im, im.data(), im.size() * sizeof(int32_t), cudaMemcpyHostToDevice, E->stream);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(d_ic, ic.data(), ic.size() * sizeof(int32_t), cudaMemcpyHostToDevice, E->stream);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(d_ip, ip.data(), ip.size() * sizeof(int8_t), cudaMemcpyHostToDevice, E->stream);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(d_spb, spb.data(), spb.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                e = cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice,
                                     E->stream);
             float ms = 0;
             for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // warm-up, then timed
                 snapshot(false);
                 EnsArgs a = ens_args(E, rep == 0 ? 1 : (uint64_t)trial_sweeps);
-                a.item_member = d_im;
-                a.item_chunk = d_ic;
-                a.item_pass = d_ip;
-                a.sp_begin = d_spb;
-                a.n_sp = n_sp;
+                a.items = d_items;
+                a.n_items = (int64_t)items.size();
                 a.n_ladders = 0;
                 a.pt_every = 0;
                 cudaEventRecord(t0, E->stream);
@@ -1777,10 +1769,7 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
                 if (e == cudaSuccess) e = cudaEventSynchronize(t1);
                 if (e == cudaSuccess) cudaEventElapsedTime(&ms, t0, t1);
             }
-            cudaFree(d_im);
-            cudaFree(d_ic);
-            cudaFree(d_ip);
-            cudaFree(d_spb);
+            if (d_items) cudaFree(d_items);
             if (d_gtab) cudaFree(d_gtab);
             if (e != cudaSuccess) break;
             if (ms < best_g) {
@@ -2223,14 +2212,12 @@ struct TickBuffers {
     TableSet *tsets = nullptr;
     int32_t *ts = nullptr;
     unsigned long long *pos = nullptr, *msweep = nullptr, *done = nullptr;
-    int32_t *im = nullptr, *ic = nullptr;
-    int8_t *ip = nullptr;
-    int64_t *spb = nullptr;
+    WorkItem *items = nullptr;
     LaunchState *ls = nullptr;
     Control *ctrl = nullptr;
     size_t cap_members = 0, cap_items = 0;
     void release() {
-        void *ps[] = {members, tsets, ts, pos, msweep, done, im, ic, ip, spb, ls, ctrl};
+        void *ps[] = {members, tsets, ts, pos, msweep, done, items, ls, ctrl};
         for (void *p : ps)
             if (p) cudaFree(p);
         *this = TickBuffers();
@@ -2262,14 +2249,16 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
     // ranks per thread: 4 for the words-only kernel; 2 for the full kernel, whose generic
     // body needs the registers (2 CTAs per SM instead of 1)
     const int ranks_w = 4, ranks_g = 2;
-    std::vector<int32_t> im, ic;
-    std::vector<int8_t> ip;
-    std::vector<int64_t> spb;
+    std::vector<WorkItem> items;
     std::vector<size_t> ids_w, ids_g;
     for (size_t k = 0; k < n; ++k) (k < nw ? ids_w : ids_g).push_back(k);
-    const int sp_w = nw ? append_items(mems.data(), ids_w, 0, ranks_w, im, ic, ip, spb) : 0;
-    const size_t spb_g = spb.size();
-    const int sp_g = n > nw ? append_items(mems.data(), ids_g, nw, ranks_g, im, ic, ip, spb) : 0;
+    const int64_t min_items = kItemsPerSm * S->ctx->sm_count;
+    if (nw) append_items(mems.data(), ids_w, 0, ranks_w, min_items, items);
+    const size_t n_w_items = items.size();  // the second group's items follow the first's
+    if (n > nw) append_items(mems.data(), ids_g, nw, ranks_g, min_items, items);
+    if (!items_in_range(items.data(), n_w_items, nw) ||
+        !items_in_range(items.data() + n_w_items, items.size() - n_w_items, n - nw))
+        return plq_fail(PLQ_EINVAL, "serving work items name a member out of range");
     cudaError_t e = cudaSuccess;
     if (!B.ls) {
         e = cudaMalloc((void **)&B.ls, sizeof(LaunchState));
@@ -2294,35 +2283,26 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         if (e == cudaSuccess) e = cudaMemsetAsync(B.done, 0, c * sizeof(unsigned long long), stream);
         B.cap_members = c;
     }
-    if (e == cudaSuccess && B.cap_items < im.size() + 1) {
-        cudaFree(B.im);
-        cudaFree(B.ic);
-        cudaFree(B.ip);
-        cudaFree(B.spb);
-        size_t c = std::max<size_t>(im.size() + 1, 2 * B.cap_items);
-        e = cudaMalloc((void **)&B.im, c * sizeof(int32_t));
-        if (e == cudaSuccess) e = cudaMalloc((void **)&B.ic, c * sizeof(int32_t));
-        if (e == cudaSuccess) e = cudaMalloc((void **)&B.ip, c * sizeof(int8_t));
-        if (e == cudaSuccess) e = cudaMalloc((void **)&B.spb, 64 * sizeof(int64_t));
+    if (e == cudaSuccess && B.cap_items < items.size() + 1) {
+        cudaFree(B.items);
+        B.items = nullptr;
+        size_t c = std::max<size_t>(items.size() + 1, 2 * B.cap_items);
+        e = cudaMalloc((void **)&B.items, c * sizeof(WorkItem));
         B.cap_items = c;
     }
     if (e != cudaSuccess) return plq_fail(PLQ_ENOMEM, std::string("tick buffers: ") + cudaGetErrorString(e));
-    if (spb.size() > 64) return plq_fail(PLQ_EINVAL, "too many passes per sweep for a serving tick");
     cudaMemcpyAsync(B.members, mems.data(), n * sizeof(EnsMember), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.tsets, tss.data(), n * sizeof(TableSet), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.ts, ts.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.pos, pos.data(), n * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(B.msweep, msw.data(), n * sizeof(unsigned long long), cudaMemcpyHostToDevice, stream);
-    if (!im.empty()) {
-        cudaMemcpyAsync(B.im, im.data(), im.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
-        cudaMemcpyAsync(B.ic, ic.data(), ic.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream);
-        cudaMemcpyAsync(B.ip, ip.data(), ip.size() * sizeof(int8_t), cudaMemcpyHostToDevice, stream);
-    }
-    cudaMemcpyAsync(B.spb, spb.data(), spb.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream);
-    // one cooperative launch per member group; item indices in the second group's
-    // super-phase bounds continue the first group's, member indices restart at its offset
-    auto launch = [&](size_t lo, size_t hi, int n_sp, size_t spb_off, bool words_only, int ranks) -> cudaError_t {
-        if (hi == lo || n_sp == 0) return cudaSuccess;
+    if (!items.empty())
+        cudaMemcpyAsync(B.items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, stream);
+    // one cooperative launch per member group, each over its own part of the item list
+    // (member indices relative to the group's first member)
+    auto launch = [&](size_t lo, size_t hi, size_t item_lo, size_t item_hi, bool words_only,
+                      int ranks) -> cudaError_t {
+        if (hi == lo || item_hi == item_lo) return cudaSuccess;
         EnsArgs a;
         std::memset(&a, 0, sizeof a);
         a.members = B.members + lo;
@@ -2332,11 +2312,8 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         a.pos = B.pos + lo;
         a.msweep = B.msweep + lo;
         a.done = B.done + lo;
-        a.item_member = B.im;
-        a.item_chunk = B.ic;
-        a.item_pass = B.ip;
-        a.sp_begin = B.spb + spb_off;
-        a.n_sp = n_sp;
+        a.items = B.items + item_lo;
+        a.n_items = (int64_t)(item_hi - item_lo);
         a.ls = B.ls;
         a.ctrl = B.ctrl;
         a.sweeps = sweeps;
@@ -2347,8 +2324,8 @@ int run_tick(plq_server *S, TickBuffers &B, cudaStream_t stream, uint64_t sweeps
         S->launches++;
         return cudaLaunchCooperativeKernel(kernel_ptr(ranks, words_only), grid, dim3(kEnsThreads), params, 0, stream);
     };
-    e = launch(0, nw, sp_w, 0, true, ranks_w);
-    if (e == cudaSuccess) e = launch(nw, n, sp_g, spb_g, false, ranks_g);
+    e = launch(0, nw, 0, n_w_items, true, ranks_w);
+    if (e == cudaSuccess) e = launch(nw, n, n_w_items, items.size(), false, ranks_g);
     unsigned int status = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &B.ctrl->status, sizeof status, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);

@@ -31,6 +31,11 @@ def _jobs():
         (plq.GAUGE, 2, (8, 8, 8, 8), plq.HEATBATH, plq.RNG_KEYED, 0.4407, 15, 40),
         (plq.GAUGE, 2, (6, 6, 6, 6), plq.METROPOLIS, plq.RNG_KEYED, 0.45, 16, 0),
         (plq.ISING, 2, (256, 128), plq.HEATBATH, plq.RNG_STREAM, 0.4406868, 17, 25),
+        # generic-body jobs (q = 5; an extent that is not a multiple of four) beside the four-site
+        # ones: every tick then makes two launches, the second over item lists that continue the
+        # first's
+        (plq.POTTS, 5, (10, 10, 10), plq.HEATBATH, plq.RNG_KEYED, 0.62, 18, 90),
+        (plq.GAUGE, 2, (6, 6, 6, 6), plq.HEATBATH, plq.RNG_KEYED, 0.45, 19, 60),
     ]
     out = []
     for kind, q, shape, upd, rng, beta, seed, sweeps in specs:
