@@ -961,7 +961,9 @@ struct plq_ensemble {
     // every member's primaries: one device buffer, the launches captured once
     long long *d_prims_all = nullptr;
     std::vector<int64_t> prims_offset;  // member m's first entry
-    cudaGraphExec_t prims_graph = nullptr;
+    PrimTask *d_prim_tasks = nullptr;   // every member's measurement task (the states never move)
+    int32_t *d_prim_task = nullptr, *d_prim_chunk = nullptr;
+    int64_t n_prim_items = 0;
 };
 
 namespace {
@@ -1287,6 +1289,7 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
     //    and one synchronisation for the whole ensemble rather than several per member
     auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
     std::vector<Tables> tables(n);
+    std::map<std::string, int32_t> table_of;  // host build of each distinct parameter set
     std::vector<std::vector<AffineHost>> jumps(n);
     size_t state_bytes = 0, table_bytes = 0, stage_bytes = 0;
     for (int32_t m = 0; m < n; ++m) {
@@ -1332,8 +1335,20 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         p.j = d.j;
         p.h = d.h;
         for (int k = 0; k < PLQ_MAX_Q; ++k) p.offsets[k] = d.offsets[k];
-        std::string err;
-        if (!build_tables(p, d.updater, d.rng, tables[m], err)) return fail(plq_fail(PLQ_EUNSUPPORTED, err));
+        // members with the same model parameters, updater and stream share one host build (the
+        // device copies stay per member: a member's tables are rewritten in place when its beta
+        // changes)
+        std::string key(reinterpret_cast<const char *>(&p), sizeof p);
+        key.append(reinterpret_cast<const char *>(&d.updater), sizeof d.updater);
+        key.append(reinterpret_cast<const char *>(&d.rng), sizeof d.rng);
+        auto built = table_of.find(key);
+        if (built != table_of.end()) {
+            tables[m] = tables[built->second];
+        } else {
+            std::string err;
+            if (!build_tables(p, d.updater, d.rng, tables[m], err)) return fail(plq_fail(PLQ_EUNSUPPORTED, err));
+            table_of.emplace(std::move(key), m);
+        }
         const Tables &t = tables[m];
         table_bytes += align(t.hb53.size() * 8) + align(t.hb24.size() * 4) + align(t.metro53.size() * 8) +
                        align(t.metro24.size() * 4);
@@ -1364,13 +1379,15 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         return fail(ens_fail(ce, "ensemble arenas"));
     }
     // 2. the uploads, in stream order: starts (links through one staging buffer and the
-    //    plane conversion), tables and jump tables
+    //    plane conversion), then every table and jump table laid out in one host image of the
+    //    table arena and copied in one transfer
     size_t soff = 0, toff = 0;
+    std::vector<uint8_t> table_image(std::max<size_t>(table_bytes, 256), 0);
     auto put = [&](const void *host, size_t bytes) -> void * {
         if (!bytes) return nullptr;
         void *dst = table_arena + toff;
+        std::memcpy(table_image.data() + toff, host, bytes);
         toff += align(bytes);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, E->stream);
         return dst;
     };
     for (int32_t m = 0; m < n && ce == cudaSuccess; ++m) {
@@ -1407,6 +1424,8 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         E->ts_of_member[m] = (int32_t)E->tsets.size();
         E->tsets.push_back(ts);
     }
+    if (ce == cudaSuccess && toff)
+        ce = cudaMemcpyAsync(table_arena, table_image.data(), toff, cudaMemcpyHostToDevice, E->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->stream);
     if (stage) cudaFree(stage);
     if (ce != cudaSuccess) return fail(ens_fail(ce, "member set-up"));
@@ -1511,10 +1530,11 @@ extern "C" int plq_ensemble_add_ladder(plq_ensemble *E, int32_t k, const int32_t
         if (!same)
             return plq_fail(PLQ_EINVAL, "ladder members must share model, shape, updater and coupling, with no field");
     }
-    // slot i of the ladder runs at betas[i]: rebuild member i's table set at that beta
+    // slot i of the ladder runs at betas[i]: rebuild member i's table set at that beta (unless
+    // it already runs at it; members outside ladders keep their own table set)
     for (int32_t i = 0; i < k; ++i) {
         const int32_t m = ids[i];
-        const int rc = rebuild_tables(E, m, betas[i], false);
+        const int rc = E->tsets[E->ts_of_member[m]].beta == betas[i] ? PLQ_OK : rebuild_tables(E, m, betas[i], false);
         if (rc != PLQ_OK) return rc;
         E->members[m].ladder = (int)E->ladders.size();
     }
@@ -1931,9 +1951,8 @@ extern "C" int plq_ensemble_primaries_all(plq_ensemble *E, int64_t *out, int32_t
     const size_t n = E->members.size();
     cudaError_t e = plq_enter_device(E->ctx->device);
     if (e != cudaSuccess) return ens_fail(e, "cudaSetDevice");
-    if (!E->prims_graph) {
-        // one buffer for all members, and every member's measurement launches
-        // captured once (the state buffers never move)
+    if (!E->d_prim_tasks) {
+        // one buffer for all members, a task per member and its work items (built once)
         E->prims_offset.assign(n + 1, 0);
         for (size_t m = 0; m < n; ++m)
             E->prims_offset[m + 1] =
@@ -1941,28 +1960,35 @@ extern "C" int plq_ensemble_primaries_all(plq_ensemble *E, int64_t *out, int32_t
         e = cudaMalloc((void **)&E->d_prims_all, sizeof(long long) * (size_t)E->prims_offset[n]);
         if (e != cudaSuccess) return ens_fail(e, "primaries buffer");
         E->allocs.push_back(E->d_prims_all);
-        cudaGraph_t g = nullptr;
-        e = cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal);
-        for (size_t m = 0; m < n && e == cudaSuccess; ++m) {
+        std::vector<PrimTask> tasks(n);
+        std::vector<int32_t> it_task, it_chunk;
+        for (size_t m = 0; m < n; ++m) {
             const EnsMember &mem = E->members[m];
-            e = launch_primaries(mem.a.state, mem.a.g, mem.a.model, mem.a.q, E->d_prims_all + E->prims_offset[m],
-                                 E->stream);
+            tasks[m] = PrimTask{mem.a.state, mem.a.g, mem.a.model, mem.a.q, E->d_prims_all + E->prims_offset[m]};
+            for (int64_t c = 0; c * kPrimChunk < mem.a.g.n_sites; ++c) {
+                it_task.push_back((int32_t)m);
+                it_chunk.push_back((int32_t)c);
+            }
         }
-        cudaError_t e2 = cudaStreamEndCapture(E->stream, &g);
-        if (e == cudaSuccess) e = e2;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&E->prims_graph, g, 0);
-        if (g) cudaGraphDestroy(g);
+        e = dev_upload(E, it_task.data(), it_task.size(), &E->d_prim_task);
+        if (e == cudaSuccess) e = dev_upload(E, it_chunk.data(), it_chunk.size(), &E->d_prim_chunk);
+        if (e == cudaSuccess) e = dev_upload(E, tasks.data(), tasks.size(), &E->d_prim_tasks);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
         if (e != cudaSuccess) {
-            E->prims_graph = nullptr;
-            return ens_fail(e, "primaries graph");
+            E->d_prim_tasks = nullptr;
+            return ens_fail(e, "primaries tasks");
         }
+        E->n_prim_items = (int64_t)it_task.size();
     }
     for (size_t m = 0; m < n; ++m) {
         const int64_t np = E->prims_offset[m + 1] - E->prims_offset[m];
         if (np > stride) return plq_fail(PLQ_EINVAL, "stride is below a member's primaries count");
     }
     std::vector<long long> host((size_t)E->prims_offset[n]);
-    e = cudaGraphLaunch(E->prims_graph, E->stream);
+    e = cudaMemsetAsync(E->d_prims_all, 0, sizeof(long long) * host.size(), E->stream);
+    if (e == cudaSuccess)
+        e = launch_primaries_multi(E->d_prim_tasks, E->d_prim_task, E->d_prim_chunk, E->n_prim_items,
+                                   E->ctx->sm_count, E->stream);
     E->launches++;
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(host.data(), E->d_prims_all, sizeof(long long) * host.size(), cudaMemcpyDeviceToHost,
@@ -2001,7 +2027,6 @@ extern "C" void plq_ensemble_destroy(plq_ensemble *E) {
     if (E->ctx) plq_enter_device(E->ctx->device);
     if (E->stream) cudaStreamSynchronize(E->stream);
     drop_graph(E);
-    if (E->prims_graph) cudaGraphExecDestroy(E->prims_graph);
     for (void *p : E->allocs) cudaFree(p);
     if (E->stream) cudaStreamDestroy(E->stream);
     delete E;

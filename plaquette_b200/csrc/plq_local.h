@@ -23,6 +23,19 @@ int primaries_count(int model, int q);
 cudaError_t launch_primaries(const uint8_t *state, const Geom &g, int model, int q,
                              long long *out, cudaStream_t stream);
 
+// Many configurations' primaries in one launch (d <= 4): task k's values go
+// to tasks[k].out, which must be zero before the launch; work item i covers
+// sites [item_chunk[i] * kPrimChunk, ...) of task item_task[i].
+constexpr int64_t kPrimChunk = 16384;
+struct PrimTask {
+    const uint8_t *state;
+    Geom g;
+    int model, q;
+    long long *out;
+};
+cudaError_t launch_primaries_multi(const PrimTask *tasks, const int32_t *item_task, const int32_t *item_chunk,
+                                   int64_t n_items, int sm_count, cudaStream_t stream);
+
 // Layout conversion of link variables: host order (site*d + dir) <-> device
 // planes (dir*n_sites + site).
 cudaError_t launch_links_to_planes(const uint8_t *in, uint8_t *out, int64_t n_sites, int d,

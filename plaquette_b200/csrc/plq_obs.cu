@@ -10,6 +10,8 @@
 // warp (per-block shared counters for the Potts label counts).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/plaquette.h"
 #include "plq_device.cuh"
 #include "plq_local.h"
@@ -24,50 +26,51 @@ __device__ __forceinline__ long long warp_sum(long long v) {
     return v;
 }
 
+// One site's (or, gauge, one site's plaquettes') contribution to the
+// primaries: acc0 the bond / agreement / plaquette sum, acc1 the Ising spin
+// sum; Potts labels counted in the block's shared counters.
 template <int D>
-__global__ void __launch_bounds__(kObsThreads)
-primaries_kernel(const uint8_t *state, Geom g, int model, int q, long long *out) {
-    __shared__ int s_counts[64];
-    if (model == PLQ_POTTS)
-        for (int i = threadIdx.x; i < q; i += blockDim.x) s_counts[i] = 0;
-    __syncthreads();
-    long long acc0 = 0, acc1 = 0;
+__device__ __forceinline__ void site_primaries(const uint8_t *state, const Geom &g, int model, int64_t s,
+                                               long long &acc0, long long &acc1, int *s_counts) {
     const int64_t n = g.n_sites;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        int32_t x[D];
-        uint32_t t = (uint32_t)s;
+    int32_t x[D];
+    uint32_t t = (uint32_t)s;
+#pragma unroll
+    for (int mu = 0; mu < D; ++mu) {
+        uint32_t qq = fdiv(t, g.dm[mu], g.dl[mu]);
+        x[mu] = (int32_t)(t - qq * (uint32_t)g.L[mu]);
+        t = qq;
+    }
+    if (model == PLQ_GAUGE) {
+        // plaquettes (s, mu, nu), mu < nu: U_mu(s) U_nu(s+mu) U_mu(s+nu) U_nu(s)
 #pragma unroll
         for (int mu = 0; mu < D; ++mu) {
-            uint32_t qq = fdiv(t, g.dm[mu], g.dl[mu]);
-            x[mu] = (int32_t)(t - qq * (uint32_t)g.L[mu]);
-            t = qq;
+            int64_t s_mu = x[mu] + 1 < g.L[mu] ? s + g.stride[mu] : s - (int64_t)(g.L[mu] - 1) * g.stride[mu];
+#pragma unroll
+            for (int nu = mu + 1; nu < D; ++nu) {
+                int64_t s_nu = x[nu] + 1 < g.L[nu] ? s + g.stride[nu] : s - (int64_t)(g.L[nu] - 1) * g.stride[nu];
+                int b = state[mu * n + s] ^ state[nu * n + s_mu] ^ state[mu * n + s_nu] ^ state[nu * n + s];
+                acc0 += 1 - 2 * b;
+            }
         }
-        if (model == PLQ_GAUGE) {
-            // plaquettes (s, mu, nu), mu < nu: U_mu(s) U_nu(s+mu) U_mu(s+nu) U_nu(s)
+    } else {
+        int si = state[s];
+        if (model == PLQ_ISING) acc1 += 1 - 2 * si;
+        else atomicAdd(&s_counts[si], 1);
 #pragma unroll
-            for (int mu = 0; mu < D; ++mu) {
-                int64_t s_mu = x[mu] + 1 < g.L[mu] ? s + g.stride[mu] : s - (int64_t)(g.L[mu] - 1) * g.stride[mu];
-#pragma unroll
-                for (int nu = mu + 1; nu < D; ++nu) {
-                    int64_t s_nu = x[nu] + 1 < g.L[nu] ? s + g.stride[nu] : s - (int64_t)(g.L[nu] - 1) * g.stride[nu];
-                    int b = state[mu * n + s] ^ state[nu * n + s_mu] ^ state[mu * n + s_nu] ^ state[nu * n + s];
-                    acc0 += 1 - 2 * b;
-                }
-            }
-        } else {
-            int si = state[s];
-            if (model == PLQ_ISING) acc1 += 1 - 2 * si;
-            else atomicAdd(&s_counts[si], 1);
-#pragma unroll
-            for (int mu = 0; mu < D; ++mu) {
-                int64_t s_mu = x[mu] + 1 < g.L[mu] ? s + g.stride[mu] : s - (int64_t)(g.L[mu] - 1) * g.stride[mu];
-                int sj = state[s_mu];
-                if (model == PLQ_ISING) acc0 += (1 - 2 * si) * (1 - 2 * sj);
-                else acc0 += si == sj;
-            }
+        for (int mu = 0; mu < D; ++mu) {
+            int64_t s_mu = x[mu] + 1 < g.L[mu] ? s + g.stride[mu] : s - (int64_t)(g.L[mu] - 1) * g.stride[mu];
+            int sj = state[s_mu];
+            if (model == PLQ_ISING) acc0 += (1 - 2 * si) * (1 - 2 * sj);
+            else acc0 += si == sj;
         }
     }
+}
+
+// The block's partial sums into out (one 64-bit atomic per warp; the Potts
+// label counters after a barrier).
+__device__ __forceinline__ void flush_primaries(long long acc0, long long acc1, int model, int q, int *s_counts,
+                                                long long *out) {
     acc0 = warp_sum(acc0);
     acc1 = warp_sum(acc1);
     if ((threadIdx.x & 31) == 0) {
@@ -79,6 +82,60 @@ primaries_kernel(const uint8_t *state, Geom g, int model, int q, long long *out)
         for (int i = threadIdx.x; i < q; i += blockDim.x)
             if (s_counts[i]) atomicAdd((unsigned long long *)&out[1 + i], (unsigned long long)s_counts[i]);
     }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kObsThreads)
+primaries_kernel(const uint8_t *state, Geom g, int model, int q, long long *out) {
+    __shared__ int s_counts[64];
+    if (model == PLQ_POTTS)
+        for (int i = threadIdx.x; i < q; i += blockDim.x) s_counts[i] = 0;
+    __syncthreads();
+    long long acc0 = 0, acc1 = 0;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < g.n_sites;
+         s += (int64_t)gridDim.x * blockDim.x)
+        site_primaries<D>(state, g, model, s, acc0, acc1, s_counts);
+    flush_primaries(acc0, acc1, model, q, s_counts, out);
+}
+
+// Many configurations' primaries in one launch: work item i is sites
+// [chunk * kPrimChunk, (chunk + 1) * kPrimChunk) of task item_task[i]; a CTA
+// takes items grid-stride.  The outputs must be zero before the launch.
+template <int D>
+__device__ __forceinline__ void primaries_item(const PrimTask &t, int64_t chunk, int *s_counts) {
+    long long acc0 = 0, acc1 = 0;
+    const int64_t end = min(t.g.n_sites, (chunk + 1) * kPrimChunk);
+    for (int64_t s = chunk * kPrimChunk + threadIdx.x; s < end; s += blockDim.x)
+        site_primaries<D>(t.state, t.g, t.model, s, acc0, acc1, s_counts);
+    flush_primaries(acc0, acc1, t.model, t.q, s_counts, t.out);
+}
+
+__global__ void __launch_bounds__(kObsThreads)
+primaries_multi_kernel(const PrimTask *tasks, const int32_t *item_task, const int32_t *item_chunk, int64_t n_items) {
+    __shared__ int s_counts[64];
+    for (int64_t i = blockIdx.x; i < n_items; i += gridDim.x) {
+        const PrimTask &t = tasks[item_task[i]];
+        if (t.model == PLQ_POTTS) {
+            for (int k = threadIdx.x; k < t.q; k += blockDim.x) s_counts[k] = 0;
+            __syncthreads();
+        }
+        switch (t.g.d) {
+            case 1: primaries_item<1>(t, item_chunk[i], s_counts); break;
+            case 2: primaries_item<2>(t, item_chunk[i], s_counts); break;
+            case 3: primaries_item<3>(t, item_chunk[i], s_counts); break;
+            case 4: primaries_item<4>(t, item_chunk[i], s_counts); break;
+            default: break;
+        }
+        __syncthreads();  // the counters and the task are reused by the next item
+    }
+}
+
+cudaError_t launch_primaries_multi(const PrimTask *tasks, const int32_t *item_task, const int32_t *item_chunk,
+                                   int64_t n_items, int sm_count, cudaStream_t stream) {
+    if (n_items <= 0) return cudaSuccess;
+    const int64_t blocks = std::min<int64_t>(n_items, (int64_t)sm_count * 8);
+    primaries_multi_kernel<<<(unsigned)blocks, kObsThreads, 0, stream>>>(tasks, item_task, item_chunk, n_items);
+    return cudaGetLastError();
 }
 
 // Fast path for site models with extent 0 a multiple of 16 and q <= 8: a

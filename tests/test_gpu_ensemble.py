@@ -143,6 +143,14 @@ def test_four_site_members_match_their_own_chains(gpu):
 
 def test_primaries_of_every_member_at_once(gpu):
     descs, starts = _members()
+    # members larger than one measurement work item (16384 sites): several items each
+    for kind, q, shape, seed in ((plq.ISING, 2, (64, 64, 8), 8), (plq.POTTS, 3, (40, 40, 20), 9),
+                                 (plq.GAUGE, 2, (12, 12, 12, 12), 10)):
+        n = int(np.prod(shape)) * (len(shape) if kind == plq.GAUGE else 1)
+        start, off = plq.hot_start(seed, q, n)
+        descs.append(plq.make_desc(kind, q, shape, plq.HEATBATH, beta=0.3, seed=seed, rng=plq.RNG_KEYED,
+                                   stream_offset=off, sweeps_between=1, batch=1))
+        starts.append(start)
     ens = Ensemble(gpu, descs, starts)
     for sweeps in (0, 4, 3):
         ens.advance(sweeps) if sweeps else None
