@@ -328,6 +328,38 @@ int plq_ising_metropolis_noalloc(uint8_t *spins, int32_t d, const int64_t *shape
                                  double beta, uint64_t seed, uint64_t stream_offset, uint64_t sweeps,
                                  void *cuda_stream, uint64_t *stream_position_out);
 
+/* ----------------------------------------------------------- slabs */
+/* No counterpart in the reference (one chain per adapter, src/device.rs:31-78).
+ * One lattice split across devices along its last axis: a slab holds planes
+ * [z0, z0 + nz) of the site lattice `desc` describes (Ising or Potts, d = 2 or
+ * 3, keyed stream, Metropolis or heat bath) plus one halo plane on each side.
+ * Before each colour pass the caller fills the halos with the neighbouring
+ * slabs' boundary planes (the previous slab's last plane into the low halo,
+ * the next slab's first plane into the high one; the ring is periodic); the
+ * pass then updates that colour (global parity) on the slab's planes with the
+ * whole lattice's draws, so the slabs together equal the single chain.
+ * `start` holds the slab's nz planes in the reference's site order.  A slab's
+ * handle is not thread-safe; its work runs on a stream of its own. */
+typedef struct plq_slab plq_slab;
+#define PLQ_SLAB_LOW_HALO 0
+#define PLQ_SLAB_FIRST_PLANE 1
+#define PLQ_SLAB_LAST_PLANE 2
+#define PLQ_SLAB_HIGH_HALO 3
+int plq_slab_create(plq_ctx *ctx, const plq_chain_desc *desc, int64_t z0, int64_t nz, const uint8_t *start,
+                    plq_slab **out);
+/* Device address and size in bytes of one of the four exchange planes. */
+int plq_slab_plane(plq_slab *s, int32_t which, void **device_ptr, int64_t *bytes);
+/* One colour pass (0 or 1: the parity of the site's coordinate sum) at the
+ * slab's sweep index, queued on its stream. */
+int plq_slab_pass(plq_slab *s, int32_t colour);
+/* The sweep is complete: later passes draw at the next sweep index. */
+int plq_slab_end_sweep(plq_slab *s);
+/* Waits for the slab's queued work (before its planes are exchanged). */
+int plq_slab_sync(plq_slab *s);
+/* The slab's nz planes to host memory (blocks). */
+int plq_slab_read(plq_slab *s, uint8_t *out);
+void plq_slab_destroy(plq_slab *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -130,6 +130,8 @@ def lib():
         L.orc_cluster_sweep.restype = C.c_double
         L.orc_keyed_local_sweep.argtypes = [P(_Model), P(_Lattice), u8p, C.c_int32, C.c_double,
                                             C.c_uint32, C.c_uint32]
+        L.orc_keyed_slab_pass.argtypes = [P(_Model), P(_Lattice), u8p, C.c_int32, C.c_double, C.c_uint32,
+                                          C.c_uint32, C.c_int32, C.c_int64, C.c_int64, C.c_int64]
         L.orc_keyed_cluster_sweep.argtypes = [P(_Model), P(_Lattice), u8p, C.c_int32, C.c_int32, C.c_double,
                                               C.c_uint32, C.c_uint32, i64p]
         L.orc_axis_pair_sums.argtypes = [P(_Model), P(_Lattice), u8p, i64p]
@@ -335,6 +337,16 @@ def keyed_local_sweep(model: Model, lat: Lattice, cfg: np.ndarray, kernel: int, 
         lat.build_staples()
     lib().orc_keyed_local_sweep(model.ref, C.byref(lat.lat), _u8(cfg), kernel, beta, seed32 & 0xFFFFFFFF,
                                 sweep & 0xFFFFFFFF)
+
+
+def keyed_slab_pass(model: Model, slab: Lattice, cfg: np.ndarray, kernel: int, beta: float, seed32: int,
+                    sweep: int, local_color: int, first: int, last: int, var_offset: int) -> None:
+    """One keyed colour pass (the reference WGSL site update) over sites
+    [first, last) of a slab lattice -- the slab's planes with a halo plane on
+    each side -- whose site s is site s + var_offset of the whole lattice; in
+    place.  local_color is the pass's colour in the slab's own parity."""
+    lib().orc_keyed_slab_pass(model.ref, C.byref(slab.lat), _u8(cfg), kernel, beta, seed32 & 0xFFFFFFFF,
+                              sweep & 0xFFFFFFFF, local_color, first, last, var_offset)
 
 
 def keyed_cluster_sweep(model: Model, lat: Lattice, cfg: np.ndarray, extent: int, relabel: int, beta: float,

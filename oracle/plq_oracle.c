@@ -685,8 +685,11 @@ static float keyed_energy_delta(const orc_model *m, const orc_lattice *lat, cons
 }
 
 /* metropolis.wgsl:32-63 and heat_bath.wgsl:28-62 */
+/* v indexes cfg and the lattice's tables; key_var is the variable index the
+ * keyed draws are taken at (v itself, except for a slab of a larger lattice,
+ * whose variables keep their indices in the whole lattice). */
 static void keyed_update(const orc_model *m, const orc_lattice *lat, uint8_t *cfg, int32_t kernel,
-                         float beta32, uint32_t seed32, uint32_t sweep, int64_t v) {
+                         float beta32, uint32_t seed32, uint32_t sweep, int64_t v, int64_t key_var) {
     int q = model_q(m);
     int cur = cfg[v];
     if (kernel == ORC_METROPOLIS) {
@@ -695,7 +698,7 @@ static void keyed_update(const orc_model *m, const orc_lattice *lat, uint8_t *cf
             prop = 1 - cur;
         } else {
             uint32_t alternatives = (uint32_t)(q - 1);
-            float u = orc_keyed_uniform(seed32 ^ PROPOSAL_KEY, (uint32_t)v, sweep);
+            float u = orc_keyed_uniform(seed32 ^ PROPOSAL_KEY, (uint32_t)key_var, sweep);
             float scaled = u * (float)alternatives;
             uint32_t draw = (uint32_t)scaled;
             if (draw >= alternatives) draw = alternatives - 1;
@@ -703,7 +706,7 @@ static void keyed_update(const orc_model *m, const orc_lattice *lat, uint8_t *cf
             if (prop >= cur) prop += 1;
         }
         float dE = keyed_energy_delta(m, lat, cfg, v, cur, prop);
-        float u = orc_keyed_uniform(seed32, (uint32_t)v, sweep);
+        float u = orc_keyed_uniform(seed32, (uint32_t)key_var, sweep);
         float x = (-beta32) * dE;
         if (dE <= 0.0f || u < exp32(x)) cfg[v] = (uint8_t)prop;
     } else {
@@ -723,7 +726,7 @@ static void keyed_update(const orc_model *m, const orc_lattice *lat, uint8_t *cf
             weights[s] = exp32(x);
             total = total + weights[s];
         }
-        float threshold = orc_keyed_uniform(seed32, (uint32_t)v, sweep) * total;
+        float threshold = orc_keyed_uniform(seed32, (uint32_t)key_var, sweep) * total;
         int chosen = q - 1;
         float cumulative = 0.0f;
         for (int s = 0; s + 1 < q; ++s) {
@@ -749,8 +752,23 @@ void orc_keyed_local_sweep(const orc_model *m, const orc_lattice *lat, uint8_t *
         for (int64_t site = 0; site < n; ++site) {
             if (lat->parity[site] != (color & 1)) continue;
             int64_t v = m->model == ORC_GAUGE ? site * d + (color >> 1) : site;
-            keyed_update(m, lat, cfg, kernel, beta32, seed32, sweep, v);
+            keyed_update(m, lat, cfg, kernel, beta32, seed32, sweep, v, v);
         }
+}
+
+/* One keyed colour pass of a site model over sites [first, last) of a slab:
+ * `slab` is the lattice of the slab's planes with one halo plane on each side
+ * (periodic along its last axis, which the interior sites never cross), its
+ * site s is site s + var_offset of the whole lattice, and local_color is the
+ * pass's colour in the slab's own parity. */
+void orc_keyed_slab_pass(const orc_model *m, const orc_lattice *slab, uint8_t *cfg, int32_t kernel, double beta,
+                         uint32_t seed32, uint32_t sweep, int32_t local_color, int64_t first, int64_t last,
+                         int64_t var_offset) {
+    float beta32 = (float)beta;
+    for (int64_t site = first; site < last; ++site) {
+        if (slab->parity[site] != local_color) continue;
+        keyed_update(m, slab, cfg, kernel, beta32, seed32, sweep, site, site + var_offset);
+    }
 }
 
 static int64_t root_find(int64_t *parent, int64_t x) {

@@ -136,6 +136,12 @@ double orc_cluster_sweep(const orc_model *m, const orc_lattice *lat, uint8_t *cf
  * exp is evaluated as (float)exp((double)x). */
 void orc_keyed_local_sweep(const orc_model *m, const orc_lattice *lat, uint8_t *cfg,
                            int32_t kernel, double beta, uint32_t seed32, uint32_t sweep);
+/* One keyed colour pass of a site model over sites [first, last) of a slab of
+ * a larger lattice (its planes with a halo plane on each side): draws at
+ * variable index site + var_offset, colour in the slab's own parity. */
+void orc_keyed_slab_pass(const orc_model *m, const orc_lattice *slab, uint8_t *cfg, int32_t kernel, double beta,
+                         uint32_t seed32, uint32_t sweep, int32_t local_color, int64_t first, int64_t last,
+                         int64_t var_offset);
 /* One keyed cluster sweep (cluster_prelude.wgsl + cluster_relabel.wgsl):
  * bonds keyed by bond index, clusters rooted at their minimum site index,
  * relabel keyed on the root.  root_out (n_sites, may be NULL) receives the

@@ -34,6 +34,7 @@ def test_python_binding_covers_the_header():
     plq.lib()
     import plaquette_b200.ensemble  # noqa: F401  (registers its signatures)
     import plaquette_b200.serving  # noqa: F401
+    import plaquette_b200.slabs  # noqa: F401
     assert set(declared_symbols()) <= set(plq.exported_symbols())
 
 
