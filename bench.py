@@ -531,6 +531,7 @@ def measure_ensemble(steps, warmup, ctx):
     t0 = time.perf_counter()
     e2 = build_ensemble(gpu, descs, views, ladders, seed, pt_every=PT_EVERY)
     e2.set_config(tuned_r, tuned_c)
+    t_made = time.perf_counter()
     n_prim = 0
     for _ in range(steps):
         e2.advance(PT_EVERY)
@@ -577,6 +578,7 @@ def measure_ensemble(steps, warmup, ctx):
         "e2e": {"value": round(updates / (e2e_s * 1e9), 3), "unit": "site updates/ns",
                 "h2d_bytes_per_step": n_vars / steps,
                 "d2h_bytes_per_step": 8 * n_prim + 8 * len(descs),
+                "create_ms": round((t_made - t0) * 1e3, 2), "steps_ms": round((t1 - t_made) * 1e3, 2),
                 "what": "ensemble create from pinned host starts, then K steps each followed by every member's "
                         "primaries and beta read back"},
         "gpu_launches": launches,
