@@ -444,12 +444,14 @@ __device__ long long packed_energy_rows(const LocalArgs &a, const W *pk, int lin
     return acc;
 }
 
-template <int D>
+// MU: the pass's direction (a compile-time constant, so the staple terms that
+// are row rotations and those that are other rows are fixed per variant).
+template <int D, int MU>
 __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk, int R, const uint32_t *tab) {
     // (rows of at most 32 links)
     const uint32_t L0 = (uint32_t)a.g.L[0];
     const uint32_t rows = row_count(a.g);
-    const int mu = a.dir;
+    constexpr int mu = MU;
     const uint32_t full = L0 == 32 ? 0xFFFFFFFFu : ((1u << L0) - 1u);
     const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
     const bool hb = a.kernel == PLQ_HEATBATH;
@@ -460,10 +462,7 @@ __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk
         if (r >= rows) break;
         int32_t op[4] = {0, 0, 0, 0}, om[4] = {0, 0, 0, 0};
         const int par = row_geometry<D>(a.g, r, op, om);
-        int32_t op_mu = 0;
-#pragma unroll
-        for (int k = 1; k < D; ++k)
-            if (k == mu) op_mu = op[k];
+        const int32_t op_mu = mu > 0 ? op[mu] : 0;
         const uint32_t Umu = pk[(uint32_t)mu * rows + r];
         uint32_t c0 = 0, c1 = 0, c2 = 0;  // satisfied staples per link
 #pragma unroll
@@ -855,10 +854,16 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
             const int64_t chunk = (int64_t)it.chunk + q;
             if (mem.pk && mem.link) {
                 uint32_t *pk = static_cast<uint32_t *>(mem.pk);
-                switch (sa.g.d) {
-                    case 2: packed_link_item<2>(sa, pk, chunk, mem.wpt, s_tab); break;
-                    case 3: packed_link_item<3>(sa, pk, chunk, mem.wpt, s_tab); break;
-                    case 4: packed_link_item<4>(sa, pk, chunk, mem.wpt, s_tab); break;
+                switch (sa.g.d * 4 + sa.dir) {
+                    case 8: packed_link_item<2, 0>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 9: packed_link_item<2, 1>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 12: packed_link_item<3, 0>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 13: packed_link_item<3, 1>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 14: packed_link_item<3, 2>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 16: packed_link_item<4, 0>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 17: packed_link_item<4, 1>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 18: packed_link_item<4, 2>(sa, pk, chunk, mem.wpt, s_tab); break;
+                    case 19: packed_link_item<4, 3>(sa, pk, chunk, mem.wpt, s_tab); break;
                     default: break;
                 }
             } else if (mem.pk) {
