@@ -223,11 +223,12 @@ class Ctx:
             self.pg.destroy_process_group()
 
 
-def traffic_record(name):
+def traffic_record(name, kernel=None):
     """roofline.traffic from the committed ncu summary of this kernel (not
-    measured in this run), with its source named."""
+    measured in this run), with its source named; none when the summary is of
+    another kernel than the one this run's path launches."""
     prof = profiled_traffic().get(name, {})
-    if not prof:
+    if not prof or (kernel is not None and prof.get("kernel") != kernel):
         return None, None
     return prof.get("dram_bytes_per_launch"), (f"copied from {prof.get('summary')} (one ncu capture of this "
                                                 f"kernel, {prof.get('captured', 'date in the summary')}); "
@@ -278,21 +279,30 @@ def measure_local(name, steps, warmup, ctx, e2e=True):
 
     sites_total = N_SITES * world * steps
     value = whole_job_rate(world, N_SITES, steps, dev_ms_max)
-    per_launch_ms = dev_ms / max(1, launches)
-    alg_bytes = BYTES_PER_UPDATE * N_SITES // w[7]  # per launch
+    kernel, per_sweep, l2_note = w[6], w[7], "inputs larger than L2 (134 MB state per lattice, two buffers for the " \
+                                             "out-of-place sweep)"
+    if path == "packed":
+        # two pass launches per sweep on the 16.8 MB packed copy (L2-resident), the bytes packed and
+        # unpacked once per advance call; their time is counted in the passes' average (conservative)
+        kernel = f"packed_pass_kernel<3,{'true' if w[2] == 'heatbath' else 'false'}>"
+        per_sweep = 2
+        l2_note = ("134 MB byte state read (packed) and written (unpacked) once per advance call; the sweeps run "
+                   "on a 16.8 MB bit-packed copy that stays in L2")
+    per_launch_ms = dev_ms / max(1, steps * per_sweep)
+    alg_bytes = BYTES_PER_UPDATE * N_SITES // per_sweep  # per launch of the dominant kernel
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic, traffic_src = traffic_record(name)
+    traffic, traffic_src = traffic_record(name, kernel)
     line = {
         "metric": "site updates/ns", "value": round(value, 3), "unit": "site updates/ns", "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": round(dev_ms_max / steps, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": w[5], "name": name, "sites_per_gpu": N_SITES, "step": "one sweep",
-                   "l2": "inputs larger than L2 (134 MB state per lattice, two buffers for the out-of-place sweep)",
+                   "l2": l2_note,
                    "parallelism": f"independent lattice per GPU x{world}", "path": path},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
-                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes, "kernel": w[6],
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes, "kernel": kernel,
                      "note": "instruction-issue bound: the reference's per-site RNG (a 128-bit LCG step or "
                              "two 32-bit hashes per draw) costs more issue slots than HBM allows at 2 B/update"},
         "gpu_launches": launches,

@@ -51,8 +51,9 @@ enum plq_updater { PLQ_METROPOLIS = 0, PLQ_HEATBATH = 1, PLQ_CLUSTER = 2 };
 enum plq_extent { PLQ_EXTENT_ALL = 0, PLQ_EXTENT_SEEDED = 1 };       /* updater.rs:358-373 */
 enum plq_relabel { PLQ_RELABEL_REDRAW = 0, PLQ_RELABEL_FORCED = 1 }; /* updater.rs:377-395 */
 enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
-/* Force the per-colour pass kernels even where the fused two-colour sweep
- * applies (both give identical results; used to check one against the other). */
+/* Force the per-colour pass kernels even where the fused two-colour sweep or
+ * the bit-packed passes apply (all give identical results; used to check one
+ * against the other). */
 #define PLQ_FLAG_NO_FUSED 1
 /* Cap every cluster-labelling find and union at one step, so any real merge
  * trips the cap: exercises the PLQ_ECAP path (gpu_cluster.rs:512-518) on the
@@ -68,6 +69,10 @@ enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
  * where the four-sites-at-a-time body applies (both give identical results;
  * used to check one against the other). */
 #define PLQ_FLAG_GENERIC_PASS 8
+/* Keep a q = 2 keyed site chain on its byte passes (the fused sweep or the
+ * four-sites-at-a-time body) where the bit-packed passes apply (identical
+ * results; used to test the byte paths). */
+#define PLQ_FLAG_NO_PACKED 16
 
 typedef struct plq_ctx plq_ctx;
 typedef struct plq_chain plq_chain;

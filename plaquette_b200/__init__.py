@@ -35,6 +35,7 @@ FLAG_NO_FUSED = 1
 FLAG_TINY_PASS_CAP = 2
 FLAG_TEST_COPY_STALL = 4
 FLAG_GENERIC_PASS = 8
+FLAG_NO_PACKED = 16
 MAX_D = 8
 MAX_Q = 64
 GPU_BATCH = 64  # src/device.rs:501

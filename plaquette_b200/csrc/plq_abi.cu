@@ -237,7 +237,7 @@ void chain_free(plq_chain *c) {
     cluster_free(c);
     void *ptrs[] = {c->d_state, c->d_state_alt, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
                     c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs, c->d_loop_bits,
-                    c->d_meas, c->d_pairs, c->d_hb53_fused};
+                    c->d_meas, c->d_pairs, c->d_hb53_fused, c->d_packed};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -403,7 +403,14 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
                 hb53_shifted.push_back(cut << 11);
             }
         }
-        if (!(desc->flags & PLQ_FLAG_NO_FUSED) && fused3d_eligible(desc->model, c->q, c->d, c->g.L, desc->updater, desc->rng) &&
+        if (!(desc->flags & (PLQ_FLAG_NO_FUSED | PLQ_FLAG_GENERIC_PASS | PLQ_FLAG_NO_PACKED)) && !c->link &&
+            packed_chain_eligible(desc->model, c->q, c->d, c->g.L, desc->updater, desc->rng)) {
+            c->packed = true;
+            e = cudaMalloc((void **)&c->d_packed, (size_t)(c->n_sites / 64) * sizeof(uint64_t));
+            if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(packed state)"));
+        }
+        if (!c->packed && !(desc->flags & PLQ_FLAG_NO_FUSED) &&
+            fused3d_eligible(desc->model, c->q, c->d, c->g.L, desc->updater, desc->rng) &&
             table_bytes <= (size_t)fused3d_table_limit_bytes() && shifted_ok) {
             c->fused = true;
             if (!hb53_shifted.empty()) {
@@ -527,10 +534,44 @@ static int fused_sweep(plq_chain *c) {
     return PLQ_OK;
 }
 
+// `sweeps` sweeps of a packed chain: the bytes packed once, two colour passes
+// per sweep on the words (the keyed sweep index as the byte passes use it),
+// the words unpacked at the end.
+static int packed_sweeps(plq_chain *c, uint64_t sweeps) {
+    if (!sweeps) return PLQ_OK;
+    const int64_t n_words = c->n_sites / 64;
+    const int sm = c->ctx->sm_count;
+    PLQ_CUDA(launch_pack64(c->d_state, c->d_packed, n_words, sm, c->stream), "pack launch");
+    c->launches++;
+    PackedPassArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.words = c->d_packed;
+    a.n_words = n_words;
+    a.L0 = c->g.L[0];
+    a.L1 = c->g.L[1];
+    a.seed32 = c->seed32;
+    const bool hb = c->desc.updater == PLQ_HEATBATH;
+    a.table = hb ? c->d_hb24 : c->d_metro24;
+    a.n_keys = 2 + 4 * c->d;  // keys cur + 2 * count, count <= 2d
+    for (uint64_t t = 0; t < sweeps; ++t) {
+        a.sweep32 = (uint32_t)c->sweeps_done;
+        for (int colour = 0; colour < 2; ++colour) {
+            a.colour = colour;
+            PLQ_CUDA(launch_packed_pass(a, c->d, hb, sm, c->stream), "packed pass launch");
+            c->launches++;
+        }
+        c->sweeps_done++;
+    }
+    PLQ_CUDA(launch_unpack64(c->d_packed, c->d_state, n_words, sm, c->stream), "unpack launch");
+    c->launches++;
+    return PLQ_OK;
+}
+
 // One sweep of local passes, in the reference's colour order
 // (updater.rs:316-343; device.rs:417-430 for the keyed sweep index).
 int local_sweep(plq_chain *c) {
     if (c->fused) return fused_sweep(c);
+    if (c->packed) return packed_sweeps(c, 1);
     LocalArgs a = local_args(c);
     a.sweep32 = (uint32_t)c->sweeps_done;
     const int64_t half = c->n_sites / 2;
@@ -590,6 +631,7 @@ int local_sweep(plq_chain *c) {
 
 static int run_sweeps(plq_chain *c, uint64_t sweeps) {
     if (c->cluster) return sweeps ? cluster_sweep_n(c, sweeps) : PLQ_OK;
+    if (c->packed) return packed_sweeps(c, sweeps);
     for (uint64_t t = 0; t < sweeps; ++t) {
         int rc = c->cluster ? cluster_sweep(c) : local_sweep(c);
         if (rc != PLQ_OK) return rc;
@@ -909,6 +951,7 @@ extern "C" const char *plq_chain_path(plq_chain *c) {
     if (!c) return "";
     if (c->cluster) return "cluster";
     if (c->fused) return "fused3d";
+    if (c->packed) return "packed";
     return c->lookback ? "lookback" : (c->words ? "words" : "pass");
 }
 extern "C" void plq_chain_destroy(plq_chain *c) { chain_free(c); }

@@ -45,6 +45,8 @@ struct plq_chain {
     uint8_t *d_state = nullptr;  // device layout (links as direction planes)
     uint8_t *d_state_alt = nullptr;  // second buffer of the out-of-place fused sweep
     bool fused = false;
+    bool packed = false;          // q = 2 keyed sites: sweeps on a bit-packed copy (plq_packed3d.cu)
+    uint64_t *d_packed = nullptr; // n_sites / 64 words
     int fused_tz = 0;
     plq::FusedMaps fused_maps[2];          // TMA descriptors of the two state buffers
     const uint8_t *fused_map_buf[2] = {nullptr, nullptr};

@@ -36,6 +36,24 @@ struct PrimTask {
 cudaError_t launch_primaries_multi(const PrimTask *tasks, const int32_t *item_task, const int32_t *item_chunk,
                                    int64_t n_items, int sm_count, cudaStream_t stream);
 
+// Bit-packed colour passes of one q = 2 site lattice on the keyed stream
+// (plq_packed3d.cu): 2D or 3D, extent 0 a multiple of 64; word g holds sites
+// [64 g, 64 g + 64).  n_keys table entries (cur + 2 * count) are read.
+struct PackedPassArgs {
+    uint64_t *words;
+    int64_t n_words;
+    int L0, L1;  // L1: the 3D lattice's extent 1 (unused in 2D)
+    int colour;
+    uint32_t seed32, sweep32;
+    const uint32_t *table;  // metro24 (Metropolis) or hb24 (heat bath)
+    int n_keys;
+};
+bool packed_chain_eligible(int model, int q, int d, const int32_t *L, int updater, int rng);
+cudaError_t launch_pack64(const uint8_t *bytes, uint64_t *words, int64_t n_words, int sm_count, cudaStream_t stream);
+cudaError_t launch_unpack64(const uint64_t *words, uint8_t *bytes, int64_t n_words, int sm_count,
+                            cudaStream_t stream);
+cudaError_t launch_packed_pass(const PackedPassArgs &a, int d, bool hb, int sm_count, cudaStream_t stream);
+
 // Layout conversion of link variables: host order (site*d + dir) <-> device
 // planes (dir*n_sites + site).
 cudaError_t launch_links_to_planes(const uint8_t *in, uint8_t *out, int64_t n_sites, int d,

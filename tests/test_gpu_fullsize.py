@@ -90,7 +90,7 @@ def test_ising_512cubed_metropolis_keyed(oracle, gpu, lat512):
                       sweeps_between=2, batch=1)
     chain = plq.GpuChain(gpu, d, start)
     got, prims = chain.next_sample()
-    assert chain.path == "fused3d"
+    assert chain.path == "packed"
     chain.close()
     model = oracle.Model.ising(1.0, 0.0)
     s32 = oracle.fold_seed(SEED)

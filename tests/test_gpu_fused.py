@@ -34,7 +34,9 @@ IDS = ["potts3-hb-stream", "potts3-hb-keyed", "ising-hb-stream", "ising-hb-keyed
 def test_fused_matches_oracle(oracle, gpu, shape, mode):
     kind, q, kernel, rng = mode
     beta = {plq.ISING: 0.2216544, plq.POTTS: 0.5505}[kind]
-    got, want, chain, model, lat = run_pair(oracle, gpu, kind, q, shape, kernel, rng, beta, 5)
+    # (q = 2 keyed chains would take the bit-packed passes: kept on the fused sweep here)
+    got, want, chain, model, lat = run_pair(oracle, gpu, kind, q, shape, kernel, rng, beta, 5,
+                                            flags=plq.FLAG_NO_PACKED)
     assert chain.path == "fused3d"
     assert np.array_equal(got, want)
     assert list(chain.primaries()) == list(model.primaries(lat, want))
@@ -47,11 +49,11 @@ def test_fused_equals_pass_kernels(gpu, mode):
     n = 256 * 64 * 64
     start, off = plq.hot_start(99, q, n)
     outs = []
-    for flags in (0, plq.FLAG_NO_FUSED):
+    for flags in (plq.FLAG_NO_PACKED, plq.FLAG_NO_FUSED):
         d = plq.make_desc(kind, q, shape, kernel, beta=0.4, seed=99, rng=rng, stream_offset=off,
                           sweeps_between=6, batch=1, flags=flags)
         c = plq.GpuChain(gpu, d, start)
-        assert c.path == ("fused3d" if flags == 0 else ("lookback" if kernel == plq.METROPOLIS and rng == plq.RNG_STREAM else "words"))
+        assert c.path == ("fused3d" if flags == plq.FLAG_NO_PACKED else ("lookback" if kernel == plq.METROPOLIS and rng == plq.RNG_STREAM else "words"))
         outs.append(next(c))
         if rng == plq.RNG_STREAM:
             outs.append(c.stream_position())
@@ -83,14 +85,15 @@ def test_tile_copy_wait_limit_reports_and_context_survives(oracle, gpu):
     shape = (128, 64, 16)
     start = np.zeros(int(np.prod(shape)), dtype=np.uint8)
     d = plq.make_desc(plq.ISING, 2, shape, plq.METROPOLIS, beta=0.3, seed=3, rng=plq.RNG_KEYED, batch=1,
-                      flags=plq.FLAG_TEST_COPY_STALL)
+                      flags=plq.FLAG_TEST_COPY_STALL | plq.FLAG_NO_PACKED)
     chain = plq.GpuChain(gpu, d, start)
     assert chain.path == "fused3d"
     with pytest.raises(plq.PlaquetteError, match="16 = tile copy wait limit") as info:
         next(chain)
     assert info.value.code == plq.PLQ_EDEVICE
     chain.close()
-    got, want, *_ = run_pair(oracle, gpu, plq.ISING, 2, shape, plq.METROPOLIS, plq.RNG_KEYED, 0.3, 2)
+    got, want, *_ = run_pair(oracle, gpu, plq.ISING, 2, shape, plq.METROPOLIS, plq.RNG_KEYED, 0.3, 2,
+                             flags=plq.FLAG_NO_PACKED)
     assert np.array_equal(got, want)
 
 

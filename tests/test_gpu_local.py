@@ -31,7 +31,7 @@ def _models(oracle, kind, q, j, h, offsets):
 
 
 def run_pair(oracle, gpu, kind, q, shape, kernel, rng_mode, beta, sweeps, *, j=1.0, h=0.0, offsets=None,
-             seed=20260718, start="hot", sweeps_between=None):
+             seed=20260718, start="hot", sweeps_between=None, flags=0):
     lat = oracle.Lattice(shape, staples=kind == plq.GAUGE)
     model = _models(oracle, kind, q, j, h, offsets)
     n_vars = model.n_vars(lat)
@@ -40,7 +40,7 @@ def run_pair(oracle, gpu, kind, q, shape, kernel, rng_mode, beta, sweeps, *, j=1
     else:
         cfg, offset = np.zeros(n_vars, dtype=np.uint8), 0
     d = plq.make_desc(kind, q, shape, kernel, beta=beta, j=j, h=h, offsets=offsets, seed=seed, rng=rng_mode,
-                      stream_offset=offset, sweeps_between=sweeps_between or sweeps, batch=1)
+                      stream_offset=offset, sweeps_between=sweeps_between or sweeps, batch=1, flags=flags)
     chain = plq.GpuChain(gpu, d, cfg)
     got = next(chain)
     want = cfg.copy()
@@ -236,11 +236,12 @@ def test_word_passes_equal_generic(gpu, case):
     n_vars = int(np.prod(shape)) * (len(shape) if kind == plq.GAUGE else 1)
     start, off = plq.hot_start(77, q, n_vars)
     outs = []
-    for flags in (0, plq.FLAG_GENERIC_PASS):
+    # (q = 2 keyed sites with extent 0 a multiple of 64 would take the bit-packed passes)
+    for flags in (plq.FLAG_NO_PACKED, plq.FLAG_GENERIC_PASS):
         d = plq.make_desc(kind, q, shape, kernel, beta=beta, seed=77, rng=rng_mode, stream_offset=off,
                           sweeps_between=5, batch=1, flags=flags)
         c = plq.GpuChain(gpu, d, start)
-        assert c.path == ("words" if flags == 0 else "pass")
+        assert c.path == ("words" if flags == plq.FLAG_NO_PACKED else "pass")
         outs.append((next(c), c.stream_position() if rng_mode == plq.RNG_STREAM else 0, list(c.primaries())))
         c.close()
     assert np.array_equal(outs[0][0], outs[1][0])
