@@ -73,6 +73,11 @@ enum plq_rng { PLQ_RNG_STREAM = 0, PLQ_RNG_KEYED = 1 };
  * four-sites-at-a-time body) where the bit-packed passes apply (identical
  * results; used to test the byte paths). */
 #define PLQ_FLAG_NO_PACKED 16
+/* Bit-packed chains only: hash both keyed rounds in every pass instead of
+ * reading each site's sweep-independent first round from the array filled at
+ * creation (identical results; used to test the hashing passes, which also
+ * serve lattices of 2^31 sites and more and chains whose array found no room). */
+#define PLQ_FLAG_NO_FIRST_HASH 32
 
 typedef struct plq_ctx plq_ctx;
 typedef struct plq_chain plq_chain;

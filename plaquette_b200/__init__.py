@@ -36,6 +36,7 @@ FLAG_TINY_PASS_CAP = 2
 FLAG_TEST_COPY_STALL = 4
 FLAG_GENERIC_PASS = 8
 FLAG_NO_PACKED = 16
+FLAG_NO_FIRST_HASH = 32
 MAX_D = 8
 MAX_Q = 64
 GPU_BATCH = 64  # src/device.rs:501

@@ -237,7 +237,7 @@ void chain_free(plq_chain *c) {
     cluster_free(c);
     void *ptrs[] = {c->d_state, c->d_state_alt, c->d_io, c->d_hb53, c->d_hb24, c->d_metro53, c->d_metro24,
                     c->d_jump, c->d_ctrl, c->d_desc, c->d_obs, c->d_snap, c->d_snap_obs, c->d_loop_bits,
-                    c->d_meas, c->d_pairs, c->d_hb53_fused, c->d_packed};
+                    c->d_meas, c->d_pairs, c->d_hb53_fused, c->d_packed, c->d_first_hash};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -408,6 +408,21 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
             c->packed = true;
             e = cudaMalloc((void **)&c->d_packed, (size_t)(c->n_sites / 64) * sizeof(uint64_t));
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(packed state)"));
+            // every site's sweep-independent first keyed round lowbias32_head(seed ^ site) (4 B/site):
+            // the passes hash only the sweep's round.  Optional -- without it (no room, or 2^31 sites and more) the passes hash both
+            // times, with identical results.
+            if (c->n_sites < (int64_t(1) << 31) && !(desc->flags & PLQ_FLAG_NO_FIRST_HASH)) {
+                const size_t hb_bytes = first_hash_bytes(c->n_sites / 64);
+                if (cudaMalloc(&c->d_first_hash, hb_bytes) == cudaSuccess) {
+                    e = launch_first_hash(c->d_first_hash, c->n_sites / 64, c->g.L[0], c->g.L[1], c->d, c->seed32,
+                                          c->ctx->sm_count, c->stream);
+                    if (e != cudaSuccess) return fail(cuda_fail(e, "first-hash launch"));
+                    c->launches++;
+                } else {
+                    c->d_first_hash = nullptr;
+                    (void)cudaGetLastError();  // the failed allocation's error; the chain hashes in its passes
+                }
+            }
         }
         if (!c->packed && !(desc->flags & PLQ_FLAG_NO_FUSED) &&
             fused3d_eligible(desc->model, c->q, c->d, c->g.L, desc->updater, desc->rng) &&
@@ -553,6 +568,7 @@ static int packed_sweeps(plq_chain *c, uint64_t sweeps) {
     const bool hb = c->desc.updater == PLQ_HEATBATH;
     a.table = hb ? c->d_hb24 : c->d_metro24;
     a.n_keys = 2 + 4 * c->d;  // keys cur + 2 * count, count <= 2d
+    a.first_hash = c->d_first_hash;
     for (uint64_t t = 0; t < sweeps; ++t) {
         a.sweep32 = (uint32_t)c->sweeps_done;
         for (int colour = 0; colour < 2; ++colour) {

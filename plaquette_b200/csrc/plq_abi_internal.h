@@ -47,6 +47,7 @@ struct plq_chain {
     bool fused = false;
     bool packed = false;          // q = 2 keyed sites: sweeps on a bit-packed copy (plq_packed3d.cu)
     uint64_t *d_packed = nullptr; // n_sites / 64 words
+    void *d_first_hash = nullptr; // packed chains: lowbias32_head(seed ^ site) of every site (plq_packed3d.cu)
     int fused_tz = 0;
     plq::FusedMaps fused_maps[2];          // TMA descriptors of the two state buffers
     const uint8_t *fused_map_buf[2] = {nullptr, nullptr};

@@ -294,7 +294,7 @@ __device__ void packed_site_item(const LocalArgs &a, W *pk, int64_t chunk, int R
     const W full = L0 == 8 * sizeof(W) ? ~(W)0 : (((W)1 << L0) - 1);
     const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
     const bool hb = a.kernel == PLQ_HEATBATH;
-    const uint32_t sweep_mix = a.sweep32 * 0x9e3779b9u;
+    const uint32_t sweep_mix = keyed_mix(a.sweep32);
 #pragma unroll 1
     for (int i = 0; i < R; ++i) {
         const uint32_t r = r0 + (uint32_t)i;
@@ -370,7 +370,7 @@ __device__ void packed_link_item(const LocalArgs &a, uint32_t *pk, int64_t chunk
     const uint32_t full = L0 == 32 ? 0xFFFFFFFFu : ((1u << L0) - 1u);
     const uint32_t r0 = (uint32_t)(chunk * (int64_t)blockDim.x * R) + threadIdx.x * (uint32_t)R;
     const bool hb = a.kernel == PLQ_HEATBATH;
-    const uint32_t sweep_mix = a.sweep32 * 0x9e3779b9u;
+    const uint32_t sweep_mix = keyed_mix(a.sweep32);
 #pragma unroll 1
     for (int i = 0; i < R; ++i) {
         const uint32_t r = r0 + (uint32_t)i;

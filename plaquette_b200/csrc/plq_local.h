@@ -47,8 +47,14 @@ struct PackedPassArgs {
     uint32_t seed32, sweep32;
     const uint32_t *table;  // metro24 (Metropolis) or hb24 (heat bath)
     int n_keys;
+    // Optional: every variable's sweep-independent first round lowbias32_head(seed ^ site)
+    // (first_hash_bytes(n_words) bytes, filled by launch_first_hash); null = hash in the pass.
+    const void *first_hash;
 };
 bool packed_chain_eligible(int model, int q, int d, const int32_t *L, int updater, int rng);
+size_t first_hash_bytes(int64_t n_words);
+cudaError_t launch_first_hash(void *first_hash, int64_t n_words, int L0, int L1, int d, uint32_t seed32,
+                              int sm_count, cudaStream_t stream);
 cudaError_t launch_pack64(const uint8_t *bytes, uint64_t *words, int64_t n_words, int sm_count, cudaStream_t stream);
 cudaError_t launch_unpack64(const uint64_t *words, uint8_t *bytes, int64_t n_words, int sm_count,
                             cudaStream_t stream);

@@ -39,13 +39,14 @@ __device__ __forceinline__ int popc_w(uint64_t v) { return __popcll(v); }
 // (pairs (cur, c0) and (c1, c2) interleaved at two-bit granularity, Hacker's
 // Delight's outer perfect shuffle without its last stage), and the key times
 // four is the byte offset of its entry in the shared-memory table tab.  The
-// draw of variable j is the keyed stream's at index v0 + j * DV.  Returns the
+// draw of variable j is the keyed stream's at index v0 + j * DV, composed as
+// keyed24 does (mix = keyed_mix(sweep)).  Returns the
 // bits to flip, at 2j: Metropolis accepts when the draw is below the entry;
 // heat bath sets the new state to (entry <= draw).
 // Eight (or, TAIL, the first m < 8) variables of a row from their key word x
 // (nibble i: variable i's key): the flip or new-state bits at 2i.
 template <int DV, bool HB, bool TAIL>
-__device__ __forceinline__ uint32_t decide8(uint32_t x, int m, uint32_t vc, uint32_t seed32, uint32_t sweep_mix,
+__device__ __forceinline__ uint32_t decide8(uint32_t x, int m, uint32_t vc, uint32_t seed32, uint32_t mix,
                                             const char *tb) {
     uint32_t o = 0;
 #pragma unroll
@@ -53,7 +54,27 @@ __device__ __forceinline__ uint32_t decide8(uint32_t x, int m, uint32_t vc, uint
         if (!TAIL || i < m) {
             const uint32_t key4 = i == 0 ? (x << 2) & 0x3Cu : (x >> (4 * i - 2)) & 0x3Cu;
             const uint32_t e = *reinterpret_cast<const uint32_t *>(tb + key4);
-            const uint32_t k = lowbias32(lowbias32(seed32 ^ (vc + (uint32_t)(i * DV))) ^ sweep_mix) >> 8;
+            const uint32_t k = lowbias32_tail(lowbias32_head(seed32 ^ (vc + (uint32_t)(i * DV))) ^ mix) >> 8;
+            const bool b = HB ? e <= k : k < e;
+            o |= (uint32_t)b << (2 * i);
+        }
+    }
+    return o;
+}
+
+// decide8 over eight (or, TAIL, the first m < 8) variables whose first rounds
+// lowbias32_head(seed ^ index) are given (h1[i] for variable i): half a keyed
+// draw's hashing per variable.
+template <bool HB, bool TAIL = false>
+__device__ __forceinline__ uint32_t decide8_h1(uint32_t x, const uint32_t (&h1)[8], uint32_t mix,
+                                               const char *tb, int m = 8) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!TAIL || i < m) {
+            const uint32_t key4 = i == 0 ? (x << 2) & 0x3Cu : (x >> (4 * i - 2)) & 0x3Cu;
+            const uint32_t e = *reinterpret_cast<const uint32_t *>(tb + key4);
+            const uint32_t k = lowbias32_tail(h1[i] ^ mix) >> 8;
             const bool b = HB ? e <= k : k < e;
             o |= (uint32_t)b << (2 * i);
         }
@@ -76,7 +97,7 @@ __device__ __forceinline__ uint32_t key_word(W P, W Q, int c) {
 
 template <class W, int DV, bool HB>
 __device__ __forceinline__ W decide_row(W Cs, W c0s, W c1s, W c2s, int n, uint32_t v0, uint32_t seed32,
-                                        uint32_t sweep_mix, const uint32_t *tab) {
+                                        uint32_t mix, const uint32_t *tab) {
     const W M = (W)0x5555555555555555ull;
     const W P = (Cs & M) | ((c0s << 1) & ~M);
     const W Q = (c1s & M) | ((c2s << 1) & ~M);
@@ -85,11 +106,11 @@ __device__ __forceinline__ W decide_row(W Cs, W c0s, W c1s, W c2s, int n, uint32
     const int full = n >> 3;
 #pragma unroll 1
     for (int c = 0; c < full; ++c)
-        out |= (W)decide8<DV, HB, false>(key_word(P, Q, c), 8, v0 + (uint32_t)(8 * c * DV), seed32, sweep_mix, tb)
+        out |= (W)decide8<DV, HB, false>(key_word(P, Q, c), 8, v0 + (uint32_t)(8 * c * DV), seed32, mix, tb)
                << (16 * c);
     if (n & 7)
         out |= (W)decide8<DV, HB, true>(key_word(P, Q, full), n & 7, v0 + (uint32_t)(8 * full * DV), seed32,
-                                        sweep_mix, tb)
+                                        mix, tb)
                << (16 * full);
     if (HB) {  // new states -> flips, over the n variables
         const W valid = 2 * n >= (int)(8 * sizeof(W)) ? ~(W)0 : (((W)1 << (2 * n)) - 1);

@@ -15,6 +15,13 @@
 // are bit-identical to the byte paths'.  A pass changes only its colour's
 // bits, so a neighbour word read while another thread rewrites it yields the
 // same bits of the other colour either way.
+//
+// The packed copy (1/8 B per site) stays in L2 and the passes are bound by
+// the ALU pipe, mostly the keyed draws' hashing.  So a chain also keeps, where
+// it has room, each site's sweep-independent first round of its draws (4 B per
+// site, filled once at creation) and a pass streams its colour's half of that
+// array from HBM instead of computing it: HBM bytes the packed passes do not
+// otherwise use, traded for ALU work.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -64,14 +71,42 @@ __global__ void __launch_bounds__(kPackedThreads) unpack64_kernel(const uint64_t
     }
 }
 
-template <int D, bool HB>
+// The first-hash array, lowbias32_head(seed ^ site) of every site (the sweep-independent
+// first round of its keyed draws, keyed24 in plq_rng.cuh): for colour c, word g and the
+// pass's variables 4 jq .. 4 jq + 3 of
+// that word (sites 64 g + x0 + 2 (4 jq + m)), one uint4 at ((c * nb + g / 32) * 8 + jq) * 32
+// + g % 32, nb = ceil(n_words / 32): the 32 words of a warp read 512 contiguous bytes per load.
+__global__ void __launch_bounds__(kPackedThreads) first_hash_kernel(uint4 *H, int64_t n_words, int64_t nb,
+                                                                   uint32_t wpr, uint32_t L1, int d, uint32_t seed32) {
+    const int64_t total = 2 * nb * 8 * 32;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t lane = (uint32_t)(i & 31);
+        const int64_t t = i >> 5;
+        const uint32_t jq = (uint32_t)(t & 7);
+        const int64_t bc = t >> 3;
+        const uint32_t colour = (uint32_t)(bc / nb);
+        const int64_t g = (bc - (int64_t)colour * nb) * 32 + lane;
+        if (g >= n_words) {
+            H[i] = make_uint4(0, 0, 0, 0);
+            continue;
+        }
+        const uint32_t r = (uint32_t)(g / wpr);
+        const uint32_t y = d == 3 ? r % L1 : r;
+        const uint32_t z = d == 3 ? r / L1 : 0;
+        const uint32_t v = (uint32_t)(64 * g) + ((colour ^ y ^ z) & 1u) + 8 * jq;
+        H[i] = make_uint4(lowbias32_head(seed32 ^ v), lowbias32_head(seed32 ^ (v + 2)),
+                          lowbias32_head(seed32 ^ (v + 4)), lowbias32_head(seed32 ^ (v + 6)));
+    }
+}
+
+template <int D, bool HB, bool CACHED>
 __global__ void __launch_bounds__(kPackedThreads) packed_pass_kernel(PackedPassArgs a) {
     __shared__ uint32_t s_tab[16];
     if (threadIdx.x < 16) s_tab[threadIdx.x] = threadIdx.x < (unsigned)a.n_keys ? a.table[threadIdx.x] : 0u;
     __syncthreads();
     const uint32_t wpr = (uint32_t)a.L0 / 64;  // words per row
     const uint32_t rows = (uint32_t)(a.n_words / wpr);
-    const uint32_t sweep_mix = a.sweep32 * 0x9e3779b9u;
+    const uint32_t sweep_mix = keyed_mix(a.sweep32);
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.n_words; g += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t r = (uint32_t)g / wpr;
         const uint32_t wi = (uint32_t)g - r * wpr;
@@ -81,6 +116,13 @@ __global__ void __launch_bounds__(kPackedThreads) packed_pass_kernel(PackedPassA
             y = r - z * (uint32_t)a.L1;
         } else {
             y = r;
+        }
+        uint4 hv[8];
+        if (CACHED) {  // this pass's 32 first hashes, issued before the neighbour loads
+            const uint4 *hp = static_cast<const uint4 *>(a.first_hash) +
+                              ((((int64_t)a.colour * ((a.n_words + 31) >> 5) + (g >> 5)) * 8) << 5) + (g & 31);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) hv[k] = __ldcs(hp + 32 * k);
         }
         const uint64_t *w = a.words;
         const uint32_t rb = r * wpr;
@@ -106,8 +148,25 @@ __global__ void __launch_bounds__(kPackedThreads) packed_pass_kernel(PackedPassA
         // the word's first site x = 64 wi is even: the pass's sites are at (colour + y + z) & 1 + 2j
         const uint32_t x0 = (uint32_t)((a.colour ^ y ^ z) & 1u);
         const uint32_t v0 = r * (uint32_t)a.L0 + 64u * wi + x0;  // keyed index of the word's first such site
-        const uint64_t flip = decide_row<uint64_t, 2, HB>(C >> x0, c0 >> x0, c1 >> x0, c2 >> x0, 32, v0, a.seed32,
-                                                          sweep_mix, s_tab);
+        uint64_t flip;
+        if (CACHED) {
+            const uint64_t M = 0x5555555555555555ull;
+            const uint64_t P = ((C >> x0) & M) | (((c0 >> x0) << 1) & ~M);
+            const uint64_t Q = ((c1 >> x0) & M) | (((c2 >> x0) << 1) & ~M);
+            const char *tb = reinterpret_cast<const char *>(s_tab);
+            flip = 0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const uint32_t h1[8] = {hv[2 * c].x,     hv[2 * c].y,     hv[2 * c].z,     hv[2 * c].w,
+                                        hv[2 * c + 1].x, hv[2 * c + 1].y, hv[2 * c + 1].z, hv[2 * c + 1].w};
+                flip |= (uint64_t)decide8_h1<HB>(key_word(P, Q, c), h1, sweep_mix, tb) << (16 * c);
+            }
+            if (HB) flip ^= P & M;  // new states -> flips
+            (void)v0;
+        } else {
+            flip = decide_row<uint64_t, 2, HB>(C >> x0, c0 >> x0, c1 >> x0, c2 >> x0, 32, v0, a.seed32, sweep_mix,
+                                               s_tab);
+        }
         a.words[g] = C ^ (flip << x0);
     }
 }
@@ -134,14 +193,32 @@ cudaError_t launch_unpack64(const uint64_t *words, uint8_t *bytes, int64_t n_wor
     return cudaGetLastError();
 }
 
+size_t first_hash_bytes(int64_t n_words) { return (size_t)((n_words + 31) / 32) * 2 * 8 * 32 * sizeof(uint4); }
+
+cudaError_t launch_first_hash(void *first_hash, int64_t n_words, int L0, int L1, int d, uint32_t seed32,
+                              int sm_count, cudaStream_t stream) {
+    if (d != 2 && d != 3) return cudaErrorInvalidValue;
+    const int64_t nb = (n_words + 31) / 32;
+    const int64_t total = nb * 2 * 8 * 32;
+    first_hash_kernel<<<blocks_for(total, sm_count), kPackedThreads, 0, stream>>>(
+        static_cast<uint4 *>(first_hash), n_words, nb, (uint32_t)L0 / 64, (uint32_t)L1, d, seed32);
+    return cudaGetLastError();
+}
+
+template <int D, bool HB>
+static void launch_pass_d(const PackedPassArgs &a, unsigned blocks, cudaStream_t stream) {
+    if (a.first_hash) packed_pass_kernel<D, HB, true><<<blocks, kPackedThreads, 0, stream>>>(a);
+    else packed_pass_kernel<D, HB, false><<<blocks, kPackedThreads, 0, stream>>>(a);
+}
+
 cudaError_t launch_packed_pass(const PackedPassArgs &a, int d, bool hb, int sm_count, cudaStream_t stream) {
     const unsigned blocks = blocks_for(a.n_words, sm_count);
     if (d == 3) {
-        if (hb) packed_pass_kernel<3, true><<<blocks, kPackedThreads, 0, stream>>>(a);
-        else packed_pass_kernel<3, false><<<blocks, kPackedThreads, 0, stream>>>(a);
+        if (hb) launch_pass_d<3, true>(a, blocks, stream);
+        else launch_pass_d<3, false>(a, blocks, stream);
     } else if (d == 2) {
-        if (hb) packed_pass_kernel<2, true><<<blocks, kPackedThreads, 0, stream>>>(a);
-        else packed_pass_kernel<2, false><<<blocks, kPackedThreads, 0, stream>>>(a);
+        if (hb) launch_pass_d<2, true>(a, blocks, stream);
+        else launch_pass_d<2, false>(a, blocks, stream);
     } else {
         return cudaErrorInvalidValue;
     }

@@ -3,7 +3,9 @@ chain's states and primaries equal the oracle's keyed sweeps (the reference
 WGSL checkerboard) on small lattices -- rows of one, two and three 64-bit
 words, 2D and 3D, Ising Metropolis and heat bath with a field, Potts q = 2 --
 and the fused byte sweep on larger ones; sweeps split over several advance
-calls continue the keyed sweep counter."""
+calls continue the keyed sweep counter.  Each case runs twice: with the
+per-site first-hash array filled at creation and with both hash rounds
+computed in the passes."""
 import numpy as np
 import pytest
 
@@ -34,9 +36,11 @@ CASES = [  # kind, q, shape, kernel, beta, extra
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{'ising' if c[0] == plq.ISING else 'potts2'}-"
                                                      f"{'x'.join(map(str, c[2]))}-{'hb' if c[3] == plq.HEATBATH else 'metro'}")
-def test_packed_matches_oracle(oracle, gpu, case):
+@pytest.mark.parametrize("flags", [0, plq.FLAG_NO_FIRST_HASH], ids=["first-hash-array", "hashed"])
+def test_packed_matches_oracle(oracle, gpu, case, flags):
     kind, q, shape, kernel, beta, extra = case
-    got, want, chain, model, lat = run_pair(oracle, gpu, kind, q, shape, kernel, plq.RNG_KEYED, beta, 5, **extra)
+    got, want, chain, model, lat = run_pair(oracle, gpu, kind, q, shape, kernel, plq.RNG_KEYED, beta, 5,
+                                            flags=flags, **extra)
     assert chain.path == "packed"
     assert np.array_equal(got, want)
     assert list(chain.primaries()) == list(model.primaries(lat, want))
@@ -48,14 +52,15 @@ def test_packed_equals_fused_sweep(gpu, kernel):
     n = int(np.prod(shape))
     start, _ = plq.hot_start(41, 2, n)
     outs = []
-    for flags in (0, plq.FLAG_NO_PACKED):
+    for flags in (0, plq.FLAG_NO_FIRST_HASH, plq.FLAG_NO_PACKED):
         d = plq.make_desc(plq.ISING, 2, shape, kernel, beta=0.2216544, seed=41, rng=plq.RNG_KEYED, sweeps_between=7,
                           batch=1, flags=flags)
         c = plq.GpuChain(gpu, d, start)
-        assert c.path == ("packed" if flags == 0 else "fused3d")
+        assert c.path == ("fused3d" if flags == plq.FLAG_NO_PACKED else "packed")
         outs.append(next(c))
         c.close()
     assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[2])
 
 
 def test_sweeps_split_over_advance_calls(gpu):
