@@ -603,6 +603,59 @@ __device__ void energy_phase(const EnsArgs &e) {
     }
 }
 
+// Primaries of packed members from their rows (the same integers as the byte
+// scan, primaries_multi_kernel): item i is rows [c * blockDim, (c + 1) * blockDim)
+// of member item_member[i]; out[0] gets the bond / agreement / plaquette sum
+// (packed_energy_rows), sites also their counts of state 1 -- the Ising spin
+// sum n - 2 * ones into out[1], Potts q = 2 label counts into out[1], out[2].
+// The outputs must be zero before the launch.
+__global__ void __launch_bounds__(kEnsThreads)
+packed_primaries_kernel(const EnsMember *members, const int32_t *item_member, const int32_t *item_chunk,
+                        int64_t n_items, long long *prims, const int64_t *prims_offset) {
+    for (int64_t i = blockIdx.x; i < n_items; i += gridDim.x) {
+        const int m = item_member[i];
+        const EnsMember &mem = members[m];
+        const LocalArgs &a = mem.a;
+        const int64_t c = item_chunk[i];
+        long long part = 0, ones = 0;
+        const uint32_t rows = row_count(a.g);
+        const uint32_t r = (uint32_t)(c * (int64_t)blockDim.x) + threadIdx.x;
+        if (mem.pk_wide) {
+            const uint64_t *pk = static_cast<const uint64_t *>(mem.pk);
+            part = a.g.d == 2 ? packed_energy_rows<2, uint64_t>(a, pk, mem.link, c)
+                              : packed_energy_rows<3, uint64_t>(a, pk, mem.link, c);
+            if (!mem.link && r < rows) ones = popc_w(pk[r]);
+        } else {
+            const uint32_t *pk = static_cast<const uint32_t *>(mem.pk);
+            switch (a.g.d) {
+                case 2: part = packed_energy_rows<2, uint32_t>(a, pk, mem.link, c); break;
+                case 3: part = packed_energy_rows<3, uint32_t>(a, pk, mem.link, c); break;
+                case 4: part = packed_energy_rows<4, uint32_t>(a, pk, mem.link, c); break;
+                default: break;
+            }
+            if (!mem.link && r < rows) ones = popc_w(pk[r]);
+        }
+        const long long tot = block_sum(part);
+        const long long tot_ones = mem.link ? 0 : block_sum(ones);
+        if (threadIdx.x == 0) {
+            long long *out = prims + prims_offset[m];
+            if (tot) atomicAdd((unsigned long long *)&out[0], (unsigned long long)tot);
+            if (!mem.link) {
+                const int64_t r0 = c * (int64_t)blockDim.x;
+                const int64_t nr = min((int64_t)rows - r0, (int64_t)blockDim.x);
+                const long long sites = nr * (long long)a.g.L[0];
+                if (a.model == PLQ_ISING) {
+                    atomicAdd((unsigned long long *)&out[1], (unsigned long long)(sites - 2 * tot_ones));
+                } else {
+                    atomicAdd((unsigned long long *)&out[1], (unsigned long long)(sites - tot_ones));
+                    atomicAdd((unsigned long long *)&out[2], (unsigned long long)tot_ones);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Swap attempts of every ladder (one thread per pair); attempt index `att`.
 // Energies E = -J * (bond, agreement or plaquette sum); the pair at slots
 // (k, k+1) exchanges betas when (b_k - b_k+1)(E_k - E_k+1) >= 0 or a keyed
@@ -884,6 +937,15 @@ struct plq_ensemble {
     PrimTask *d_prim_tasks = nullptr;   // every member's measurement task (the states never move)
     int32_t *d_prim_task = nullptr, *d_prim_chunk = nullptr;
     int64_t n_prim_items = 0;
+    // The same from the packed rows: after a batched launch every packed member's rows still
+    // hold its configuration (unpacking leaves them), so its primaries are row popcounts.
+    // pk_current: no byte state has been written since the last batched launch.
+    bool pk_current = false;
+    int32_t *d_prim_task_bytes = nullptr, *d_prim_chunk_bytes = nullptr;  // items of unpacked members
+    int64_t n_prim_items_bytes = 0;
+    int32_t *d_pk_prim_member = nullptr, *d_pk_prim_chunk = nullptr;     // row chunks of packed members
+    int64_t n_pk_prim_items = 0;
+    int64_t *d_prims_offset = nullptr;
 };
 
 namespace {
@@ -1520,6 +1582,7 @@ extern "C" int plq_ensemble_advance(plq_ensemble *E, uint64_t sweeps) {
             E->launches++;
             if (e != cudaSuccess) return ens_fail(e, "persistent launch");
             E->sweeps_done += sweeps;
+            E->pk_current = true;
             return PLQ_OK;
         }
         E->graph_sweeps = sweeps;
@@ -1530,6 +1593,7 @@ extern "C" int plq_ensemble_advance(plq_ensemble *E, uint64_t sweeps) {
     E->launches++;
     if (e != cudaSuccess) return ens_fail(e, "graph launch");
     E->sweeps_done += sweeps;
+    E->pk_current = true;
     return PLQ_OK;
 }
 
@@ -1537,6 +1601,7 @@ extern "C" int plq_ensemble_advance_unbatched(plq_ensemble *E, uint64_t sweeps) 
     if (!E) return plq_fail(PLQ_EINVAL, "NULL ensemble");
     cudaError_t e = plq_enter_device(E->ctx->device);
     if (e != cudaSuccess) return ens_fail(e, "cudaSetDevice");
+    if (sweeps) E->pk_current = false;  // the byte states move on without the packed rows
     // host mirrors of the device-resident state the per-member launches need
     LaunchState ls;
     std::vector<unsigned long long> pos(E->members.size());
@@ -1625,6 +1690,9 @@ extern "C" int plq_ensemble_tune(plq_ensemble *E, int32_t trial_sweeps, int32_t 
     LaunchState ls;
     std::vector<std::vector<int32_t>> slots;
     auto snapshot = [&](bool save) {
+        // a restore rewrites the bytes; the trial launches (plq_ensemble_advance among them) left
+        // the packed rows at their own states
+        if (!save) E->pk_current = false;
         int64_t off = 0;
         for (size_t m = 0; m < E->members.size(); ++m) {
             if (save)
@@ -1881,17 +1949,31 @@ extern "C" int plq_ensemble_primaries_all(plq_ensemble *E, int64_t *out, int32_t
         if (e != cudaSuccess) return ens_fail(e, "primaries buffer");
         E->allocs.push_back(E->d_prims_all);
         std::vector<PrimTask> tasks(n);
-        std::vector<int32_t> it_task, it_chunk;
+        std::vector<int32_t> it_task, it_chunk, itb_task, itb_chunk, pk_member, pk_chunk;
         for (size_t m = 0; m < n; ++m) {
             const EnsMember &mem = E->members[m];
             tasks[m] = PrimTask{mem.a.state, mem.a.g, mem.a.model, mem.a.q, E->d_prims_all + E->prims_offset[m]};
             for (int64_t c = 0; c * kPrimChunk < mem.a.g.n_sites; ++c) {
                 it_task.push_back((int32_t)m);
                 it_chunk.push_back((int32_t)c);
+                if (!mem.pk) {
+                    itb_task.push_back((int32_t)m);
+                    itb_chunk.push_back((int32_t)c);
+                }
             }
+            if (mem.pk)
+                for (int64_t c = 0; c * kEnsThreads < (int64_t)row_count(mem.a.g); ++c) {
+                    pk_member.push_back((int32_t)m);
+                    pk_chunk.push_back((int32_t)c);
+                }
         }
         e = dev_upload(E, it_task.data(), it_task.size(), &E->d_prim_task);
         if (e == cudaSuccess) e = dev_upload(E, it_chunk.data(), it_chunk.size(), &E->d_prim_chunk);
+        if (e == cudaSuccess) e = dev_upload(E, itb_task.data(), itb_task.size(), &E->d_prim_task_bytes);
+        if (e == cudaSuccess) e = dev_upload(E, itb_chunk.data(), itb_chunk.size(), &E->d_prim_chunk_bytes);
+        if (e == cudaSuccess) e = dev_upload(E, pk_member.data(), pk_member.size(), &E->d_pk_prim_member);
+        if (e == cudaSuccess) e = dev_upload(E, pk_chunk.data(), pk_chunk.size(), &E->d_pk_prim_chunk);
+        if (e == cudaSuccess) e = dev_upload(E, E->prims_offset.data(), E->prims_offset.size(), &E->d_prims_offset);
         if (e == cudaSuccess) e = dev_upload(E, tasks.data(), tasks.size(), &E->d_prim_tasks);
         if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
         if (e != cudaSuccess) {
@@ -1899,6 +1981,8 @@ extern "C" int plq_ensemble_primaries_all(plq_ensemble *E, int64_t *out, int32_t
             return ens_fail(e, "primaries tasks");
         }
         E->n_prim_items = (int64_t)it_task.size();
+        E->n_prim_items_bytes = (int64_t)itb_task.size();
+        E->n_pk_prim_items = (int64_t)pk_member.size();
     }
     for (size_t m = 0; m < n; ++m) {
         const int64_t np = E->prims_offset[m + 1] - E->prims_offset[m];
@@ -1906,10 +1990,27 @@ extern "C" int plq_ensemble_primaries_all(plq_ensemble *E, int64_t *out, int32_t
     }
     std::vector<long long> host((size_t)E->prims_offset[n]);
     e = cudaMemsetAsync(E->d_prims_all, 0, sizeof(long long) * host.size(), E->stream);
-    if (e == cudaSuccess)
-        e = launch_primaries_multi(E->d_prim_tasks, E->d_prim_task, E->d_prim_chunk, E->n_prim_items,
-                                   E->ctx->sm_count, E->stream);
-    E->launches++;
+    if (E->pk_current && E->n_pk_prim_items) {
+        // packed members from their rows, the rest from their bytes
+        if (e == cudaSuccess && E->n_prim_items_bytes) {
+            e = launch_primaries_multi(E->d_prim_tasks, E->d_prim_task_bytes, E->d_prim_chunk_bytes,
+                                       E->n_prim_items_bytes, E->ctx->sm_count, E->stream);
+            E->launches++;
+        }
+        if (e == cudaSuccess) {
+            const unsigned blocks = (unsigned)std::min<int64_t>(E->n_pk_prim_items, (int64_t)E->ctx->sm_count * 8);
+            packed_primaries_kernel<<<blocks, kEnsThreads, 0, E->stream>>>(
+                E->d_members, E->d_pk_prim_member, E->d_pk_prim_chunk, E->n_pk_prim_items, E->d_prims_all,
+                E->d_prims_offset);
+            e = cudaGetLastError();
+            E->launches++;
+        }
+    } else {
+        if (e == cudaSuccess)
+            e = launch_primaries_multi(E->d_prim_tasks, E->d_prim_task, E->d_prim_chunk, E->n_prim_items,
+                                       E->ctx->sm_count, E->stream);
+        E->launches++;
+    }
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(host.data(), E->d_prims_all, sizeof(long long) * host.size(), cudaMemcpyDeviceToHost,
                             E->stream);

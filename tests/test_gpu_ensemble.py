@@ -196,6 +196,12 @@ def test_tuner_chooses_a_shape_per_member_shape(gpu):
         c.advance(5)
         assert np.array_equal(ens.read(m), c.read()), m
         assert np.array_equal(later.read(m), c.read()), m
+    # after a batched launch, tuning: its trial launches move the packed rows and it restores the
+    # bytes, so the primaries of every member at once must come from the bytes again
+    later.tune(3)
+    every = later.primaries_all()
+    for m in range(later.n):
+        assert list(every[m]) == list(later.primaries(m)), m
 
 
 @pytest.mark.parametrize("spec", [
@@ -235,3 +241,8 @@ def test_packed_members_match_their_own_chains(gpu, spec):
     assert np.array_equal(a.betas(), b.betas())
     for m in range(3):
         assert np.array_equal(a.read(m), b.read(m)), m
+    # primaries of every member at once: a's from the packed rows its launch left, b's from the
+    # bytes the per-lattice launches wrote; both equal the byte scan of each member
+    pa, pb = a.primaries_all(), b.primaries_all()
+    for m in range(3):
+        assert list(pa[m]) == list(pb[m]) == list(a.primaries(m)), m
