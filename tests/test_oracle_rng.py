@@ -194,6 +194,34 @@ def test_keyed_uniform_restatement(oracle):
         assert 0.0 <= got < 1.0
 
 
+def test_keyed_draw_split_form():
+    """The device composes a keyed draw lowbias32(lowbias32(a) ^ m) as
+    tail(head(a) ^ m ^ (m >> 16)), head/tail being lowbias32 without its last /
+    first xorshift by 16: x -> x ^ (x >> 16) is linear over xor and its own
+    inverse on 32 bits, so the two middle xorshifts cancel.  Checked here at
+    random and at the edge values of both words."""
+    M = 0xFFFFFFFF
+
+    def head(x):
+        x ^= x >> 16
+        x = (x * 0x7FEB352D) & M
+        x ^= x >> 15
+        return (x * 0x846CA68B) & M
+
+    def tail(y):
+        y = (y * 0x7FEB352D) & M
+        y ^= y >> 15
+        y = (y * 0x846CA68B) & M
+        return y ^ (y >> 16)
+
+    rs = np.random.default_rng(7)
+    pairs = [(int(a), int(t)) for a, t in rs.integers(0, 2**32, (4000, 2), dtype=np.uint64)]
+    pairs += [(a, t) for a in (0, 1, 0xFFFF, 0x10000, M) for t in (0, 1, 0x10000, M)]
+    for a, sweep in pairs:
+        m = (sweep * 0x9E3779B9) & M
+        assert _lowbias32_py(_lowbias32_py(a) ^ m) == tail(head(a) ^ m ^ (m >> 16))
+
+
 def test_fold_seed(oracle):
     # src/device.rs:761-763
     for s in [0, 1, 2**32, 2**64 - 1, 20260718, 0xDEADBEEF_12345678]:
