@@ -409,10 +409,13 @@ extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const 
             e = cudaMalloc((void **)&c->d_packed, (size_t)(c->n_sites / 64) * sizeof(uint64_t));
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMalloc(packed state)"));
             // every site's sweep-independent first keyed round lowbias32_head(seed ^ site) (4 B/site):
-            // the passes hash only the sweep's round.  Optional -- without it (no room, or 2^31 sites and more) the passes hash both
-            // times, with identical results.
-            if (c->n_sites < (int64_t(1) << 31) && !(desc->flags & PLQ_FLAG_NO_FIRST_HASH)) {
-                const size_t hb_bytes = first_hash_bytes(c->n_sites / 64);
+            // the passes hash only the sweep's round.  Optional: without it (2^31 sites and more, or
+            // the array would take over a quarter of the free memory, or its allocation fails) the
+            // passes hash both rounds, with identical results.
+            size_t free_b = 0, total_b = 0;
+            const size_t hb_bytes = first_hash_bytes(c->n_sites / 64);
+            if (c->n_sites < (int64_t(1) << 31) && !(desc->flags & PLQ_FLAG_NO_FIRST_HASH) &&
+                cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && hb_bytes <= free_b / 4) {
                 if (cudaMalloc(&c->d_first_hash, hb_bytes) == cudaSuccess) {
                     e = launch_first_hash(c->d_first_hash, c->n_sites / 64, c->g.L[0], c->g.L[1], c->d, c->seed32,
                                           c->ctx->sm_count, c->stream);
