@@ -795,7 +795,7 @@ __global__ void __launch_bounds__(kEnsThreads, WORDS_ONLY ? 4 : 2) ensemble_kern
             pf = pass_fields(e, m, p, r);
             const int k = (int)threadIdx.x - 32;
             const int nk = 2 + 4 * (mem.link ? mem.a.g.d - 1 : mem.a.g.d);  // keys of a q = 2 table
-            if (mem.pk && k < nk) tv = (mem.a.kernel == PLQ_HEATBATH ? pf.hb24 : pf.metro24)[k];
+            if (mem.pk && k < nk) tv = table_entry((mem.a.kernel == PLQ_HEATBATH ? pf.hb24 : pf.metro24)[k]);
         } else if (threadIdx.x == 64 && pending >= 0) {
             __threadfence();
             atomicAdd(&e.done[pending], (unsigned long long)pending_n);

@@ -38,11 +38,20 @@ __device__ __forceinline__ int popc_w(uint64_t v) { return __popcll(v); }
 // cur + 2 * count, a nibble: eight variables' keys are gathered into one word
 // (pairs (cur, c0) and (c1, c2) interleaved at two-bit granularity, Hacker's
 // Delight's outer perfect shuffle without its last stage), and the key times
-// four is the byte offset of its entry in the shared-memory table tab.  The
-// draw of variable j is the keyed stream's at index v0 + j * DV, composed as
-// keyed24 does (mix = keyed_mix(sweep)).  Returns the
-// bits to flip, at 2j: Metropolis accepts when the draw is below the entry;
-// heat bath sets the new state to (entry <= draw).
+// four is the byte offset of its entry in the shared-memory table tab, whose
+// entries are at most 2^24 (the table's "always" sentinel clamped there, which
+// every 24-bit draw is below).  The draw of variable j is the keyed stream's at
+// index v0 + j * DV, composed as keyed24 does (mix = keyed_mix(sweep)).
+// Returns the bits to flip, at 2j: Metropolis accepts when the draw is below
+// the entry; heat bath sets the new state to (entry <= draw).
+//
+// A decision is k < e for k < 2^24 and e <= 2^24, so k - e lies in
+// (-2^24, 2^24) and its top two bits are 11 exactly when k < e, 00 otherwise:
+// a funnel shift moves them in below the decisions so far (variables taken
+// from the last to the first, so variable i's pair lands at bits 2i, 2i + 1)
+// and one mask keeps bit 2i.
+__device__ __forceinline__ uint32_t table_entry(uint32_t e) { return e < (1u << 24) ? e : (1u << 24); }
+
 // Eight (or, TAIL, the first m < 8) variables of a row from their key word x
 // (nibble i: variable i's key): the flip or new-state bits at 2i.
 template <int DV, bool HB, bool TAIL>
@@ -50,16 +59,15 @@ __device__ __forceinline__ uint32_t decide8(uint32_t x, int m, uint32_t vc, uint
                                             const char *tb) {
     uint32_t o = 0;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 7; i >= 0; --i) {
         if (!TAIL || i < m) {
             const uint32_t key4 = i == 0 ? (x << 2) & 0x3Cu : (x >> (4 * i - 2)) & 0x3Cu;
             const uint32_t e = *reinterpret_cast<const uint32_t *>(tb + key4);
             const uint32_t k = lowbias32_tail(lowbias32_head(seed32 ^ (vc + (uint32_t)(i * DV))) ^ mix) >> 8;
-            const bool b = HB ? e <= k : k < e;
-            o |= (uint32_t)b << (2 * i);
+            o = __funnelshift_l(k - e, o, 2);
         }
     }
-    return o;
+    return HB ? ~o & (TAIL ? 0x5555u >> (16 - 2 * m) : 0x5555u) : o & 0x5555u;
 }
 
 // decide8 over eight (or, TAIL, the first m < 8) variables whose first rounds
@@ -70,16 +78,15 @@ __device__ __forceinline__ uint32_t decide8_h1(uint32_t x, const uint32_t (&h1)[
                                                const char *tb, int m = 8) {
     uint32_t o = 0;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 7; i >= 0; --i) {
         if (!TAIL || i < m) {
             const uint32_t key4 = i == 0 ? (x << 2) & 0x3Cu : (x >> (4 * i - 2)) & 0x3Cu;
             const uint32_t e = *reinterpret_cast<const uint32_t *>(tb + key4);
             const uint32_t k = lowbias32_tail(h1[i] ^ mix) >> 8;
-            const bool b = HB ? e <= k : k < e;
-            o |= (uint32_t)b << (2 * i);
+            o = __funnelshift_l(k - e, o, 2);
         }
     }
-    return o;
+    return HB ? ~o & (TAIL ? 0x5555u >> (16 - 2 * m) : 0x5555u) : o & 0x5555u;
 }
 
 // The key word of variables 8c .. 8c + 7: pairs (cur, c0) of P and (c1, c2)

@@ -100,9 +100,9 @@ __global__ void __launch_bounds__(kPackedThreads) first_hash_kernel(uint4 *H, in
 }
 
 template <int D, bool HB, bool CACHED>
-__global__ void __launch_bounds__(kPackedThreads) packed_pass_kernel(PackedPassArgs a) {
+__global__ void __launch_bounds__(kPackedThreads, 8) packed_pass_kernel(PackedPassArgs a) {
     __shared__ uint32_t s_tab[16];
-    if (threadIdx.x < 16) s_tab[threadIdx.x] = threadIdx.x < (unsigned)a.n_keys ? a.table[threadIdx.x] : 0u;
+    if (threadIdx.x < 16) s_tab[threadIdx.x] = threadIdx.x < (unsigned)a.n_keys ? table_entry(a.table[threadIdx.x]) : 0u;
     __syncthreads();
     const uint32_t wpr = (uint32_t)a.L0 / 64;  // words per row
     const uint32_t rows = (uint32_t)(a.n_words / wpr);
