@@ -141,3 +141,20 @@ def test_integration_binding_lists_every_entry_point():
     block = block[:block.index("\n}\n")]
     bound = set(re.findall(r"pub fn (plq_[a-z0-9_]+)\(", block))
     assert set(declared_symbols()) <= bound, sorted(set(declared_symbols()) - bound)
+
+
+def test_python_constants_mirror_the_header():
+    """The ctypes layer's status codes, descriptor flags and limits equal the
+    header's #defines (a flag added to one side only would silently select
+    another pass body)."""
+    text = open(os.path.join(ROOT, "include", "plaquette.h")).read()
+    defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"^#define (PLQ_[A-Z0-9_]+) (\d+)", text, re.M)}
+    codes = ["PLQ_OK", "PLQ_ENODEV", "PLQ_EINVAL", "PLQ_EUNSUPPORTED", "PLQ_ECUDA", "PLQ_ENOMEM", "PLQ_ECAP",
+             "PLQ_EDEVICE", "PLQ_EBUSY"]
+    for name in codes:
+        assert getattr(plq, name) == defines[name], name
+    flags = [n for n in defines if n.startswith("PLQ_FLAG_")]
+    assert len(flags) >= 6
+    for name in flags:
+        assert getattr(plq, name[len("PLQ_"):]) == defines[name], name
+    assert plq.MAX_D == defines["PLQ_MAX_D"] and plq.MAX_Q == defines["PLQ_MAX_Q"]
