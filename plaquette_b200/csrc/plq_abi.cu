@@ -6,11 +6,14 @@
 // enqueues sweeps without waiting, `next` hands back an owned copy.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/plaquette.h"
@@ -253,7 +256,7 @@ void chain_free(plq_chain *c) {
 // step: a byte b is flagged when b >= 128 or b + (128 - q) reaches 128; a carry
 // out of a byte happens only when that byte is flagged already, so a clean
 // block is clean byte for byte.  The flagged block is then scanned bytewise.
-int64_t first_state_at_least(const uint8_t *a, int64_t n, int q) {
+static int64_t first_state_at_least_serial(const uint8_t *a, int64_t n, int q) {
     const uint64_t H = 0x8080808080808080ull, add = 0x0101010101010101ull * (uint64_t)(128 - q);
     int64_t i = 0;
     for (; i + 64 <= n; i += 64) {
@@ -268,6 +271,61 @@ int64_t first_state_at_least(const uint8_t *a, int64_t n, int q) {
     for (; i < n; ++i)
         if (a[i] >= q) return i;
     return -1;
+}
+
+// The start checks run on several host threads: the scan is memory-bound at a few GB/s per
+// thread, and a 512^3 start (134 MB) or a whole ensemble's starts (tens of MB) would otherwise
+// take several milliseconds of creation.  Work is dealt out in increasing order and a thread
+// stops taking pieces past the earliest failure found, so the result is the serial scan's.
+static int scan_threads(int64_t pieces) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    return (int)std::min<int64_t>(pieces, std::min(16u, hw ? hw : 1u));
+}
+
+template <class F>
+static int64_t first_failing(int64_t pieces, F scan_piece) {
+    const int T = scan_threads(pieces);
+    if (T <= 1) {
+        for (int64_t p = 0; p < pieces; ++p)
+            if (scan_piece(p)) return p;
+        return -1;
+    }
+    std::atomic<int64_t> next{0}, first_bad{pieces};
+    auto work = [&]() {
+        for (;;) {
+            const int64_t p = next.fetch_add(1);
+            if (p >= first_bad.load()) return;
+            if (scan_piece(p)) {
+                int64_t cur = first_bad.load();
+                while (p < cur && !first_bad.compare_exchange_weak(cur, p)) {
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(work);
+    work();
+    for (std::thread &t : pool) t.join();
+    const int64_t b = first_bad.load();
+    return b < pieces ? b : -1;
+}
+
+int64_t first_state_at_least(const uint8_t *a, int64_t n, int q) {
+    constexpr int64_t kPiece = int64_t(1) << 22;  // 4 MiB
+    const int64_t pieces = (n + kPiece - 1) / kPiece;
+    if (pieces <= 2) return first_state_at_least_serial(a, n, q);
+    const int64_t p = first_failing(pieces, [&](int64_t k) {
+        return first_state_at_least_serial(a + k * kPiece, std::min(kPiece, n - k * kPiece), q) >= 0;
+    });
+    if (p < 0) return -1;
+    return p * kPiece + first_state_at_least_serial(a + p * kPiece, std::min(kPiece, n - p * kPiece), q);
+}
+
+int32_t first_bad_start(int32_t n, const uint8_t *const *starts, const int64_t *n_vars, const int *q) {
+    const int64_t m = first_failing(n, [&](int64_t k) {
+        return starts[k] && first_state_at_least_serial(starts[k], n_vars[k], q[k]) >= 0;
+    });
+    return (int32_t)m;
 }
 
 extern "C" int plq_chain_create(plq_ctx *ctx, const plq_chain_desc *desc, const uint8_t *start,

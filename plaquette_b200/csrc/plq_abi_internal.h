@@ -93,6 +93,8 @@ struct plq_chain {
 int plq_fail(int code, const std::string &msg);
 // Index of the first byte >= q (q <= 64) in a[0, n), or -1 (64 bytes per step).
 int64_t first_state_at_least(const uint8_t *a, int64_t n, int q);
+// The smallest member index m whose start (if not null) holds a state >= q[m], or -1.
+int32_t first_bad_start(int32_t n, const uint8_t *const *starts, const int64_t *n_vars, const int *q);
 std::string shape_string(const plq_chain_desc *d);
 void chain_free(plq_chain *c);
 int local_sweep(plq_chain *c);

@@ -1254,6 +1254,19 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         if (d.sweep_offset != descs[0].sweep_offset)
             return plq_fail(PLQ_EINVAL, "ensemble members share one sweep counter: every sweep_offset must be equal");
     }
+    if (starts) {  // every member's start below its q, checked on the host threads
+        std::vector<int64_t> nv(n);
+        std::vector<int> qs(n);
+        for (int32_t m = 0; m < n; ++m) {
+            const plq_chain_desc &d = descs[m];
+            int64_t ns = 1;
+            for (int i = 0; i < d.d; ++i) ns *= d.shape[i];
+            nv[m] = d.model == PLQ_GAUGE ? ns * d.d : ns;
+            qs[m] = d.model == PLQ_POTTS ? d.q : 2;
+        }
+        if (first_bad_start(n, starts, nv.data(), qs.data()) >= 0)
+            return plq_fail(PLQ_EINVAL, "start state out of range");
+    }
     cudaError_t ce = plq_enter_device(ctx->device);
     if (ce != cudaSuccess) return ens_fail(ce, "cudaSetDevice");
     plq_ensemble *E = new plq_ensemble();
@@ -1306,8 +1319,6 @@ extern "C" int plq_ensemble_create(plq_ctx *ctx, int32_t n, const plq_chain_desc
         a.words = !(d.flags & PLQ_FLAG_GENERIC_PASS) &&
                   words_eligible(d.model, q, d.d, a.g.L, d.updater, d.rng) ? 1 : 0;
         mem.wpt = tuned_wpt(d);
-        if (starts && starts[m] && first_state_at_least(starts[m], mem.n_vars, q) >= 0)
-            return fail(plq_fail(PLQ_EINVAL, "start state out of range"));
         ModelParams p;
         std::memset(&p, 0, sizeof p);
         p.model = d.model;

@@ -246,3 +246,19 @@ def test_packed_members_match_their_own_chains(gpu, spec):
     pa, pb = a.primaries_all(), b.primaries_all()
     for m in range(3):
         assert list(pa[m]) == list(pb[m]) == list(a.primaries(m)), m
+
+
+def test_out_of_range_start_is_refused(gpu):
+    """A start state >= q in any member (checked on the host threads before
+    anything is allocated) refuses the whole ensemble."""
+    descs, starts = [], []
+    for k, shape in enumerate(((16, 16, 16), (8, 8, 8), (32, 16))):
+        n = int(np.prod(shape))
+        starts.append(plq.hot_start(200 + k, 2, n)[0])
+        descs.append(plq.make_desc(plq.ISING, 2, shape, plq.METROPOLIS, beta=0.3, seed=200 + k, rng=plq.RNG_KEYED,
+                                   batch=1))
+    Ensemble(gpu, descs, starts).close()
+    bad = [s.copy() for s in starts]
+    bad[1][37] = 2
+    with pytest.raises(plq.PlaquetteError, match="start state out of range"):
+        Ensemble(gpu, descs, bad)
